@@ -1,0 +1,136 @@
+/* bbb_internal.h -- shared declarations of libbbb200's CUDA layer.
+ *
+ * Device data layout (HBM):
+ *  - Flow fields keep the reference's ghost-padded layouts (Gcc, Gfx, Gfy,
+ *    Gfz with one ghost layer, x fastest), so push/pull are plain copies and
+ *    the boundary-condition semantics stay identical.
+ *  - Krylov vectors are un-ghosted and dense (n = nx*ny*nz for the
+ *    pressure, (nx+1)*ny*nz etc. for the Helmholtz components), row length a
+ *    multiple of 32 elements at the benchmark sizes, so every warp access is
+ *    a full 128-byte line.  Periodic neighbours are found by index wrap.
+ *  - The matrix is never stored: one byte per unknown (bbb_mask bits) holds
+ *    the six face weights |flag| and the identity-row bit; diagonal and
+ *    Jacobi scale are recomputed from it in registers.
+ */
+#ifndef BBB_INTERNAL_H
+#define BBB_INTERNAL_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/bluebottle_b200.h"
+
+/* mask bits */
+#define BBB_MW 0x01
+#define BBB_ME 0x02
+#define BBB_MS 0x04
+#define BBB_MN 0x08
+#define BBB_MB 0x10
+#define BBB_MT 0x20
+#define BBB_MID 0x40   /* identity row (particle cell / particle face) */
+
+/* one linear system on a dense box nx*ny*nz */
+struct bbb_box {
+  int nx, ny, nz;
+  int perx, pery, perz;     /* periodic wrap along each axis            */
+  int dupx, dupy, dupz;     /* the axis carries the duplicated periodic
+                               face (Gfx along x etc.): wrap skips it     */
+  long long n;
+};
+
+/* constant part of a 7-point operator: off-diagonal weight along each axis
+ * and the diagonal convention */
+struct bbb_op {
+  double wx, wy, wz;        /* weight of one face (|flag| = 1)            */
+  int helmholtz;            /* 0: Poisson  A = sum w (x_nb - x_c)
+                               1: Helmholtz A = x_c + sum w (x_c - x_nb) */
+};
+
+/* device-resident scalars of one Krylov solve; kernels read and write them
+ * so that no host round trip is needed inside an iteration */
+struct bbb_kry {
+  double rho, alpha, omega, beta;  /* BiCGSTAB / CG recurrences           */
+  double tol;                      /* absolute tolerance rtol*||b||       */
+  double bnorm, rnorm;             /* ||b||, latest residual norm         */
+  double sumx;                     /* sum of the solution (mean removal)  */
+  double t_s, t_t, s_s;            /* (t,s), (t,t), (s,s) of the last K2  */
+  int iter, maxit, done, converged, s_conv, status, first, pad;
+  unsigned int ticket;             /* last-block election counter         */
+};
+
+/* device state of the library (one GPU) */
+struct bbb_dev {
+  int ready;
+  int dev;
+  cudaStream_t stream;
+  /* ghosted flow fields */
+  real *p0, *p, *phi;
+  real *u, *v, *w, *u0, *v0, *w0, *us, *vs, *ws;
+  real *conv_u, *conv_v, *conv_w, *conv0_u, *conv0_v, *conv0_w;
+  real *diff_u, *diff_v, *diff_w, *diff0_u, *diff0_v, *diff0_w;
+  int *phase, *phase_shell, *flag_u, *flag_v, *flag_w;
+  /* matrix-free operator masks (dense, un-ghosted) */
+  uint8_t *mask_p, *mask_u, *mask_v, *mask_w;
+  int masks_valid;
+  /* Krylov workspace, FP64 (dense; sized for the largest system) */
+  long long nmax;
+  double *kb, *kx, *kr, *krh, *kp[2], *kv[2], *ks, *kt;
+  /* FP32 workspace of the mixed-precision form */
+  float *fb, *fx, *fr, *frh, *fp[2], *fv[2], *fs, *ft;
+  double *partials;                /* per-block reduction partials       */
+  int max_blocks;
+  bbb_kry *kry;                    /* device scalars                     */
+  bbb_kry *kry_host;               /* pinned mirror                      */
+  /* particles */
+  int np, stride;
+  part_struct *parts;
+  real *coef[18];
+  real *node_pp, *node_ur, *node_ut, *node_up;   /* nparts*26 each */
+  real *perr;                      /* per-particle Lamb error            */
+  real *red_host;                  /* pinned scratch for host reductions */
+  double *red_dev;                 /* device scratch for small reductions */
+  unsigned int *red_ticket;
+  long long launches;
+};
+
+extern bbb_dev g_dev;
+
+/* grid geometry passed to kernels by value */
+struct bbb_geom {
+  int nx, ny, nz;
+  int cc_s1, cc_s2, fx_s1, fx_s2, fy_s1, fy_s2, fz_s1, fz_s2;
+  long long cc_n, fx_n, fy_n, fz_n;          /* ghosted element counts */
+  double dx, dy, dz, xs, ys, zs, xe, ye, ze, xl, yl, zl;
+};
+
+bbb_geom bbb_make_geom(void);
+
+/* status / error plumbing (bbb_host.c) */
+#ifdef __cplusplus
+extern "C" {
+#endif
+void bbb_set_status(int status, const char *where);
+int bbb_fail_exit(void);
+extern bbb_options g_opt;
+extern bbb_stats g_stats;
+void bbb_record_solver(const char *name, int niter, real resid);
+#ifdef __cplusplus
+}
+#endif
+
+#define BBB_CK(call) do { cudaError_t e_ = (call); if(e_ != cudaSuccess) { \
+  bbb_set_status(BBB_ERR_CUDA, cudaGetErrorString(e_)); } } while(0)
+#define BBB_LAUNCHED() do { g_dev.launches++; \
+  cudaError_t e_ = cudaPeekAtLastError(); if(e_ != cudaSuccess) \
+    bbb_set_status(BBB_ERR_CUDA, cudaGetErrorString(e_)); } while(0)
+
+/* entry points between the .cu files */
+void bbb_dev_require(void);
+void bbb_build_masks(void);
+int bbb_poisson_solve(int record);
+int bbb_helmholtz_solve(int comp);
+void bbb_part_BC_fields(real *uu, real *vv, real *ww);
+void bbb_star_rhs(int comp_mask, int explicit_ab2);
+void bbb_pp_rhs_to_b(void);
+double bbb_dev_sum_interior_cc(const real *f);
+
+#endif

@@ -1,0 +1,834 @@
+/* bbb_krylov.cu -- matrix-free Jacobi-preconditioned Krylov solvers.
+ *
+ * Replaces the reference's CUSP calls (src/cuda_bicgstab.cu:44-1073):
+ * the 13-diagonal DIA matrices it rebuilds every call (13 words per row,
+ * src/bicgstab_kernel.cu:643-1856) are never formed.  One byte per unknown
+ * holds the six face weights |flag| and the identity-row bit; the operator
+ * is applied from that byte inside the fused kernels.
+ *
+ * BiCGSTAB (right-preconditioned, as CUSP's krylov::bicgstab) runs as three
+ * fused passes per iteration, with all scalars kept on the device:
+ *   K1  p = r + beta (p - omega v);  v = A M p;   (rh, v)      -> alpha
+ *   K2  s = r - alpha v;             t = A M s;   (t,s) (t,t) (s,s)
+ *   K3  x += alpha M p + omega M s;  r = s - omega t;  (rh,r) (r,r) sum x
+ * 17 vector words + 3 mask bytes per unknown and iteration.  CG (CUSP's
+ * krylov::cg, used for the Crank-Nicolson Helmholtz solves) runs as two:
+ *   C1  p = M r + beta p;  y = A p;  (y, p)
+ *   C2  x += alpha p;  r -= alpha y;  (r, M r) (r, r)
+ * Stopping rule of CUSP's monitor: ||r|| <= rtol ||b||, iteration count
+ * advanced once per full iteration, early exit when ||s|| meets it.
+ *
+ * Stencil kernels tile x-y as 32x8 (one thread per column) and march along
+ * z through a slab; the x-y halo of the producer values sits in a
+ * three-plane shared-memory ring (one barrier per plane), the z neighbours
+ * of a column stay in registers.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+#include "bbb_internal.h"
+#include "bbb_reduce.cuh"
+
+#define TX 32
+#define TY 8
+#define HX (TX + 2)
+#define HY (TY + 2)
+#define NTHR (TX * TY)
+
+/* operator constants in the form the kernels use */
+struct opc {
+  double wx, wy, wz;   /* Poisson: +|f|/dx^2; Helmholtz: 0.5 nu dt/dx^2 */
+  int helm;
+};
+
+struct boxc {
+  int nx, ny, nz;
+  int wW, wE, wS, wN, wB, wT;   /* wrapped neighbour index at each edge */
+  int slab;                     /* planes per block                    */
+};
+
+static boxc make_box(int nx, int ny, int nz, int perx, int pery, int perz,
+  int dupx, int dupy, int dupz)
+{
+  boxc b;
+  b.nx = nx; b.ny = ny; b.nz = nz;
+  b.wW = perx ? (dupx ? nx - 2 : nx - 1) : 0;
+  b.wE = perx ? (dupx ? 1 : 0) : nx - 1;
+  b.wS = pery ? (dupy ? ny - 2 : ny - 1) : 0;
+  b.wN = pery ? (dupy ? 1 : 0) : ny - 1;
+  b.wB = perz ? (dupz ? nz - 2 : nz - 1) : 0;
+  b.wT = perz ? (dupz ? 1 : 0) : nz - 1;
+  /* blocks: ~8 per SM resident; aim for several waves of x-y tiles */
+  long long tiles = (long long)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY);
+  int slabs = (int)((148LL * 8 * 4 + tiles - 1) / tiles);
+  if(slabs < 1) slabs = 1;
+  int kz = (nz + slabs - 1) / slabs;
+  if(kz < 4) kz = 4;
+  if(kz > nz) kz = nz;
+  b.slab = kz;
+  return b;
+}
+
+static dim3 box_grid(const boxc &b)
+{
+  return dim3((b.nx + TX - 1) / TX, (b.ny + TY - 1) / TY,
+    (b.nz + b.slab - 1) / b.slab);
+}
+
+__device__ __forceinline__ int mapx(const boxc &b, int g)
+{ return g < 0 ? b.wW : (g >= b.nx ? (g == b.nx ? b.wE : b.nx - 1) : g); }
+__device__ __forceinline__ int mapy(const boxc &b, int g)
+{ return g < 0 ? b.wS : (g >= b.ny ? (g == b.ny ? b.wN : b.ny - 1) : g); }
+__device__ __forceinline__ int mapz(const boxc &b, int g)
+{ return g < 0 ? b.wB : (g >= b.nz ? (g == b.nz ? b.wT : b.nz - 1) : g); }
+
+/* diagonal of the row with mask m, in the reference's summation order */
+__device__ __forceinline__ double op_diag(uint8_t m, const opc &O)
+{
+  if(m & BBB_MID) return 1.;
+  double fW = (m & BBB_MW) ? 1. : 0., fE = (m & BBB_ME) ? 1. : 0.;
+  double fS = (m & BBB_MS) ? 1. : 0., fN = (m & BBB_MN) ? 1. : 0.;
+  double fB = (m & BBB_MB) ? 1. : 0., fT = (m & BBB_MT) ? 1. : 0.;
+  if(!O.helm) {
+    double d = 0.;
+    d -= (fW + fE) * O.wx;
+    d -= (fS + fN) * O.wy;
+    d -= (fB + fT) * O.wz;
+    return d;
+  }
+  double d = 1.;
+  d += fW * O.wx; d += fE * O.wx;
+  d += fS * O.wy; d += fN * O.wy;
+  d += fB * O.wz; d += fT * O.wz;
+  return d;
+}
+
+/* y = (A q)_c from the centre value, its six neighbours and the row mask;
+ * neighbours in the order of the DIA diagonals: B, S, W, C, E, N, T */
+template <typename T>
+__device__ __forceinline__ T op_apply(uint8_t m, const opc &O, T qB, T qS,
+  T qW, T qC, T qE, T qN, T qT)
+{
+  if(m & BBB_MID) return qC;
+  T sg = O.helm ? (T)-1. : (T)1.;
+  T wx = (T)O.wx * sg, wy = (T)O.wy * sg, wz = (T)O.wz * sg;
+  T d = (T)op_diag(m, O);
+  T acc = (T)0.;
+  acc += ((m & BBB_MB) ? wz : (T)0.) * qB;
+  acc += ((m & BBB_MS) ? wy : (T)0.) * qS;
+  acc += ((m & BBB_MW) ? wx : (T)0.) * qW;
+  acc += d * qC;
+  acc += ((m & BBB_ME) ? wx : (T)0.) * qE;
+  acc += ((m & BBB_MN) ? wy : (T)0.) * qN;
+  acc += ((m & BBB_MT) ? wz : (T)0.) * qT;
+  return acc;
+}
+
+__device__ __forceinline__ long long lin(const boxc &b, int i, int j, int k)
+{ return i + (long long)b.nx * (j + (long long)b.ny * k); }
+
+/* ------------------------------------------------ tiled stencil driver
+ * P: producer, evaluated at any (mapped) cell: raw value and the value the
+ *    operator is applied to.  E: epilogue at each owned cell.  The driver
+ *    fills the shared ring for every plane of the slab and calls E with
+ *    (A q) at the owned cell. */
+template <typename T, class P, class E, int NRED>
+__device__ __forceinline__ void tile_stencil(const boxc &B, const opc &O,
+  const uint8_t *__restrict__ mask, P &prod, E &epi, double (&red)[NRED])
+{
+  __shared__ T ring[3][HY][HX];
+  int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
+  int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  int k0 = blockIdx.z * B.slab, k1 = min(k0 + B.slab, B.nz);
+  int i = i0 + tx, j = j0 + ty;
+  bool valid = (i < B.nx) && (j < B.ny);
+  int gi = mapx(B, i), gj = mapy(B, j);
+  /* halo cell of this thread (80 of them; corners are not needed) */
+  int hsx = -1, hsy = -1, hgi = 0, hgj = 0;
+  if(tid < 32) { hsx = tid + 1; hsy = 0; }
+  else if(tid < 64) { hsx = tid - 32 + 1; hsy = HY - 1; }
+  else if(tid < 72) { hsx = 0; hsy = tid - 64 + 1; }
+  else if(tid < 80) { hsx = HX - 1; hsy = tid - 72 + 1; }
+  if(hsx >= 0) { hgi = mapx(B, i0 - 1 + hsx); hgj = mapy(B, j0 - 1 + hsy); }
+
+  T raw_prev, raw_cur, raw_next, q_prev, q_cur, q_next;
+  uint8_t m_cur = 0, m_next = 0;
+  {
+    int kk = mapz(B, k0 - 1);
+    prod.eval(lin(B, gi, gj, kk), raw_prev, q_prev);
+  }
+  {
+    long long c = lin(B, gi, gj, k0);
+    prod.eval(c, raw_cur, q_cur);
+    m_cur = mask[c];
+    ring[0][ty + 1][tx + 1] = q_cur;
+    if(hsx >= 0) {
+      T hr, hq;
+      prod.eval(lin(B, hgi, hgj, k0), hr, hq);
+      ring[0][hsy][hsx] = hq;
+    }
+  }
+  for(int k = k0; k < k1; k++) {
+    int slot = (k - k0) % 3, nslot = (k - k0 + 1) % 3;
+    int kn = mapz(B, k + 1);
+    long long cn = lin(B, gi, gj, kn);
+    prod.eval(cn, raw_next, q_next);
+    m_next = mask[cn];
+    if(k + 1 < k1) {
+      ring[nslot][ty + 1][tx + 1] = q_next;
+      if(hsx >= 0) {
+        T hr, hq;
+        prod.eval(lin(B, hgi, hgj, k + 1), hr, hq);
+        ring[nslot][hsy][hsx] = hq;
+      }
+    }
+    __syncthreads();
+    if(valid) {
+      T Aq = op_apply<T>(m_cur, O, q_prev, ring[slot][ty][tx + 1],
+        ring[slot][ty + 1][tx], q_cur, ring[slot][ty + 1][tx + 2],
+        ring[slot][ty + 2][tx + 1], q_next);
+      epi.at(lin(B, i, j, k), raw_cur, Aq, red);
+    }
+    raw_prev = raw_cur; q_prev = q_cur;
+    raw_cur = raw_next; q_cur = q_next;
+    m_cur = m_next;
+  }
+  (void)raw_prev;
+}
+
+template <typename T>
+__device__ __forceinline__ T dinv_of(uint8_t m, const opc &O)
+{
+  return (T)(1. / op_diag(m, O));
+}
+
+/* ------------------------------------------------ masks */
+
+/* Poisson rows: faces of cell (i,j,k) read at the reference's positions
+ * (src/bicgstab_kernel.cu:1683-1716); identity where phase > -1
+ * (src/bicgstab_kernel.cu:1826-1856) */
+__global__ void k_mask_p(const int *fu, const int *fv, const int *fw,
+  const int *phs, bbb_geom G, uint8_t *mask)
+{
+  long long n = (long long)G.nx * G.ny * G.nz;
+  for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+      t += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(t % G.nx) + 1;
+    long long r = t / G.nx;
+    int j = (int)(r % G.ny) + 1, k = (int)(r / G.ny) + 1;
+    long long W = i + (long long)j * G.fx_s1 + (long long)k * G.fx_s2;
+    long long S = i + (long long)j * G.fy_s1 + (long long)k * G.fy_s2;
+    long long Bq = i + (long long)j * G.fz_s1 + (long long)k * G.fz_s2;
+    uint8_t m = 0;
+    m |= fu[W] != 0 ? BBB_MW : 0;
+    m |= fu[W + 1] != 0 ? BBB_ME : 0;
+    m |= fv[S] != 0 ? BBB_MS : 0;
+    m |= fv[S + G.fy_s1] != 0 ? BBB_MN : 0;
+    m |= fw[Bq] != 0 ? BBB_MB : 0;
+    m |= fw[Bq + G.fz_s2] != 0 ? BBB_MT : 0;
+    if(phs[i + (long long)j * G.cc_s1 + (long long)k * G.cc_s2] > -1) m |= BBB_MID;
+    mask[t] = m;
+  }
+}
+
+/* Helmholtz rows of component c on its face grid: face weights at the
+ * mixed staggered positions the reference uses (src/bicgstab_kernel.cu:
+ * 829-944), identity where the component's own flag < 0
+ * (src/bicgstab_kernel.cu:730-827) */
+__global__ void k_mask_face(const int *fu, const int *fv, const int *fw,
+  bbb_geom G, int comp, int nx, int ny, int nz, uint8_t *mask)
+{
+  long long n = (long long)nx * ny * nz;
+  const int *fs = comp == 0 ? fu : (comp == 1 ? fv : fw);
+  int s1 = comp == 0 ? G.fx_s1 : (comp == 1 ? G.fy_s1 : G.fz_s1);
+  int s2 = comp == 0 ? G.fx_s2 : (comp == 1 ? G.fy_s2 : G.fz_s2);
+  for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+      t += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(t % nx) + 1;
+    long long r = t / nx;
+    int j = (int)(r % ny) + 1, k = (int)(r / ny) + 1;
+    long long W = i + (long long)j * G.fx_s1 + (long long)k * G.fx_s2;
+    long long S = i + (long long)j * G.fy_s1 + (long long)k * G.fy_s2;
+    long long Bq = i + (long long)j * G.fz_s1 + (long long)k * G.fz_s2;
+    uint8_t m = 0;
+    m |= fu[W] != 0 ? BBB_MW : 0;
+    m |= fu[W + 1] != 0 ? BBB_ME : 0;
+    m |= fv[S] != 0 ? BBB_MS : 0;
+    m |= fv[S + G.fy_s1] != 0 ? BBB_MN : 0;
+    m |= fw[Bq] != 0 ? BBB_MB : 0;
+    m |= fw[Bq + G.fz_s2] != 0 ? BBB_MT : 0;
+    if(fs[i + (long long)j * s1 + (long long)k * s2] < 0) m |= BBB_MID;
+    mask[t] = m;
+  }
+}
+
+void bbb_build_masks(void)
+{
+  if(g_dev.masks_valid) return;
+  bbb_geom G = bbb_make_geom();
+  k_mask_p<<<1184, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
+    g_dev.flag_w, g_dev.phase, G, g_dev.mask_p);
+  BBB_LAUNCHED();
+  k_mask_face<<<1184, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
+    g_dev.flag_w, G, 0, G.nx + 1, G.ny, G.nz, g_dev.mask_u);
+  BBB_LAUNCHED();
+  k_mask_face<<<1184, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
+    g_dev.flag_w, G, 1, G.nx, G.ny + 1, G.nz, g_dev.mask_v);
+  BBB_LAUNCHED();
+  k_mask_face<<<1184, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
+    g_dev.flag_w, G, 2, G.nx, G.ny, G.nz + 1, g_dev.mask_w);
+  BBB_LAUNCHED();
+  g_dev.masks_valid = 1;
+}
+
+/* ------------------------------------------------ BiCGSTAB kernels */
+
+/* residual set-up: r = b - A x; rh = r; p = r; (r, r) */
+template <typename T>
+struct prod_x {
+  const T *x;
+  __device__ __forceinline__ void eval(long long c, T &raw, T &q) const
+  { raw = x[c]; q = raw; }
+};
+template <typename T>
+struct epi_res {
+  const T *b; T *r, *rh, *p;
+  __device__ __forceinline__ void at(long long c, T xr, T Ax, double (&red)[2]) const
+  {
+    T rv = b[c] - Ax;
+    r[c] = rv; rh[c] = rv; p[c] = rv;
+    red[0] += (double)rv * (double)rv;
+    red[1] += (double)xr;
+    (void)xr;
+  }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(NTHR) k_bicg_setup(boxc B, opc O,
+  const uint8_t *__restrict__ mask, const T *__restrict__ b, const T *x,
+  T *r, T *rh, T *p, bbb_kry *s, double *partials, double rtol, int maxit)
+{
+  __shared__ double sh[32 * 2];
+  prod_x<T> P{x};
+  epi_res<T> E{b, r, rh, p};
+  double red[2] = {0., 0.};
+  tile_stencil<T>(B, O, mask, P, E, red);
+  if(bbb_grid_partial<2>(red, partials, &s->ticket, sh)) {
+    bbb_grid_finish_sum<2>(red, partials, &s->ticket, sh);
+    if(threadIdx.x == 0 && threadIdx.y == 0) {
+      double rn = sqrt(red[0]);
+      s->rho = red[0];
+      s->rnorm = rn;
+      s->tol = rtol * s->bnorm;
+      s->sumx = red[1];
+      s->iter = 0;
+      s->maxit = maxit;
+      s->first = 1;
+      s->s_conv = 0;
+      s->alpha = s->omega = s->beta = 0.;
+      s->converged = (rn <= s->tol);
+      s->done = s->converged || (maxit <= 0) || !isfinite(rn);
+      s->status = isfinite(rn) ? 0 : BBB_ERR_NONFINITE;
+    }
+  }
+}
+
+/* p = r + beta p + (-beta omega) v, CUSP's axpbypcz form */
+template <typename T>
+struct prod_k1 {
+  const T *r, *p, *v; const uint8_t *mask; opc O; T beta, bo; int first;
+  __device__ __forceinline__ void eval(long long c, T &raw, T &q) const
+  {
+    T pn = first ? p[c] : r[c] + beta * p[c] + bo * v[c];
+    raw = pn;
+    q = dinv_of<T>(mask[c], O) * pn;
+  }
+};
+template <typename T>
+struct epi_k1 {
+  const T *rh; T *pn, *vn;
+  __device__ __forceinline__ void at(long long c, T praw, T Aq, double (&red)[1]) const
+  {
+    pn[c] = praw;
+    vn[c] = Aq;
+    red[0] += (double)rh[c] * (double)Aq;
+  }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(NTHR) k_bicg1(boxc B, opc O,
+  const uint8_t *__restrict__ mask, const T *r, const T *p_old,
+  const T *v_old, const T *__restrict__ rh, T *p_new, T *v_new, bbb_kry *s,
+  double *partials)
+{
+  if(((volatile bbb_kry *)s)->done) return;
+  __shared__ double sh[32];
+  prod_k1<T> P{r, p_old, v_old, mask, O, (T)s->beta,
+    (T)(-s->beta * s->omega), s->first};
+  epi_k1<T> E{rh, p_new, v_new};
+  double red[1] = {0.};
+  tile_stencil<T>(B, O, mask, P, E, red);
+  if(bbb_grid_partial<1>(red, partials, &s->ticket, sh)) {
+    bbb_grid_finish_sum<1>(red, partials, &s->ticket, sh);
+    if(threadIdx.x == 0 && threadIdx.y == 0) {
+      s->alpha = s->rho / red[0];
+      s->first = 0;
+    }
+  }
+}
+
+template <typename T>
+struct prod_k2 {
+  const T *r, *v; const uint8_t *mask; opc O; T alpha;
+  __device__ __forceinline__ void eval(long long c, T &raw, T &q) const
+  {
+    T sv = r[c] - alpha * v[c];
+    raw = sv;
+    q = dinv_of<T>(mask[c], O) * sv;
+  }
+};
+template <typename T>
+struct epi_k2 {
+  T *sv, *tv;
+  __device__ __forceinline__ void at(long long c, T sraw, T Aq, double (&red)[3]) const
+  {
+    sv[c] = sraw;
+    tv[c] = Aq;
+    red[0] += (double)Aq * (double)sraw;
+    red[1] += (double)Aq * (double)Aq;
+    red[2] += (double)sraw * (double)sraw;
+  }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(NTHR) k_bicg2(boxc B, opc O,
+  const uint8_t *__restrict__ mask, const T *r, const T *v, T *s_out,
+  T *t_out, bbb_kry *s, double *partials)
+{
+  if(((volatile bbb_kry *)s)->done) return;
+  __shared__ double sh[32 * 3];
+  prod_k2<T> P{r, v, mask, O, (T)s->alpha};
+  epi_k2<T> E{s_out, t_out};
+  double red[3] = {0., 0., 0.};
+  tile_stencil<T>(B, O, mask, P, E, red);
+  if(bbb_grid_partial<3>(red, partials, &s->ticket, sh)) {
+    bbb_grid_finish_sum<3>(red, partials, &s->ticket, sh);
+    if(threadIdx.x == 0 && threadIdx.y == 0) {
+      s->t_s = red[0];
+      s->t_t = red[1];
+      s->s_s = red[2];
+      double sn = sqrt(red[2]);
+      s->s_conv = (sn <= s->tol);
+      if(s->s_conv) s->rnorm = sn;
+    }
+  }
+}
+
+/* pointwise third pass */
+template <typename T>
+__global__ void __launch_bounds__(256) k_bicg3(long long n, opc O,
+  const uint8_t *__restrict__ mask, T *x, const T *__restrict__ p,
+  const T *__restrict__ sv, const T *__restrict__ tv, T *r,
+  const T *__restrict__ rh, bbb_kry *s, double *partials)
+{
+  if(((volatile bbb_kry *)s)->done) return;
+  __shared__ double sh[32 * 3];
+  double alpha = s->alpha;
+  int sconv = s->s_conv;
+  double omega = sconv ? 0. : s->t_s / s->t_t;
+  T a = (T)alpha, om = (T)omega;
+  double red[3] = {0., 0., 0.};
+  for(long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+      c += (long long)gridDim.x * blockDim.x) {
+    T di = dinv_of<T>(mask[c], O);
+    T xv = x[c];
+    if(sconv) {
+      xv = xv + a * (di * p[c]);
+    } else {
+      T svv = sv[c];
+      xv = xv + a * (di * p[c]) + om * (di * svv);
+      T rv = svv - om * tv[c];
+      r[c] = rv;
+      red[0] += (double)rh[c] * (double)rv;
+      red[1] += (double)rv * (double)rv;
+    }
+    x[c] = xv;
+    red[2] += (double)xv;
+  }
+  if(bbb_grid_partial<3>(red, partials, &s->ticket, sh)) {
+    bbb_grid_finish_sum<3>(red, partials, &s->ticket, sh);
+    if(threadIdx.x == 0) {
+      s->sumx = red[2];
+      if(sconv) {
+        s->converged = 1;
+        s->done = 1;
+      } else {
+        double rho_new = red[0];
+        s->beta = (rho_new / s->rho) * (alpha / omega);
+        s->rho = rho_new;
+        s->omega = omega;
+        s->iter += 1;
+        double rn = sqrt(red[1]);
+        s->rnorm = rn;
+        s->converged = (rn <= s->tol);
+        if(!isfinite(rn)) { s->status = BBB_ERR_NONFINITE; s->done = 1; }
+        if(s->converged || s->iter >= s->maxit) s->done = 1;
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------ Poisson set-up and
+ * write-back (src/bicgstab_kernel.cu:483-562, src/particle_kernel.cu:
+ * 840-940, src/cuda_bicgstab.cu:971-1045) */
+
+/* b = rho_f/dt div(u*) in fluid cells, 0 in particle cells; x = phi;
+ * ||b||^2 -> s->bnorm */
+__global__ void k_pp_rhs(const real *us, const real *vs, const real *ws,
+  const real *ph, const int *phs, bbb_geom G, double rho_dt, double *b,
+  double *x, bbb_kry *s, double *partials)
+{
+  __shared__ double sh[32];
+  double red[1] = {0.};
+  long long n = (long long)G.nx * G.ny * G.nz;
+  double ddx = 1. / G.dx, ddy = 1. / G.dy, ddz = 1. / G.dz;
+  for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+      t += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(t % G.nx) + 1;
+    long long rr = t / G.nx;
+    int j = (int)(rr % G.ny) + 1, k = (int)(rr / G.ny) + 1;
+    long long cu = i + (long long)j * G.fx_s1 + (long long)k * G.fx_s2;
+    long long cv = i + (long long)j * G.fy_s1 + (long long)k * G.fy_s2;
+    long long cw = i + (long long)j * G.fz_s1 + (long long)k * G.fz_s2;
+    long long cc = i + (long long)j * G.cc_s1 + (long long)k * G.cc_s2;
+    double sv = (us[cu + 1] - us[cu]) * ddx;
+    sv += (vs[cv + G.fy_s1] - vs[cv]) * ddy;
+    sv += (ws[cw + G.fz_s2] - ws[cw]) * ddz;
+    sv *= rho_dt;
+    if(phs[cc] > -1) sv = 0.;
+    b[t] = sv;
+    x[t] = ph[cc];
+    red[0] += sv * sv;
+  }
+  if(bbb_grid_partial<1>(red, partials, &s->ticket, sh)) {
+    bbb_grid_finish_sum<1>(red, partials, &s->ticket, sh);
+    if(threadIdx.x == 0) s->bnorm = sqrt(red[0]);
+  }
+}
+
+__global__ void k_pp_writeback(const double *x, real *ph, bbb_geom G,
+  const bbb_kry *s)
+{
+  long long n = (long long)G.nx * G.ny * G.nz;
+  double mean = s->sumx / (double)n;
+  for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+      t += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(t % G.nx) + 1;
+    long long rr = t / G.nx;
+    int j = (int)(rr % G.ny) + 1, k = (int)(rr / G.ny) + 1;
+    ph[i + (long long)j * G.cc_s1 + (long long)k * G.cc_s2] = x[t] + -mean * 1.;
+  }
+}
+
+/* run iterations until the device says done; host polls in growing
+ * batches so that a converged solve costs at most a few no-op launches */
+template <typename LaunchIter>
+static int drive(LaunchIter launch_iter, int maxit)
+{
+  int batch = 1, total = 0;
+  for(;;) {
+    for(int q = 0; q < batch; q++) launch_iter(total + q);
+    total += batch;
+    BBB_CK(cudaMemcpyAsync(g_dev.kry_host, g_dev.kry, sizeof(bbb_kry),
+      cudaMemcpyDeviceToHost, g_dev.stream));
+    BBB_CK(cudaStreamSynchronize(g_dev.stream));
+    if(bbb_last_status() == BBB_ERR_CUDA) return -1;
+    if(g_dev.kry_host->done) break;
+    if(total > maxit + 4) break;
+    if(batch < 16) batch *= 2;
+  }
+  return g_dev.kry_host->iter;
+}
+
+int bbb_poisson_solve(int record)
+{
+  bbb_dev_require();
+  if(!g_dev.ready) return -1;
+  bbb_build_masks();
+  bbb_geom G = bbb_make_geom();
+  boxc B = make_box(G.nx, G.ny, G.nz, bc.pW == BBB_PERIODIC,
+    bc.pS == BBB_PERIODIC, bc.pB == BBB_PERIODIC, 0, 0, 0);
+  opc O;
+  O.wx = 1. / (G.dx * G.dx); O.wy = 1. / (G.dy * G.dy); O.wz = 1. / (G.dz * G.dz);
+  O.helm = 0;
+  long long n = (long long)G.nx * G.ny * G.nz;
+  bbb_kry *s = g_dev.kry;
+  k_pp_rhs<<<1184, 256, 0, g_dev.stream>>>(g_dev.us, g_dev.vs, g_dev.ws,
+    g_dev.phi, g_dev.phase, G, rho_f / dt, g_dev.kb, g_dev.kx, s, g_dev.partials);
+  BBB_LAUNCHED();
+  dim3 grd = box_grid(B), blk(TX, TY);
+  k_bicg_setup<double><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
+    g_dev.kb, g_dev.kx, g_dev.kr, g_dev.krh, g_dev.kp[0], s, g_dev.partials,
+    pp_residual, pp_max_iter);
+  BBB_LAUNCHED();
+  int cur = 0;
+  int it = drive([&](int q) {
+    (void)q;
+    k_bicg1<double><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
+      g_dev.kr, g_dev.kp[cur], g_dev.kv[cur], g_dev.krh, g_dev.kp[cur ^ 1],
+      g_dev.kv[cur ^ 1], s, g_dev.partials);
+    BBB_LAUNCHED();
+    k_bicg2<double><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
+      g_dev.kr, g_dev.kv[cur ^ 1], g_dev.ks, g_dev.kt, s, g_dev.partials);
+    BBB_LAUNCHED();
+    k_bicg3<double><<<1184, 256, 0, g_dev.stream>>>(n, O, g_dev.mask_p,
+      g_dev.kx, g_dev.kp[cur ^ 1], g_dev.ks, g_dev.kt, g_dev.kr, g_dev.krh,
+      s, g_dev.partials);
+    BBB_LAUNCHED();
+    cur ^= 1;
+  }, pp_max_iter);
+  k_pp_writeback<<<1184, 256, 0, g_dev.stream>>>(g_dev.kx, g_dev.phi, G, s);
+  BBB_LAUNCHED();
+  BBB_CK(cudaMemcpyAsync(g_dev.kry_host, s, sizeof(bbb_kry),
+    cudaMemcpyDeviceToHost, g_dev.stream));
+  BBB_CK(cudaStreamSynchronize(g_dev.stream));
+  bbb_kry *h = g_dev.kry_host;
+  real resid = h->bnorm > 0 ? h->rnorm / h->bnorm : h->rnorm;
+  g_stats.pp_solves++;
+  g_stats.pp_iters_total += h->iter;
+  g_stats.pp_iters_last = h->iter;
+  g_stats.pp_resid_last = resid;
+  g_stats.pp_outer_last = 1;
+  if(record) bbb_record_solver("solver_expd.rec", h->iter, resid);
+  if(h->status == BBB_ERR_NONFINITE) bbb_set_status(BBB_ERR_NONFINITE, "pressure-Poisson");
+  if(!h->converged) {
+    bbb_set_status(BBB_ERR_NOT_CONVERGED, "pressure-Poisson");
+    if(bbb_fail_exit()) {
+      printf("The pressure-Poisson equation did not converge.              \n");
+      exit(EXIT_FAILURE);
+    }
+  }
+  return it;
+}
+
+/* src/cuda_bicgstab.cu:715-1073 */
+extern "C" void cuda_PP_bicgstab(int rank)
+{
+  (void)rank;
+  bbb_poisson_solve(1);
+}
+
+/* src/cuda_bicgstab.cu:1178-1204: the un-ghosted Poisson right-hand side
+ * (kept for callers that use it on its own) */
+extern "C" void cuda_PP_rhs(int dev)
+{
+  (void)dev;
+  bbb_dev_require();
+  if(!g_dev.ready) return;
+  bbb_geom G = bbb_make_geom();
+  k_pp_rhs<<<1184, 256, 0, g_dev.stream>>>(g_dev.us, g_dev.vs, g_dev.ws,
+    g_dev.phi, g_dev.phase, G, rho_f / dt, g_dev.kb, g_dev.kx, g_dev.kry,
+    g_dev.partials);
+  BBB_LAUNCHED();
+}
+
+/* ------------------------------------------------ Helmholtz CG */
+
+template <typename T>
+struct prod_c1 {
+  const T *r, *p; const uint8_t *mask; opc O; T beta; int first;
+  __device__ __forceinline__ void eval(long long c, T &raw, T &q) const
+  {
+    T pn = first ? p[c] : (T)1. * (dinv_of<T>(mask[c], O) * r[c]) + beta * p[c];
+    raw = pn;
+    q = pn;
+  }
+};
+template <typename T>
+struct epi_c1 {
+  T *pn, *y;
+  __device__ __forceinline__ void at(long long c, T praw, T Ap, double (&red)[1]) const
+  {
+    pn[c] = praw;
+    y[c] = Ap;
+    red[0] += (double)Ap * (double)praw;
+  }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(NTHR) k_cg1(boxc B, opc O,
+  const uint8_t *__restrict__ mask, const T *r, const T *p_old, T *p_new,
+  T *y, bbb_kry *s, double *partials)
+{
+  if(((volatile bbb_kry *)s)->done) return;
+  __shared__ double sh[32];
+  prod_c1<T> P{r, p_old, mask, O, (T)s->beta, s->first};
+  epi_c1<T> E{p_new, y};
+  double red[1] = {0.};
+  tile_stencil<T>(B, O, mask, P, E, red);
+  if(bbb_grid_partial<1>(red, partials, &s->ticket, sh)) {
+    bbb_grid_finish_sum<1>(red, partials, &s->ticket, sh);
+    if(threadIdx.x == 0 && threadIdx.y == 0) {
+      s->alpha = s->rho / red[0];
+      s->first = 0;
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_cg2(long long n, opc O,
+  const uint8_t *__restrict__ mask, T *x, const T *__restrict__ p, T *r,
+  const T *__restrict__ y, bbb_kry *s, double *partials)
+{
+  if(((volatile bbb_kry *)s)->done) return;
+  __shared__ double sh[32 * 2];
+  T a = (T)s->alpha;
+  double red[2] = {0., 0.};
+  for(long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+      c += (long long)gridDim.x * blockDim.x) {
+    T pv = p[c];
+    x[c] = a * pv + x[c];
+    T rv = -a * y[c] + r[c];
+    r[c] = rv;
+    T z = dinv_of<T>(mask[c], O) * rv;
+    red[0] += (double)rv * (double)z;
+    red[1] += (double)rv * (double)rv;
+  }
+  if(bbb_grid_partial<2>(red, partials, &s->ticket, sh)) {
+    bbb_grid_finish_sum<2>(red, partials, &s->ticket, sh);
+    if(threadIdx.x == 0) {
+      s->beta = red[0] / s->rho;
+      s->rho = red[0];
+      s->iter += 1;
+      double rn = sqrt(red[1]);
+      s->rnorm = rn;
+      s->converged = (rn <= s->tol);
+      if(!isfinite(rn)) { s->status = BBB_ERR_NONFINITE; s->done = 1; }
+      if(s->converged || s->iter >= s->maxit) s->done = 1;
+    }
+  }
+}
+
+/* b = u* on the interior faces of the component, x = 0, r = b, p = M r */
+__global__ void k_cg_setup(const real *star, bbb_geom G, int comp, int nx,
+  int ny, int nz, opc O, const uint8_t *mask, double *x, double *r,
+  double *p, bbb_kry *s, double *partials, double rtol, int maxit)
+{
+  __shared__ double sh[32 * 2];
+  int s1 = comp == 0 ? G.fx_s1 : (comp == 1 ? G.fy_s1 : G.fz_s1);
+  int s2 = comp == 0 ? G.fx_s2 : (comp == 1 ? G.fy_s2 : G.fz_s2);
+  long long n = (long long)nx * ny * nz;
+  double red[2] = {0., 0.};
+  for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+      t += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(t % nx) + 1;
+    long long rr = t / nx;
+    int j = (int)(rr % ny) + 1, k = (int)(rr / ny) + 1;
+    double bv = star[i + (long long)j * s1 + (long long)k * s2];
+    x[t] = 0.;
+    r[t] = bv;
+    double z = dinv_of<double>(mask[t], O) * bv;
+    p[t] = z;
+    red[0] += bv * z;
+    red[1] += bv * bv;
+  }
+  if(bbb_grid_partial<2>(red, partials, &s->ticket, sh)) {
+    bbb_grid_finish_sum<2>(red, partials, &s->ticket, sh);
+    if(threadIdx.x == 0) {
+      double rn = sqrt(red[1]);
+      s->rho = red[0];
+      s->bnorm = rn;
+      s->rnorm = rn;
+      s->tol = rtol * rn;
+      s->iter = 0;
+      s->maxit = maxit;
+      s->first = 1;
+      s->beta = 0.;
+      s->converged = (rn <= s->tol);
+      s->done = s->converged || (maxit <= 0) || !isfinite(rn);
+      s->status = isfinite(rn) ? 0 : BBB_ERR_NONFINITE;
+    }
+  }
+}
+
+__global__ void k_cg_writeback(const double *x, real *star, bbb_geom G,
+  int comp, int nx, int ny, int nz)
+{
+  int s1 = comp == 0 ? G.fx_s1 : (comp == 1 ? G.fy_s1 : G.fz_s1);
+  int s2 = comp == 0 ? G.fx_s2 : (comp == 1 ? G.fy_s2 : G.fz_s2);
+  long long n = (long long)nx * ny * nz;
+  for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+      t += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(t % nx) + 1;
+    long long rr = t / nx;
+    int j = (int)(rr % ny) + 1, k = (int)(rr / ny) + 1;
+    star[i + (long long)j * s1 + (long long)k * s2] = x[t];
+  }
+}
+
+int bbb_helmholtz_solve(int comp)
+{
+  bbb_dev_require();
+  if(!g_dev.ready) return -1;
+  bbb_build_masks();
+  bbb_geom G = bbb_make_geom();
+  int nx = G.nx + (comp == 0), ny = G.ny + (comp == 1), nz = G.nz + (comp == 2);
+  int per[3][3] = {{bc.uW, bc.uS, bc.uB}, {bc.vW, bc.vS, bc.vB}, {bc.wW, bc.wS, bc.wB}};
+  boxc B = make_box(nx, ny, nz, per[comp][0] == BBB_PERIODIC,
+    per[comp][1] == BBB_PERIODIC, per[comp][2] == BBB_PERIODIC,
+    comp == 0, comp == 1, comp == 2);
+  opc O;
+  O.wx = 0.5 * nu * dt * (1. / (G.dx * G.dx));
+  O.wy = 0.5 * nu * dt * (1. / (G.dy * G.dy));
+  O.wz = 0.5 * nu * dt * (1. / (G.dz * G.dz));
+  O.helm = 1;
+  const uint8_t *mask = comp == 0 ? g_dev.mask_u : (comp == 1 ? g_dev.mask_v : g_dev.mask_w);
+  real *star = comp == 0 ? g_dev.us : (comp == 1 ? g_dev.vs : g_dev.ws);
+  long long n = (long long)nx * ny * nz;
+  bbb_kry *s = g_dev.kry;
+  k_cg_setup<<<1184, 256, 0, g_dev.stream>>>(star, G, comp, nx, ny, nz, O,
+    mask, g_dev.kx, g_dev.kr, g_dev.kp[0], s, g_dev.partials, pp_residual,
+    pp_max_iter);
+  BBB_LAUNCHED();
+  dim3 grd = box_grid(B), blk(TX, TY);
+  int cur = 0;
+  int it = drive([&](int q) {
+    (void)q;
+    k_cg1<double><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, g_dev.kr,
+      g_dev.kp[cur], g_dev.kp[cur ^ 1], g_dev.kv[0], s, g_dev.partials);
+    BBB_LAUNCHED();
+    k_cg2<double><<<1184, 256, 0, g_dev.stream>>>(n, O, mask, g_dev.kx,
+      g_dev.kp[cur ^ 1], g_dev.kr, g_dev.kv[0], s, g_dev.partials);
+    BBB_LAUNCHED();
+    cur ^= 1;
+  }, pp_max_iter);
+  k_cg_writeback<<<1184, 256, 0, g_dev.stream>>>(g_dev.kx, star, G, comp,
+    nx, ny, nz);
+  BBB_LAUNCHED();
+  bbb_kry *h = g_dev.kry_host;
+  real resid = h->bnorm > 0 ? h->rnorm / h->bnorm : h->rnorm;
+  g_stats.helm_iters_total += h->iter;
+  bbb_record_solver("solver_helmholtz_expd.rec", h->iter, resid);
+  if(!h->converged) {
+    bbb_set_status(BBB_ERR_NOT_CONVERGED, "Helmholtz");
+    if(bbb_fail_exit()) {
+      printf("The Helmholtz equation did not converge.              \n");
+      exit(EXIT_FAILURE);
+    }
+  }
+  return it;
+}
+
+/* src/cuda_bicgstab.cu:44-316 (and the v, w variants): RHS, boundary
+ * conditions on u*, particle velocities on u*, then the CG solve */
+static void helmholtz_entry(int comp)
+{
+  bbb_star_rhs(1 << comp, 0);
+  cuda_dom_BC_star();
+  if(nparts > 0) cuda_part_BC_star();
+  bbb_helmholtz_solve(comp);
+}
+
+extern "C" void cuda_ustar_helmholtz(int rank) { (void)rank; helmholtz_entry(0); }
+extern "C" void cuda_vstar_helmholtz(int rank) { (void)rank; helmholtz_entry(1); }
+extern "C" void cuda_wstar_helmholtz(int rank) { (void)rank; helmholtz_entry(2); }

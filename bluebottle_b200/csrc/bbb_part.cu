@@ -1,0 +1,1145 @@
+/* bbb_part.cu -- Physalis particle coupling on the device.
+ *
+ *  - cage build (src/cuda_particle.cu:357-896): the reference computes the
+ *    cage extents on the host and launches up to seven build_phase kernels
+ *    per particle from a host loop; here one kernel computes every extent
+ *    and one CTA per particle marks its cells.  Overlapping cages resolve
+ *    to the highest particle index (atomicMax), which is what the
+ *    reference's index-ordered launches produce.  Distances use explicitly
+ *    rounded operations (no fused multiply-add) so the integer results
+ *    (phase, phase_shell, flag_u/v/w) match an FP64 CPU evaluation bit for
+ *    bit.
+ *  - Lamb boundary velocities, internal rigid-body fill and the in-particle
+ *    pressure (src/particle_kernel.cu:535-1018, src/bluebottle_kernel.cu:
+ *    3916-4022).
+ *  - quadrature, coefficients and forces (src/quadrature_kernel.cu:45-576)
+ *    with one 32-thread block per particle, node per lane.
+ *  - coefficient error (src/quadrature_kernel.cu:578-654) and the
+ *    Newton-Euler update (src/bluebottle_kernel.cu:2247-2398).
+ */
+#include <float.h>
+#include <math.h>
+#include <string.h>
+#include "bbb_internal.h"
+#include "bbb_reduce.cuh"
+
+#define PI BBB_PI
+#define DIV_ST BBB_DIV_ST
+
+/* ------------------------------------------------ cage build */
+
+__global__ void k_reset_cages(int *phs, int *shl, long long ncc, int *fu,
+  long long nfx, int *fv, long long nfy, int *fw, long long nfz)
+{
+  long long st = (long long)gridDim.x * blockDim.x;
+  for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ncc; t += st) {
+    phs[t] = -1; shl[t] = 1;
+  }
+  for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nfx; t += st) fu[t] = 1;
+  for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nfy; t += st) fv[t] = 1;
+  for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nfz; t += st) fw[t] = 1;
+}
+
+__device__ __forceinline__ void cage_extent(int n_in, double pos, double s,
+  double dlt, int gs, int ge, int *cs, int *cbs, int *ce, int *cbe)
+{
+  double q = round(__ddiv_rn(__dsub_rn(pos, s), dlt));
+  int is = (int)__dadd_rn(__dsub_rn(q, __dmul_rn(0.5, (double)n_in)), (double)BBB_DOM_BUF);
+  int ie = is + n_in;
+  int ibs, ibe;
+  if(is < gs) { is = is + ge; ibs = ge; ibe = gs; }
+  else if(ie > ge) { ie = ie - ge; ibs = ge; ibe = gs; }
+  else { ibs = ie; ibe = ie; }
+  *cs = is; *cbs = ibs; *ce = ie; *cbe = ibe;
+}
+
+/* cage extents, src/cuda_particle.cu:462-531 */
+__global__ void k_cage_extents(part_struct *parts, int np, bbb_geom G,
+  int gis, int gie, int gjs, int gje, int gks, int gke)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= np) return;
+  part_struct *q = &parts[i];
+  cage_struct c;
+  c.in = (int)(2.0 * ceil(__ddiv_rn(q->r, G.dx))) + 2;
+  c.jn = (int)(2.0 * ceil(__ddiv_rn(q->r, G.dy))) + 2;
+  c.kn = (int)(2.0 * ceil(__ddiv_rn(q->r, G.dz))) + 2;
+  if(G.nx % 2) c.in = c.in - 1;
+  if(G.ny % 2) c.jn = c.jn - 1;
+  if(G.nz % 2) c.kn = c.kn - 1;
+  c.cx = (int)__ddiv_rn(__dadd_rn(__dsub_rn(q->x, G.xs), __dmul_rn(0.5, G.dx)), G.dx);
+  c.cy = (int)__ddiv_rn(__dadd_rn(__dsub_rn(q->y, G.ys), __dmul_rn(0.5, G.dy)), G.dy);
+  c.cz = (int)__ddiv_rn(__dadd_rn(__dsub_rn(q->z, G.zs), __dmul_rn(0.5, G.dz)), G.dz);
+  cage_extent(c.in, q->x, G.xs, G.dx, gis, gie, &c.is, &c.ibs, &c.ie, &c.ibe);
+  cage_extent(c.jn, q->y, G.ys, G.dy, gjs, gje, &c.js, &c.jbs, &c.je, &c.jbe);
+  cage_extent(c.kn, q->z, G.zs, G.dz, gks, gke, &c.ks, &c.kbs, &c.ke, &c.kbe);
+  q->cage = c;
+}
+
+/* one CTA per particle: the (up to eight) periodic pieces of its cage,
+ * src/cuda_particle.cu:544-667 with build_phase src/particle_kernel.cu:93 */
+__global__ void k_build_phase(const part_struct *parts, int *phs, bbb_geom G,
+  int xPer, int yPer, int zPer)
+{
+  int p = blockIdx.x;
+  const part_struct *q = &parts[p];
+  cage_struct c = q->cage;
+  if(c.in <= 0 || c.jn <= 0 || c.kn <= 0) return;
+  double x = q->x, y = q->y, z = q->z, r = q->r;
+  double Xp = __dadd_rn(x, (double)(x < __dadd_rn(G.xs, r)) * G.xl * xPer);
+  double Xm = __dsub_rn(x, G.xl * (double)(x > __dsub_rn(G.xe, r)) * xPer);
+  double Yp = __dadd_rn(y, (double)(y < __dadd_rn(G.ys, r)) * G.yl * yPer);
+  double Ym = __dsub_rn(y, G.yl * (double)(y > __dsub_rn(G.ye, r)) * yPer);
+  double Zp = __dadd_rn(z, (double)(z < __dadd_rn(G.zs, r)) * G.zl * zPer);
+  double Zm = __dsub_rn(z, G.zl * (double)(z > __dsub_rn(G.ze, r)) * zPer);
+  int sx = c.ibe < c.ie, sy = c.jbe < c.je, sz = c.kbe < c.ke;
+  for(int piece = 0; piece < 8; piece++) {
+    int px = piece & 1, py = (piece >> 1) & 1, pz = (piece >> 2) & 1;
+    if((px && !sx) || (py && !sy) || (pz && !sz)) continue;
+    int is = px ? c.ibe : c.is, ie = px ? c.ie : c.ibs;
+    int js = py ? c.jbe : c.js, je = py ? c.je : c.jbs;
+    int ks = pz ? c.kbe : c.ks, ke = pz ? c.ke : c.kbs;
+    double X = px ? Xm : Xp, Y = py ? Ym : Yp, Z = pz ? Zm : Zp;
+    int ni = ie - is, nj = je - js, nk = ke - ks;
+    if(ni <= 0 || nj <= 0 || nk <= 0) continue;
+    double cxo = __dsub_rn(X, G.xs), cyo = __dsub_rn(Y, G.ys), czo = __dsub_rn(Z, G.zs);
+    long long tot = (long long)ni * nj * nk;
+    for(long long t = threadIdx.x; t < tot; t += blockDim.x) {
+      int ti = is + (int)(t % ni);
+      long long rr = t / ni;
+      int tj = js + (int)(rr % nj), tk = ks + (int)(rr / nj);
+      /* a cage wider than the domain can reach past the ghost layer */
+      if(ti < 0 || ti > G.nx + 1 || tj < 0 || tj > G.ny + 1 || tk < 0
+        || tk > G.nz + 1) continue;
+      double xx = __dsub_rn(__dmul_rn(__dsub_rn((double)ti, 0.5), G.dx), cxo);
+      double yy = __dsub_rn(__dmul_rn(__dsub_rn((double)tj, 0.5), G.dy), cyo);
+      double zz = __dsub_rn(__dmul_rn(__dsub_rn((double)tk, 0.5), G.dz), czo);
+      double d = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(xx, xx), __dmul_rn(yy, yy)),
+        __dmul_rn(zz, zz)));
+      if(floor(__ddiv_rn(d, r)) < 1)
+        atomicMax(&phs[ti + (long long)tj * G.cc_s1 + (long long)tk * G.cc_s2], p);
+    }
+  }
+}
+
+/* ghost copies of a cell-centred int field along one axis
+ * (cage_phases_periodic_*, src/particle_kernel.cu:174-221) */
+__global__ void k_periodic_cc(int *f, bbb_geom G, int ax)
+{
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  int b = blockIdx.y * blockDim.y + threadIdx.y;
+  int ni = G.nx + 2, nj = G.ny + 2, nk = G.nz + 2;
+  long long s1 = G.cc_s1, s2 = G.cc_s2;
+  if(ax == 0) {
+    if(a >= nj || b >= nk) return;
+    long long base = a * s1 + b * s2;
+    f[base + 0] = f[base + (ni - 2)];
+    f[base + (ni - 1)] = f[base + 1];
+  } else if(ax == 1) {
+    if(a >= ni || b >= nk) return;
+    long long base = a + b * s2;
+    f[base + 0] = f[base + (nj - 2) * s1];
+    f[base + (nj - 1) * s1] = f[base + 1 * s1];
+  } else {
+    if(a >= ni || b >= nj) return;
+    long long base = a + b * s1;
+    f[base + 0] = f[base + (nk - 2) * s2];
+    f[base + (nk - 1) * s2] = f[base + 1 * s2];
+  }
+}
+
+/* phase_shell sweeps, one thread per line as src/particle_kernel.cu:223-291 */
+__global__ void k_phase_shell(const int *phs, int *shl, bbb_geom G, int ax)
+{
+  int a = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  int b = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  long long s1 = G.cc_s1, s2 = G.cc_s2;
+  long long base, st;
+  int n;
+  if(ax == 0) { if(a > G.ny || b > G.nz) return; base = a * s1 + b * s2; st = 1; n = G.nx; }
+  else if(ax == 1) { if(a > G.nx || b > G.nz) return; base = a + b * s2; st = s1; n = G.ny; }
+  else { if(a > G.nx || b > G.ny) return; base = a + b * s1; st = s2; n = G.nz; }
+  for(int i = 1; i <= n + 1; i++) {
+    long long W = base + (i - 1) * st, E = base + i * st;
+    shl[E] = shl[E] * (1 - (phs[W] < 0 && phs[E] > -1));
+    shl[W] = shl[W] * (1 - (phs[W] > -1 && phs[E] < 0));
+  }
+}
+
+/* cage_flag_u/v/w, src/particle_kernel.cu:410-497 */
+__global__ void k_cage_flags(const int *phs, const int *shl, int *fu, int *fv,
+  int *fw, bbb_geom G)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  int k = blockIdx.z + 1;
+  if(i > G.nx + 1 || j > G.ny + 1) return;
+  long long C = i + (long long)j * G.cc_s1 + (long long)k * G.cc_s2;
+#define FLAG(a, b) (1 - 2 * ((phs[a] < 0 && phs[b] > -1) || (phs[a] > -1 && phs[b] < 0) \
+    || (shl[a] < 1 && shl[b] < 1)))
+  if(j <= G.ny && k <= G.nz)
+    fu[i + (long long)j * G.fx_s1 + (long long)k * G.fx_s2] = FLAG(C - 1, C);
+  if(i <= G.nx && k <= G.nz)
+    fv[i + (long long)j * G.fy_s1 + (long long)k * G.fy_s2] = FLAG(C - G.cc_s1, C);
+  if(i <= G.nx && j <= G.ny)
+    fw[i + (long long)j * G.fz_s1 + (long long)k * G.fz_s2] = FLAG(C - G.cc_s2, C);
+#undef FLAG
+}
+
+/* flag_external_*, src/particle_kernel.cu:499-533 */
+__global__ void k_flag_external(int *f, int s1, int s2, int ni, int nj, int nk,
+  int ax)
+{
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  int b = blockIdx.y * blockDim.y + threadIdx.y;
+  if(ax == 0) {
+    if(a >= nj || b >= nk) return;
+    long long base = (long long)a * s1 + (long long)b * s2;
+    f[base + 1] = 0; f[base + (ni - 2)] = 0;
+  } else if(ax == 1) {
+    if(a >= ni || b >= nk) return;
+    long long base = a + (long long)b * s2;
+    f[base + 1LL * s1] = 0; f[base + (long long)(nj - 2) * s1] = 0;
+  } else {
+    if(a >= ni || b >= nj) return;
+    long long base = a + (long long)b * s1;
+    f[base + 1LL * s2] = 0; f[base + (long long)(nk - 2) * s2] = 0;
+  }
+}
+
+/* periodic ghost copies of a face flag field (cage_flag_*_periodic_*,
+ * src/particle_kernel.cu:293-408); `normal` shifts the source by the
+ * duplicated face */
+__global__ void k_periodic_face(int *f, int s1, int s2, int ni, int nj, int nk,
+  int ax, int normal)
+{
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  int b = blockIdx.y * blockDim.y + threadIdx.y;
+  int sh = normal ? 1 : 0;
+  if(ax == 0) {
+    if(a >= nj || b >= nk) return;
+    long long base = (long long)a * s1 + (long long)b * s2;
+    f[base + 0] = f[base + (ni - 2 - sh)];
+    f[base + (ni - 1)] = f[base + 1 + sh];
+  } else if(ax == 1) {
+    if(a >= ni || b >= nk) return;
+    long long base = a + (long long)b * s2;
+    f[base + 0] = f[base + (long long)(nj - 2 - sh) * s1];
+    f[base + (long long)(nj - 1) * s1] = f[base + (long long)(1 + sh) * s1];
+  } else {
+    if(a >= ni || b >= nj) return;
+    long long base = a + (long long)b * s1;
+    f[base + 0] = f[base + (long long)(nk - 2 - sh) * s2];
+    f[base + (long long)(nk - 1) * s2] = f[base + (long long)(1 + sh) * s2];
+  }
+}
+
+static dim3 face_grid(int n1, int n2) { return dim3((n1 + 31) / 32, (n2 + 7) / 8); }
+
+extern "C" void cuda_build_cages(void)
+{
+  bbb_dev_require();
+  if(!g_dev.ready) return;
+  const dom_struct *d = &Dom;
+  bbb_geom G = bbb_make_geom();
+  cudaStream_t s = g_dev.stream;
+  dim3 blk(32, 8);
+  k_reset_cages<<<1184, 256, 0, s>>>(g_dev.phase, g_dev.phase_shell, d->Gcc.s3b,
+    g_dev.flag_u, d->Gfx.s3b, g_dev.flag_v, d->Gfy.s3b, g_dev.flag_w, d->Gfz.s3b);
+  BBB_LAUNCHED();
+  if(nparts > 0 && g_dev.np == nparts) {
+    k_cage_extents<<<(nparts + 127) / 128, 128, 0, s>>>(g_dev.parts, nparts, G,
+      d->Gcc.is, d->Gcc.ie, d->Gcc.js, d->Gcc.je, d->Gcc.ks, d->Gcc.ke);
+    BBB_LAUNCHED();
+    k_build_phase<<<nparts, 256, 0, s>>>(g_dev.parts, g_dev.phase, G,
+      bc.uE == BBB_PERIODIC, bc.vN == BBB_PERIODIC, bc.wT == BBB_PERIODIC);
+    BBB_LAUNCHED();
+  }
+  int perx = bc.uW == BBB_PERIODIC && bc.uE == BBB_PERIODIC;
+  int pery = bc.uS == BBB_PERIODIC && bc.uN == BBB_PERIODIC;
+  int perz = bc.uB == BBB_PERIODIC && bc.uT == BBB_PERIODIC;
+  int ni = G.nx + 2, nj = G.ny + 2, nk = G.nz + 2;
+  int *pers[2] = {g_dev.phase, g_dev.phase_shell};
+  for(int f = 0; f < 2; f++) {
+    if(f == 1) {
+      k_phase_shell<<<face_grid(G.ny, G.nz), blk, 0, s>>>(g_dev.phase, g_dev.phase_shell, G, 0);
+      BBB_LAUNCHED();
+      k_phase_shell<<<face_grid(G.nx, G.nz), blk, 0, s>>>(g_dev.phase, g_dev.phase_shell, G, 1);
+      BBB_LAUNCHED();
+      k_phase_shell<<<face_grid(G.nx, G.ny), blk, 0, s>>>(g_dev.phase, g_dev.phase_shell, G, 2);
+      BBB_LAUNCHED();
+    }
+    if(perx) { k_periodic_cc<<<face_grid(nj, nk), blk, 0, s>>>(pers[f], G, 0); BBB_LAUNCHED(); }
+    if(pery) { k_periodic_cc<<<face_grid(ni, nk), blk, 0, s>>>(pers[f], G, 1); BBB_LAUNCHED(); }
+    if(perz) { k_periodic_cc<<<face_grid(ni, nj), blk, 0, s>>>(pers[f], G, 2); BBB_LAUNCHED(); }
+  }
+  dim3 grd((G.nx + 1 + 31) / 32, (G.ny + 1 + 7) / 8, G.nz + 1);
+  k_cage_flags<<<grd, blk, 0, s>>>(g_dev.phase, g_dev.phase_shell, g_dev.flag_u,
+    g_dev.flag_v, g_dev.flag_w, G);
+  BBB_LAUNCHED();
+  const grid_info *X = &d->Gfx, *Y = &d->Gfy, *Z = &d->Gfz;
+  if(bc.uW != BBB_PERIODIC && bc.uE != BBB_PERIODIC) {
+    k_flag_external<<<face_grid(X->jnb, X->knb), blk, 0, s>>>(g_dev.flag_u, X->s1b, X->s2b,
+      X->inb, X->jnb, X->knb, 0);
+    BBB_LAUNCHED();
+  }
+  if(bc.vS != BBB_PERIODIC && bc.vN != BBB_PERIODIC) {
+    k_flag_external<<<face_grid(Y->inb, Y->knb), blk, 0, s>>>(g_dev.flag_v, Y->s1b, Y->s2b,
+      Y->inb, Y->jnb, Y->knb, 1);
+    BBB_LAUNCHED();
+  }
+  if(bc.wB != BBB_PERIODIC && bc.wT != BBB_PERIODIC) {
+    k_flag_external<<<face_grid(Z->inb, Z->jnb), blk, 0, s>>>(g_dev.flag_w, Z->s1b, Z->s2b,
+      Z->inb, Z->jnb, Z->knb, 2);
+    BBB_LAUNCHED();
+  }
+  /* periodic flag ghosts; v's x test reads bc.vW twice as the reference
+   * does (src/cuda_particle.cu:845) */
+  struct { int *f; const grid_info *g; int per[3]; int comp; } F[3] = {
+    {g_dev.flag_u, X, {bc.uW == BBB_PERIODIC && bc.uE == BBB_PERIODIC,
+      bc.uS == BBB_PERIODIC && bc.uN == BBB_PERIODIC,
+      bc.uB == BBB_PERIODIC && bc.uT == BBB_PERIODIC}, 0},
+    {g_dev.flag_v, Y, {bc.vW == BBB_PERIODIC && bc.vW == BBB_PERIODIC,
+      bc.vS == BBB_PERIODIC && bc.vN == BBB_PERIODIC,
+      bc.vB == BBB_PERIODIC && bc.vT == BBB_PERIODIC}, 1},
+    {g_dev.flag_w, Z, {bc.wW == BBB_PERIODIC && bc.wE == BBB_PERIODIC,
+      bc.wS == BBB_PERIODIC && bc.wN == BBB_PERIODIC,
+      bc.wB == BBB_PERIODIC && bc.wT == BBB_PERIODIC}, 2}};
+  for(int f = 0; f < 3; f++) {
+    const grid_info *g = F[f].g;
+    int n[3] = {g->inb, g->jnb, g->knb};
+    for(int ax = 0; ax < 3; ax++) {
+      if(!F[f].per[ax]) continue;
+      int t1 = ax == 0 ? 1 : 0, t2 = ax == 2 ? 1 : 2;
+      k_periodic_face<<<face_grid(n[t1], n[t2]), blk, 0, s>>>(F[f].f, g->s1b, g->s2b,
+        g->inb, g->jnb, g->knb, ax, F[f].comp == ax);
+      BBB_LAUNCHED();
+    }
+  }
+  g_dev.masks_valid = 0;
+}
+
+/* ------------------------------------------------ Lamb's series */
+
+__device__ __forceinline__ double d_Nnm(int n, int m)
+{
+  double top = 1, bot = 1;
+  for(int i = 1; i <= (n - m); i++) top *= (double)i;
+  for(int i = 1; i <= (n + m); i++) bot *= (double)i;
+  return sqrt((2. * n + 1.) / 4. / PI * top / bot);
+}
+
+__device__ __forceinline__ double d_Pnm(int n, int m, double theta)
+{
+  double x = cos(theta), y = sin(theta);
+  switch(n * 10 + m) {
+    case 0: return 1;
+    case 10: return x;
+    case 11: return -y;
+    case 20: return 0.5 * (3. * x * x - 1.);
+    case 21: return -3. * x * y;
+    case 22: return 3. * y * y;
+    case 30: return 0.5 * x * (5. * x * x - 3.);
+    case 31: return -1.5 * (5. * x * x - 1.) * y;
+    case 32: return 15. * x * y * y;
+    case 33: return -15. * y * y * y;
+    case 40: return 0.125 * (35. * x * x * x * x - 30. * x * x + 3.);
+    case 41: return -2.5 * (7. * x * x - 3.) * x * y;
+    case 42: return 7.5 * (7. * x * x - 1.) * y * y;
+    case 43: return -105. * x * y * y * y;
+    case 44: return 105. * y * y * y * y;
+    case 50: return 0.125 * x * (63. * x * x * x * x - 70. * x * x + 15.);
+    case 51: return -1.875 * y * (21. * x * x * x * x - 14. * x * x + 1.);
+    case 52: return 52.5 * x * y * y * (3. * x * x - 1.);
+    case 53: return -52.5 * y * y * y * (9. * x * x - 1.);
+    case 54: return 945. * x * y * y * y * y;
+    case 55: return -945. * y * y * y * y * y;
+  }
+  return 0;
+}
+
+__device__ __forceinline__ void d_xyz2rtp(double x, double y, double z,
+  double *r, double *theta, double *phi)
+{
+  double XY = x * x + y * y;
+  double XYZ = XY + z * z;
+  if(XYZ >= 0 && XYZ < DIV_ST) XYZ = DIV_ST;
+  *r = sqrt(XYZ);
+  *theta = acos(z / *r);
+  if(XY >= 0 && XY < DIV_ST) XY = DIV_ST;
+  *phi = acos(x / sqrt(XY));
+  if(y < 0.) *phi = 2. * PI - *phi;
+}
+
+__device__ __forceinline__ int d_cbase(int n)
+{ int c = 0; for(int j = 0; j < n; j++) c += j + 1; return c; }
+
+__device__ __forceinline__ double d_clamp_st(double st)
+{
+  if(st >= 0 && st < DIV_ST) st = DIV_ST;
+  else if(st < 0 && st > -DIV_ST) st = -DIV_ST;
+  return st;
+}
+
+__device__ double d_X(int n, double theta, double phi, const double *re,
+  const double *im, int pp, int stride)
+{
+  int c = d_cbase(n) + pp * stride;
+  double sum = d_Nnm(n, 0) * d_Pnm(n, 0, theta) * re[c];
+  for(int m = 1; m <= n; m++) {
+    c++;
+    sum += 2. * d_Nnm(n, m) * d_Pnm(n, m, theta)
+      * (re[c] * cos(m * phi) - im[c] * sin(m * phi));
+  }
+  return sum;
+}
+
+__device__ double d_Y(int n, double theta, double phi, const double *re,
+  const double *im, int pp, int stride)
+{
+  double ct = cos(theta);
+  double st = d_clamp_st(sin(theta));
+  int c = d_cbase(n) + pp * stride;
+  int m = 0;
+  double sum = d_Nnm(n, m)
+    * (-(n + 1) * ct / st * d_Pnm(n, m, theta) + (n - m + 1) / st * d_Pnm(n + 1, m, theta))
+    * re[c];
+  for(m = 1; m <= n; m++) {
+    c++;
+    sum += 2. * d_Nnm(n, m)
+      * (-(n + 1) * ct / st * d_Pnm(n, m, theta) + (n - m + 1) / st * d_Pnm(n + 1, m, theta))
+      * (re[c] * cos(m * phi) - im[c] * sin(m * phi));
+  }
+  return sum;
+}
+
+__device__ double d_Z(int n, double theta, double phi, const double *re,
+  const double *im, int pp, int stride)
+{
+  double st = d_clamp_st(sin(theta));
+  int c = d_cbase(n) + pp * stride;
+  double sum = 0.;
+  for(int m = 1; m <= n; m++) {
+    c++;
+    sum += -2. * m / st * d_Nnm(n, m) * d_Pnm(n, m, theta)
+      * (re[c] * sin(m * phi) + im[c] * cos(m * phi));
+  }
+  return sum;
+}
+
+struct coef_ptrs { const double *c[6]; };
+
+__device__ void d_lamb_vel(int order, double a, double r, double theta,
+  double phi, double nu, const coef_ptrs &cf, int p, int stride, double *Ux,
+  double *Uy, double *Uz)
+{
+  const double *pre = cf.c[0], *pim = cf.c[1], *fre = cf.c[2], *fim = cf.c[3],
+               *cre = cf.c[4], *cim = cf.c[5];
+  double ar = a / r, ra = r / a;
+  double ur = 0.;
+  double ut = 0.5 * ra * d_Y(0, theta, phi, pre, pim, p, stride);
+  double up = 0.5 * ra * d_Z(0, theta, phi, pre, pim, p, stride);
+  for(int n = 1; n <= order; n++) {
+    double powranp1 = pow(ra, n + 1.);
+    double powranm1 = pow(ra, n - 1.);
+    double powarnp2 = pow(ar, n + 2.);
+    double powarnp1 = pow(ar, n + 1.);
+    double powarn = pow(ar, (double)n);
+    double od2np3 = 1. / (2. * n + 3.);
+    double odnp1 = 1. / (n + 1.);
+    ur += (0.5 * n * od2np3 * powranp1
+      + 0.25 * n * ((2. * n + 1.) * od2np3 * ar * ar - 1.) * powarn)
+      * d_X(n, theta, phi, pre, pim, p, stride);
+    ur += (n * powranm1
+      + 0.5 * n * (2. * n - 1. - (2. * n + 1.) * ra * ra) * pow(ar, n + 2.))
+      * d_X(n, theta, phi, fre, fim, p, stride);
+    ut += (0.5 * (n + 3.) * odnp1 * od2np3 * powranp1
+      + 0.25 * odnp1 * (n - 2. - n * (2. * n + 1.) * od2np3 * ar * ar) * powarn)
+      * d_Y(n, theta, phi, pre, pim, p, stride);
+    ut += (powranm1
+      + 0.5 * odnp1 * ((n - 2.) * (2. * n + 1.) * ra * ra - n * (2. * n - 1.)) * powarnp2)
+      * d_Y(n, theta, phi, fre, fim, p, stride);
+    ut += (powranm1 - powarnp1) * d_Z(n, theta, phi, cre, cim, p, stride);
+    up += (0.5 * (n + 3.) * odnp1 * od2np3 * powranp1
+      + 0.25 * odnp1 * (n - 2. - n * (2. * n + 1.) * od2np3 * ar * ar) * powarn)
+      * d_Z(n, theta, phi, pre, pim, p, stride);
+    up += (powranm1
+      + 0.5 * odnp1 * ((n - 2.) * (2. * n + 1.) * ra * ra - n * (2. * n - 1.)) * powarnp2)
+      * d_Z(n, theta, phi, fre, fim, p, stride);
+    up += (-powranm1 + powarnp1) * d_Y(n, theta, phi, cre, cim, p, stride);
+  }
+  ur *= nu / a;
+  ut *= nu / a;
+  up *= nu / a;
+  *Ux = ur * sin(theta) * cos(phi) + ut * cos(theta) * cos(phi) - up * sin(phi);
+  *Uy = ur * sin(theta) * sin(phi) + ut * cos(theta) * sin(phi) + up * cos(phi);
+  *Uz = ur * cos(theta) - ut * sin(theta);
+}
+
+__device__ __forceinline__ double d_wrap_rel(double x, double a, double L)
+{
+  if(x <= 2. * a - L) x += L;
+  if(x >= L - 2. * a) x -= L;
+  return x;
+}
+
+/* part_BC_u/v/w (src/particle_kernel.cu:535-838): every interior face of
+ * each component, ghost rows included.  Faces that neither border a
+ * particle cell nor carry flag < 1 are left untouched without evaluating
+ * the series. */
+__global__ void k_part_BC(real *uu, real *vv, real *ww, const int *phs,
+  const int *fu, const int *fv, const int *fw, const part_struct *parts,
+  coef_ptrs cf, int stride, double nu, bbb_geom G)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z;
+  for(int comp = 0; comp < 3; comp++) {
+    int ilo = comp == 0 ? 1 : 0, ihi = comp == 0 ? G.nx + 2 : G.nx + 2;
+    int jlo = comp == 1 ? 1 : 0, jhi = comp == 1 ? G.ny + 2 : G.ny + 2;
+    int klo = comp == 2 ? 1 : 0, khi = comp == 2 ? G.nz + 2 : G.nz + 2;
+    if(i < ilo || i >= ihi || j < jlo || j >= jhi || k < klo || k >= khi) continue;
+    int s1 = comp == 0 ? G.fx_s1 : (comp == 1 ? G.fy_s1 : G.fz_s1);
+    int s2 = comp == 0 ? G.fx_s2 : (comp == 1 ? G.fy_s2 : G.fz_s2);
+    long long C = i + (long long)j * s1 + (long long)k * s2;
+    const int *flag = comp == 0 ? fu : (comp == 1 ? fv : fw);
+    if(flag[C] >= 1) continue;
+    long long cc = i + (long long)j * G.cc_s1 + (long long)k * G.cc_s2;
+    long long cstep = comp == 0 ? 1 : (comp == 1 ? G.cc_s1 : G.cc_s2);
+    int P0 = phs[cc - cstep], P1 = phs[cc];
+    int P = P0 > -1 ? P0 : (P1 > -1 ? P1 : -1);
+    if(P < 0) continue;
+    const part_struct *q = &parts[P];
+    double a = q->r;
+    double x = (comp == 0 ? (i - BBB_DOM_BUF) * G.dx : (i - 0.5) * G.dx) + G.xs - q->x;
+    double y = (comp == 1 ? (j - BBB_DOM_BUF) * G.dy : (j - 0.5) * G.dy) + G.ys - q->y;
+    double z = (comp == 2 ? (k - BBB_DOM_BUF) * G.dz : (k - 0.5) * G.dz) + G.zs - q->z;
+    x = d_wrap_rel(x, a, G.xl);
+    y = d_wrap_rel(y, a, G.yl);
+    z = d_wrap_rel(z, a, G.zl);
+    double r, theta, phi;
+    d_xyz2rtp(x, y, z, &r, &theta, &phi);
+    double Ux, Uy, Uz;
+    d_lamb_vel(q->order, a, r, theta, phi, nu, cf, P, stride, &Ux, &Uy, &Uz);
+    double rr = 0.1 / nu * (r * r * r * r * r - a * a * a * a * a) / (r * r * r);
+    double val;
+    if(comp == 0) {
+      val = Ux + q->u + (q->oy * z - q->oz * y);
+      val += rr * (q->oydot * z - q->ozdot * y);
+      uu[C] = val;
+    } else if(comp == 1) {
+      val = Uy + q->v + (-(q->ox * z - q->oz * x));
+      val += rr * (-(q->oxdot * z - q->ozdot * x));
+      vv[C] = val;
+    } else {
+      val = Uz + q->w + (q->ox * y - q->oy * x);
+      val += rr * (q->oxdot * y - q->oydot * x);
+      ww[C] = val;
+    }
+  }
+}
+
+static coef_ptrs cur_coefs(void)
+{
+  coef_ptrs c;
+  for(int a = 0; a < 6; a++) c.c[a] = g_dev.coef[a];
+  return c;
+}
+
+void bbb_part_BC_fields(real *uu, real *vv, real *ww)
+{
+  bbb_dev_require();
+  if(!g_dev.ready || nparts <= 0 || g_dev.np != nparts) return;
+  bbb_geom G = bbb_make_geom();
+  dim3 blk(32, 8), grd((G.nx + 2 + 31) / 32, (G.ny + 2 + 7) / 8, G.nz + 2);
+  k_part_BC<<<grd, blk, 0, g_dev.stream>>>(uu, vv, ww, g_dev.phase,
+    g_dev.flag_u, g_dev.flag_v, g_dev.flag_w, g_dev.parts, cur_coefs(),
+    coeff_stride, nu, G);
+  BBB_LAUNCHED();
+}
+
+/* src/cuda_particle.cu:899-944 */
+extern "C" void cuda_part_BC(void) { bbb_part_BC_fields(g_dev.u, g_dev.v, g_dev.w); }
+/* src/cuda_particle.cu:947-992 */
+extern "C" void cuda_part_BC_star(void) { bbb_part_BC_fields(g_dev.us, g_dev.vs, g_dev.ws); }
+
+/* src/cuda_particle.cu:996-1017: zero the Poisson right-hand side inside
+ * particles (the net effect of part_BC_p for finite values) */
+__global__ void k_zero_rhs_solid(double *b, const int *phs, bbb_geom G)
+{
+  long long n = (long long)G.nx * G.ny * G.nz;
+  for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+      t += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(t % G.nx) + 1;
+    long long rr = t / G.nx;
+    int j = (int)(rr % G.ny) + 1, k = (int)(rr / G.ny) + 1;
+    if(phs[i + (long long)j * G.cc_s1 + (long long)k * G.cc_s2] > -1) b[t] = 0.;
+  }
+}
+
+extern "C" void cuda_part_BC_p(int dev)
+{
+  (void)dev;
+  bbb_dev_require();
+  if(!g_dev.ready) return;
+  bbb_geom G = bbb_make_geom();
+  k_zero_rhs_solid<<<1184, 256, 0, g_dev.stream>>>(g_dev.kb, g_dev.phase, G);
+  BBB_LAUNCHED();
+}
+
+/* part_BC_p_fill, src/particle_kernel.cu:942-1018 */
+__global__ void k_p_fill(real *pp, const int *phs, const part_struct *parts,
+  coef_ptrs cf, int stride, double mu, double nu, double rho_f, double gpx,
+  double gpy, double gpz, bbb_geom G)
+{
+  long long n = (long long)G.nx * G.ny * G.nz;
+  for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+      t += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(t % G.nx) + 1;
+    long long rr = t / G.nx;
+    int j = (int)(rr % G.ny) + 1, k = (int)(rr / G.ny) + 1;
+    long long CC = i + (long long)j * G.cc_s1 + (long long)k * G.cc_s2;
+    int p = phs[CC];
+    if(p < 0) continue;
+    const part_struct *q = &parts[p];
+    double a = q->r;
+    double x = d_wrap_rel((i - 0.5) * G.dx + G.xs - q->x, a, G.xl);
+    double y = d_wrap_rel((j - 0.5) * G.dy + G.ys - q->y, a, G.yl);
+    double z = d_wrap_rel((k - 0.5) * G.dz + G.zs - q->z, a, G.zl);
+    double r, theta, phi;
+    d_xyz2rtp(x, y, z, &r, &theta, &phi);
+    double v = d_X(0, theta, phi, cf.c[0], cf.c[1], p, stride);
+    v *= mu * nu / (a * a);
+    double o2 = (q->oy * z - q->oz * y) * (q->oy * z - q->oz * y);
+    o2 += (q->ox * z - q->oz * x) * (q->ox * z - q->oz * x);
+    o2 += (q->ox * y - q->oy * x) * (q->ox * y - q->oy * x);
+    double acc = (-gpx / rho_f - q->udot) * x + (-gpy / rho_f - q->vdot) * y
+      + (-gpz / rho_f - q->wdot) * z;
+    v += 0.5 * rho_f * o2 + rho_f * acc;
+    pp[CC] = v;
+  }
+}
+
+extern "C" void cuda_part_p_fill(void)
+{
+  bbb_dev_require();
+  if(!g_dev.ready || nparts <= 0 || g_dev.np != nparts) return;
+  bbb_geom G = bbb_make_geom();
+  k_p_fill<<<1184, 256, 0, g_dev.stream>>>(g_dev.p, g_dev.phase, g_dev.parts,
+    cur_coefs(), coeff_stride, mu, nu, rho_f, gradP.x, gradP.y, gradP.z, G);
+  BBB_LAUNCHED();
+}
+
+/* internal_u/v/w, src/bluebottle_kernel.cu:3916-4022 */
+__global__ void k_internal(real *uu, real *vv, real *ww, const int *phs,
+  const int *fu, const int *fv, const int *fw, const part_struct *parts,
+  bbb_geom G)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  int k = blockIdx.z + 1;
+  if(i > G.nx + 1 || j > G.ny + 1) return;
+  long long cc = i + (long long)j * G.cc_s1 + (long long)k * G.cc_s2;
+  for(int comp = 0; comp < 3; comp++) {
+    if(comp == 0 && (j > G.ny || k > G.nz)) continue;
+    if(comp == 1 && (i > G.nx || k > G.nz)) continue;
+    if(comp == 2 && (i > G.nx || j > G.ny)) continue;
+    int s1 = comp == 0 ? G.fx_s1 : (comp == 1 ? G.fy_s1 : G.fz_s1);
+    int s2 = comp == 0 ? G.fx_s2 : (comp == 1 ? G.fy_s2 : G.fz_s2);
+    long long C = i + (long long)j * s1 + (long long)k * s2;
+    long long cstep = comp == 0 ? 1 : (comp == 1 ? G.cc_s1 : G.cc_s2);
+    int pw = phs[cc - cstep], pe = phs[cc];
+    const int *flag = comp == 0 ? fu : (comp == 1 ? fv : fw);
+    if(!(pw > -1 && pe > -1 && flag[C] != -1)) continue;
+    const part_struct *q = &parts[pe];
+    double rx = (comp == 0 ? (i - BBB_DOM_BUF) * G.dx : (i - 0.5) * G.dx) + G.xs - q->x;
+    double ry = (comp == 1 ? (j - BBB_DOM_BUF) * G.dy : (j - 0.5) * G.dy) + G.ys - q->y;
+    double rz = (comp == 2 ? (k - BBB_DOM_BUF) * G.dz : (k - 0.5) * G.dz) + G.zs - q->z;
+    rx = d_wrap_rel(rx, q->r, G.xl);
+    ry = d_wrap_rel(ry, q->r, G.yl);
+    rz = d_wrap_rel(rz, q->r, G.zl);
+    if(comp == 0) uu[C] = (q->oy * rz - q->oz * ry) + q->u;
+    else if(comp == 1) vv[C] = (q->oz * rx - q->ox * rz) + q->v;
+    else ww[C] = (q->ox * ry - q->oy * rx) + q->w;
+  }
+}
+
+extern "C" void cuda_parts_internal(void)
+{
+  bbb_dev_require();
+  if(!g_dev.ready || nparts <= 0 || g_dev.np != nparts) return;
+  bbb_geom G = bbb_make_geom();
+  dim3 blk(32, 8), grd((G.nx + 1 + 31) / 32, (G.ny + 1 + 7) / 8, G.nz + 1);
+  k_internal<<<grd, blk, 0, g_dev.stream>>>(g_dev.u, g_dev.v, g_dev.w,
+    g_dev.phase, g_dev.flag_u, g_dev.flag_v, g_dev.flag_w, g_dev.parts, G);
+  BBB_LAUNCHED();
+}
+
+/* ------------------------------------------------ quadrature
+ * 26-node degree-7 Lebedev rule (src/cuda_quadrature.cu:86-150): 6 axis
+ * nodes (poles nudged by DIV_ST), 12 edge midpoints, 8 cube vertices;
+ * weights 4 pi {1/21, 4/105, 27/840}. */
+__constant__ double c_node_t[26];
+__constant__ double c_node_p[26];
+static int g_nodes_ready = 0;
+
+static void upload_nodes(void)
+{
+  if(g_nodes_ready) return;
+  double PI14 = 0.25 * PI, PI12 = 0.5 * PI, PI34 = 0.75 * PI,
+         PI54 = 1.25 * PI, PI32 = 1.5 * PI, PI74 = 1.75 * PI;
+  double alph1 = 0.955316618124509, alph2 = 2.186276035465284;
+  double t[26] = {PI12, PI12, PI12, PI12, 0. + DIV_ST, PI - DIV_ST,
+    PI12, PI12, PI12, PI12, PI14, PI14, PI14, PI14, PI34, PI34, PI34, PI34,
+    alph1, alph1, alph1, alph1, alph2, alph2, alph2, alph2};
+  double p[26] = {0., PI12, PI, PI32, 0., 0.,
+    PI14, PI34, PI54, PI74, 0., PI12, PI, PI32, 0., PI12, PI, PI32,
+    PI14, PI34, PI54, PI74, PI14, PI34, PI54, PI74};
+  BBB_CK(cudaMemcpyToSymbol(c_node_t, t, sizeof(t)));
+  BBB_CK(cudaMemcpyToSymbol(c_node_p, p, sizeof(p)));
+  g_nodes_ready = 1;
+}
+
+struct lamb_args {
+  part_struct *parts;
+  const real *p, *u, *v, *w;
+  coef_ptrs cur;
+  double *cf[6];          /* writable current coefficients */
+  const double *cf0[6];   /* previous iterate             */
+  int stride, np;
+  double mu, nu, rho_f, relax, gpx, gpy, gpz;
+  BC bc;
+  bbb_geom G;
+  int s_cc1, s_cc2;
+};
+
+__global__ void __launch_bounds__(32) k_lamb(lamb_args L)
+{
+  const double A1 = 0.598398600683775, A2 = 0.478718880547015,
+               A3 = 0.403919055461543;
+  int part = blockIdx.x;
+  int node = threadIdx.x;
+  __shared__ double s_pp[32], s_ut[32], s_up[32];
+  __shared__ double s_I[6][32];
+  part_struct *q = &L.parts[part];
+  const bbb_geom &G = L.G;
+  const BC &bc = L.bc;
+  if(node < 26) {
+    double th = c_node_t[node], ph_ = c_node_p[node];
+    double xp = q->rs * sin(th) * cos(ph_);
+    double yp = q->rs * sin(th) * sin(ph_);
+    double zp = q->rs * cos(th);
+    double x = xp + q->x, y = yp + q->y, z = zp + q->z;
+    int nd = -1;
+    if(x - G.xs < 0) {
+      if(bc.uW == BBB_DIRICHLET || bc.vW == BBB_DIRICHLET || bc.wW == BBB_DIRICHLET)
+        if(nd == -1) nd = -10;
+    } if(x - G.xe > 0) {
+      if(bc.uE == BBB_DIRICHLET || bc.vE == BBB_DIRICHLET || bc.wE == BBB_DIRICHLET)
+        if(nd == -1) nd = -11;
+    } if(y - G.ys < 0) {
+      if(bc.uS == BBB_DIRICHLET || bc.vS == BBB_DIRICHLET || bc.wS == BBB_DIRICHLET)
+        if(nd == -1) nd = -12;
+    } if(y - G.ye > 0) {
+      if(bc.uN == BBB_DIRICHLET || bc.vN == BBB_DIRICHLET || bc.wN == BBB_DIRICHLET)
+        if(nd == -1) nd = -13;
+    } if(z - G.zs < 0) {
+      if(bc.uB == BBB_DIRICHLET || bc.vB == BBB_DIRICHLET || bc.wB == BBB_DIRICHLET)
+        if(nd == -1) nd = -14;
+    } if(z - G.ze > 0) {
+      if(bc.uT == BBB_DIRICHLET || bc.vT == BBB_DIRICHLET || bc.wT == BBB_DIRICHLET)
+        if(nd == -1) nd = -15;
+    }
+    q->nodes[node] = nd;
+    if(x < G.xs && bc.uW == BBB_PERIODIC) x = x + G.xl;
+    else if(x > G.xe && bc.uE == BBB_PERIODIC) x = x - G.xl;
+    if(y < G.ys && bc.vS == BBB_PERIODIC) y = y + G.yl;
+    else if(y > G.ye && bc.vN == BBB_PERIODIC) y = y - G.yl;
+    if(z < G.zs && bc.wB == BBB_PERIODIC) z = z + G.zl;
+    else if(z > G.ze && bc.wT == BBB_PERIODIC) z = z - G.zl;
+    double ddx = 1. / G.dx, ddy = 1. / G.dy, ddz = 1. / G.dz;
+    int i = (int)floor(__dmul_rn(__dsub_rn(x, G.xs), ddx)) + BBB_DOM_BUF;
+    int j = (int)floor(__dmul_rn(__dsub_rn(y, G.ys), ddy)) + BBB_DOM_BUF;
+    int k = (int)floor(__dmul_rn(__dsub_rn(z, G.zs), ddz)) + BBB_DOM_BUF;
+    i = max(1, min(i, G.nx)); j = max(1, min(j, G.ny)); k = max(1, min(k, G.nz));
+    long long C = i + (long long)j * G.cc_s1 + (long long)k * G.cc_s2;
+    double xx = (i - 0.5) * G.dx + G.xs, yy = (j - 0.5) * G.dy + G.ys,
+           zz = (k - 0.5) * G.dz + G.zs;
+    const real *p = L.p;
+    double dpdx = 0.5 * (p[C + 1] - p[C - 1]) * ddx;
+    double dpdy = 0.5 * (p[C + G.cc_s1] - p[C - G.cc_s1]) * ddy;
+    double dpdz = 0.5 * (p[C + G.cc_s2] - p[C - G.cc_s2]) * ddz;
+    double pv = p[C] + dpdx * (x - xx) + dpdy * (y - yy) + dpdz * (z - zz);
+    double ox = q->ox, oy = q->oy, oz = q->oz;
+    double o2 = (oy * zp - oz * yp) * (oy * zp - oz * yp);
+    o2 += (ox * zp - oz * xp) * (ox * zp - oz * xp);
+    o2 += (ox * yp - oy * xp) * (ox * yp - oy * xp);
+    double acc = (-L.gpx / L.rho_f - q->udot) * xp + (-L.gpy / L.rho_f - q->vdot) * yp
+      + (-L.gpz / L.rho_f - q->wdot) * zp;
+    pv -= 0.5 * L.rho_f * o2 + L.rho_f * acc;
+    pv = (nd == -1) * pv;
+
+    double rs3 = q->rs * q->rs * q->rs, rs5 = rs3 * q->rs * q->rs;
+    double a5 = q->r * q->r * q->r * q->r * q->r;
+    double ocr[3] = {oy * zp - oz * yp, -(ox * zp - oz * xp), ox * yp - oy * xp};
+    double odcr[3] = {q->oydot * zp - q->ozdot * yp, -(q->oxdot * zp - q->ozdot * xp),
+      q->oxdot * yp - q->oydot * xp};
+    double pu[3] = {q->u, q->v, q->w};
+    double wall[3][6] = {{bc.uWD, bc.uED, bc.uSD, bc.uND, bc.uBD, bc.uTD},
+      {bc.vWD, bc.vED, bc.vSD, bc.vND, bc.vBD, bc.vTD},
+      {bc.wWD, bc.wED, bc.wSD, bc.wND, bc.wBD, bc.wTD}};
+    double vel[3];
+    for(int c = 0; c < 3; c++) {
+      const real *f = c == 0 ? L.u : (c == 1 ? L.v : L.w);
+      int s1 = c == 0 ? G.fx_s1 : (c == 1 ? G.fy_s1 : G.fz_s1);
+      int s2 = c == 0 ? G.fx_s2 : (c == 1 ? G.fy_s2 : G.fz_s2);
+      double fxr = __dmul_rn(__dsub_rn(x, G.xs), ddx);
+      double fyr = __dmul_rn(__dsub_rn(y, G.ys), ddy);
+      double fzr = __dmul_rn(__dsub_rn(z, G.zs), ddz);
+      int ii = (int)(c == 0 ? round(fxr) : floor(fxr)) + BBB_DOM_BUF;
+      int jj = (int)(c == 1 ? round(fyr) : floor(fyr)) + BBB_DOM_BUF;
+      int kk = (int)(c == 2 ? round(fzr) : floor(fzr)) + BBB_DOM_BUF;
+      int ihi = G.nx + (c == 0), jhi = G.ny + (c == 1), khi = G.nz + (c == 2);
+      ii = max(1, min(ii, ihi)); jj = max(1, min(jj, jhi)); kk = max(1, min(kk, khi));
+      double fx = c == 0 ? (ii - BBB_DOM_BUF) * G.dx + G.xs : (ii - 0.5) * G.dx + G.xs;
+      double fy = c == 1 ? (jj - BBB_DOM_BUF) * G.dy + G.ys : (jj - 0.5) * G.dy + G.ys;
+      double fz = c == 2 ? (kk - BBB_DOM_BUF) * G.dz + G.zs : (kk - 0.5) * G.dz + G.zs;
+      long long CF = ii + (long long)jj * s1 + (long long)kk * s2;
+      double dfdx = 0.5 * (f[CF + 1] - f[CF - 1]) * ddx;
+      double dfdy = 0.5 * (f[CF + s1] - f[CF - s1]) * ddy;
+      double dfdz = 0.5 * (f[CF + s2] - f[CF - s2]) * ddz;
+      double val = f[CF] + dfdx * (x - fx) + dfdy * (y - fy) + dfdz * (z - fz);
+      double vw = (nd == -10) * wall[c][0] + (nd == -11) * wall[c][1]
+        + (nd == -12) * wall[c][2] + (nd == -13) * wall[c][3]
+        + (nd == -14) * wall[c][4] + (nd == -15) * wall[c][5];
+      val -= pu[c] + ocr[c];
+      val -= 0.1 / L.nu * (rs5 - a5) / rs3 * odcr[c];
+      vw -= pu[c] + ocr[c];
+      vw -= 0.1 / L.nu * (rs5 - a5) / rs3 * odcr[c];
+      vel[c] = (nd == -1) * val + (nd < -1) * vw;
+    }
+    double stt = sin(th), ctt = cos(th), sp = sin(ph_), cp = cos(ph_);
+    s_pp[node] = pv;
+    s_ut[node] = ctt * (vel[0] * cp + vel[1] * sp) - vel[2] * stt;
+    s_up[node] = -vel[0] * sp + vel[1] * cp;
+  }
+  __syncwarp();
+  /* inner products and the coefficient solve, one coefficient at a time */
+  double ars = q->r / q->rs, rsa = q->rs / q->r;
+  int ncoef = q->ncoeff < 15 ? q->ncoeff : 15;
+  const int nn_[15] = {0, 1, 1, 2, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4, 4};
+  const int mm_[15] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3, 0, 1, 2, 3, 4};
+  double mu = L.mu, nu = L.nu, relax = L.relax, r = q->r;
+  for(int coeff = 0; coeff < ncoef; coeff++) {
+    int n = nn_[coeff], m = mm_[coeff];
+    if(node < 26) {
+      double theta = c_node_t[node], phi = c_node_p[node];
+      double N_nm = d_Nnm(n, m);
+      double P_nm = d_Pnm(n, m, theta);
+      double P_n1m = d_Pnm(n + 1, m, theta);
+      double dPdt = (n - m + 1.) * P_n1m - (n + 1.) * cos(theta) * P_nm;
+      double dPdp = m * P_nm;
+      double pv = s_pp[node], tv = s_ut[node], fv = s_up[node];
+      s_I[0][node] = N_nm * P_nm * pv * cos(m * phi);
+      s_I[1][node] = -N_nm * P_nm * pv * sin(m * phi);
+      s_I[2][node] = N_nm / sin(theta) * (dPdt * tv * cos(m * phi) - dPdp * fv * sin(m * phi));
+      s_I[3][node] = N_nm / sin(theta) * (-dPdt * tv * sin(m * phi) - dPdp * fv * cos(m * phi));
+      s_I[4][node] = N_nm / sin(theta) * (dPdp * tv * sin(m * phi) + dPdt * fv * cos(m * phi));
+      s_I[5][node] = N_nm / sin(theta) * (dPdp * tv * cos(m * phi) - dPdt * fv * sin(m * phi));
+    }
+    __syncwarp();
+    if(node < 6) {
+      /* lane a sums integrand a in the reference's serial node order */
+      int a = node;
+      double s = s_I[a][0] * A1;
+      for(int i = 1; i < 6; i++) s += A1 * s_I[a][i];
+      for(int i = 6; i < 18; i++) s += A2 * s_I[a][i];
+      for(int i = 18; i < 26; i++) s += A3 * s_I[a][i];
+      s_I[a][31] = s;
+    }
+    __syncwarp();
+    if(node == 0) {
+      double S[6];
+      for(int a = 0; a < 6; a++) S[a] = s_I[a][31];
+      long long ci = (long long)L.stride * part + coeff;
+      if(n == 0) {
+        L.cf[0][ci] = L.cf0[0][ci] + relax * (r * r / mu / nu * S[0] * pow(ars, (double)n) - L.cf0[0][ci]);
+        L.cf[1][ci] = L.cf0[1][ci] + relax * (r * r / mu / nu * S[1] * pow(ars, (double)n) - L.cf0[1][ci]);
+        L.cf[2][ci] = 0.; L.cf[3][ci] = 0.; L.cf[4][ci] = 0.; L.cf[5][ci] = 0.;
+      } else {
+        double A = (1. - 0.5 * n * (2. * n - 1.) / (n + 1.) * pow(ars, 2. * n + 1.)) * pow(rsa, (double)n);
+        double B = n * (2. * n - 1.) * (2. * n + 1.) / (n + 1.) * pow(ars, n + 1.);
+        double Cc = 0.25 * n * (2. * (n + 3.) / (2. * n + 3.)
+          + (n - 2. - n * (2. * n + 1.) / (2. * n + 3.) * ars * ars) * pow(ars, 2. * n + 1.))
+          * pow(rsa, n + 1.);
+        double D = n * (n + 1. + 0.5 * ((n - 2.) * (2. * n + 1.) * rsa * rsa
+          - n * (2. * n - 1.)) * pow(ars, 2. * n + 1.)) * pow(rsa, n - 1.);
+        double den = A * D + B * Cc;
+        double pre = (r * r / mu / nu * S[0] * D + r / nu * S[2] * B) / den;
+        double pim = (r * r / mu / nu * S[1] * D + r / nu * S[3] * B) / den;
+        double fre = (r / nu * S[2] * A - r * r / mu / nu * S[0] * Cc) / den;
+        double fim = (r / nu * S[3] * A - r * r / mu / nu * S[1] * Cc) / den;
+        double E = n * (n + 1.) * (pow(ars, 2. * n + 1.) - 1.) * pow(rsa, (double)n);
+        double cre = r / nu * S[4] / E;
+        double cim = r / nu * S[5] / E;
+        L.cf[0][ci] = L.cf0[0][ci] * (1. - relax) + relax * pre;
+        L.cf[1][ci] = L.cf0[1][ci] * (1. - relax) + relax * pim;
+        L.cf[2][ci] = L.cf0[2][ci] * (1. - relax) + relax * fre;
+        L.cf[3][ci] = L.cf0[3][ci] * (1. - relax) + relax * fim;
+        L.cf[4][ci] = L.cf0[4][ci] * (1. - relax) + relax * cre;
+        L.cf[5][ci] = L.cf0[5][ci] * (1. - relax) + relax * cim;
+      }
+    }
+    __syncwarp();
+  }
+  if(node == 0) {
+    /* forces and torques, src/quadrature_kernel.cu:545-576 */
+    double vol = 4. / 3. * PI * q->r * q->r * q->r;
+    double N10 = sqrt(3. / 4. / PI), N11 = sqrt(3. / 8. / PI);
+    long long b = (long long)L.stride * part;
+    double *const *cf = L.cf;
+    q->Fx = L.rho_f * vol * (q->udot + L.gpx)
+      - PI * mu * nu * 2. * N11 * (cf[0][b + 2] + 6. * cf[2][b + 2]);
+    q->Fy = L.rho_f * vol * (q->vdot + L.gpy)
+      + PI * mu * nu * 2. * N11 * (cf[1][b + 2] + 6. * cf[3][b + 2]);
+    q->Fz = L.rho_f * vol * (q->wdot + L.gpz)
+      + PI * mu * nu * N10 * (cf[0][b + 1] + 6. * cf[2][b + 1]);
+    q->Lx = L.rho_f * vol * q->r * q->r * q->oxdot
+      - 8. * PI * mu * nu * 2. * N11 * q->r * cf[4][b + 2];
+    q->Ly = L.rho_f * vol * q->r * q->r * q->oydot
+      + 8. * PI * mu * nu * 2. * N11 * q->r * cf[5][b + 2];
+    q->Lz = L.rho_f * vol * q->r * q->r * q->ozdot
+      + 8. * PI * mu * nu * N10 * q->r * cf[4][b + 1];
+  }
+}
+
+/* src/cuda_quadrature.cu:64-313 */
+extern "C" void cuda_Lamb(void)
+{
+  bbb_dev_require();
+  if(!g_dev.ready || nparts <= 0 || g_dev.np != nparts) return;
+  upload_nodes();
+  lamb_args L;
+  L.parts = g_dev.parts;
+  L.p = g_dev.p; L.u = g_dev.u; L.v = g_dev.v; L.w = g_dev.w;
+  L.cur = cur_coefs();
+  for(int a = 0; a < 6; a++) { L.cf[a] = g_dev.coef[a]; L.cf0[a] = g_dev.coef[6 + a]; }
+  L.stride = coeff_stride; L.np = nparts;
+  L.mu = mu; L.nu = nu; L.rho_f = rho_f; L.relax = lamb_relax;
+  L.gpx = gradP.x; L.gpy = gradP.y; L.gpz = gradP.z;
+  L.bc = bc;
+  L.G = bbb_make_geom();
+  k_lamb<<<nparts, 32, 0, g_dev.stream>>>(L);
+  BBB_LAUNCHED();
+}
+
+/* per-particle coefficient change, the computation compute_error
+ * (src/quadrature_kernel.cu:578-654) intends, with a private sort list per
+ * particle; then the device maximum */
+__global__ void k_lamb_err(const double *const *unused, int np, int stride,
+  double lamb_cut, const double *c0, const double *c1, const double *c2,
+  const double *c3, const double *c4, const double *c5, const double *o0,
+  const double *o1, const double *o2, const double *o3, const double *o4,
+  const double *o5, double *partials, unsigned int *ticket, double *out)
+{
+  (void)unused;
+  __shared__ double sh[32];
+  double e = FLT_MIN;
+  for(int part = blockIdx.x * blockDim.x + threadIdx.x; part < np;
+      part += gridDim.x * blockDim.x) {
+    const double *cs[6] = {c0, c1, c2, c3, c4, c5};
+    const double *os[6] = {o0, o1, o2, o3, o4, o5};
+    double big = -1.;
+    for(int a = 0; a < 6; a++) for(int i = 0; i < stride; i++) {
+      double c = cs[a][(long long)part * stride + i];
+      if(c * c > FLT_MIN && fabs(c) > big) big = fabs(c);
+    }
+    double pe = FLT_MIN;
+    if(big >= 0.) {
+      for(int a = 0; a < 6; a++) for(int i = 0; i < stride; i++) {
+        double c = cs[a][(long long)part * stride + i];
+        if(!(c * c > FLT_MIN)) continue;
+        if(fabs(c) > lamb_cut * big) {
+          double div = fabs(c);
+          if(div < 1e-16) div = 1e-16;
+          double er = fabs((c - os[a][(long long)part * stride + i]) / div);
+          if(er > pe) pe = er;
+        }
+      }
+    }
+    if(pe > e) e = pe;
+  }
+  double v[1] = {e};
+  bbb_block_max<1>(v, sh);
+  __shared__ unsigned int s_last;
+  if(threadIdx.x == 0) {
+    partials[blockIdx.x] = v[0];
+    __threadfence();
+    unsigned int t = atomicAdd(ticket, 1u);
+    s_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if(!s_last) return;
+  __threadfence();
+  double m[1] = {FLT_MIN};
+  for(int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+    m[0] = fmax(m[0], ((volatile double *)partials)[b]);
+  bbb_block_max<1>(m, sh);
+  if(threadIdx.x == 0) { *out = m[0]; *ticket = 0u; }
+}
+
+/* src/cuda_quadrature.cu:316-398 */
+extern "C" real cuda_lamb_err(void)
+{
+  bbb_dev_require();
+  if(!g_dev.ready || nparts <= 0 || g_dev.np != nparts) return 0.;
+  int blocks = (nparts + 255) / 256;
+  if(blocks > 1184) blocks = 1184;
+  double **c = g_dev.coef;
+  k_lamb_err<<<blocks, 256, 0, g_dev.stream>>>(NULL, nparts, coeff_stride,
+    lamb_cut, c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8], c[9],
+    c[10], c[11], g_dev.partials, g_dev.red_ticket + 8, g_dev.red_dev + 32);
+  BBB_LAUNCHED();
+  size_t n = sizeof(real) * (size_t)coeff_stride * nparts;
+  for(int a = 0; a < 6; a++)
+    BBB_CK(cudaMemcpyAsync(g_dev.coef[6 + a], g_dev.coef[a], n,
+      cudaMemcpyDeviceToDevice, g_dev.stream));
+  BBB_CK(cudaMemcpyAsync(g_dev.red_host, g_dev.red_dev + 32, sizeof(double),
+    cudaMemcpyDeviceToHost, g_dev.stream));
+  BBB_CK(cudaStreamSynchronize(g_dev.stream));
+  return g_dev.red_host[0];
+}
+
+/* src/cuda_particle.cu:1046-1081 */
+extern "C" void cuda_store_coeffs(void)
+{
+  bbb_dev_require();
+  if(!g_dev.ready || nparts <= 0 || g_dev.np != nparts) return;
+  size_t n = sizeof(real) * (size_t)coeff_stride * nparts;
+  for(int a = 0; a < 6; a++)
+    BBB_CK(cudaMemcpyAsync(g_dev.coef[12 + a], g_dev.coef[a], n,
+      cudaMemcpyDeviceToDevice, g_dev.stream));
+}
+
+/* ------------------------------------------------ Newton-Euler
+ * collision_init (src/bluebottle_kernel.cu:2400), spring_parts (:3592),
+ * move_parts_a/b and rotate (:2247-2398).  Lubrication and contact forces
+ * (collision_parts, collision_walls) are not part of this build; the
+ * interaction force and torque are zero. */
+__device__ void d_rotate(double qr, double qi, double qj, double qk,
+  double *pi, double *pj, double *pk)
+{
+  double Pr = *pi * qi + *pj * qj + *pk * qk;
+  double Pi = *pi * qr - *pj * qk + *pk * qj;
+  double Pj = *pi * qk + *pj * qr - *pk * qi;
+  double Pk = -*pi * qj + *pj * qi + *pk * qr;
+  *pi = qr * Pi + qi * Pr + qj * Pk - qk * Pj;
+  *pj = qr * Pj - qi * Pk + qj * Pr + qk * Pi;
+  *pk = qr * Pk + qi * Pj - qj * Pi + qk * Pr;
+}
+
+__device__ void d_springs(part_struct *q)
+{
+  q->iFx = 0.; q->iFy = 0.; q->iFz = 0.;
+  q->iLx = 0.; q->iLy = 0.; q->iLz = 0.;
+  if(q->spring_k > 0.) {
+    double nx = q->x - q->spring_x, ny = q->y - q->spring_y, nz = q->z - q->spring_z;
+    double n = sqrt(nx * nx + ny * ny + nz * nz);
+    double lx = q->spring_l * (nx / n), ly = q->spring_l * (ny / n),
+           lz = q->spring_l * (nz / n);
+    q->kFx = -q->spring_k * (q->x - q->spring_x - lx);
+    q->kFy = -q->spring_k * (q->y - q->spring_y - ly);
+    q->kFz = -q->spring_k * (q->z - q->spring_z - lz);
+  }
+}
+
+__device__ void d_move(part_struct *q, int final, double dt, double rho_f,
+  g_struct g, gradP_struct gp, bbb_geom G)
+{
+  double vol = 4. / 3. * PI * q->r * q->r * q->r;
+  double m = vol * q->rho;
+  if(q->translating) {
+    q->udot = (q->Fx + q->kFx + q->iFx + q->aFx - vol * gp.x) / m
+      + (q->rho - rho_f) / q->rho * g.x;
+    q->vdot = (q->Fy + q->kFy + q->iFy + q->aFy - vol * gp.y) / m
+      + (q->rho - rho_f) / q->rho * g.y;
+    q->wdot = (q->Fz + q->kFz + q->iFz + q->aFz - vol * gp.z) / m
+      + (q->rho - rho_f) / q->rho * g.z;
+    q->u = q->u0 + 0.5 * dt * (q->udot + q->udot0);
+    q->v = q->v0 + 0.5 * dt * (q->vdot + q->vdot0);
+    q->w = q->w0 + 0.5 * dt * (q->wdot + q->wdot0);
+    if(final) {
+      q->x = q->x0 + 0.5 * dt * (q->u + q->u0);
+      if(q->x < G.xs) q->x = q->x + G.xl;
+      else if(q->x > G.xe) q->x = q->x - G.xl;
+      q->y = q->y0 + 0.5 * dt * (q->v + q->v0);
+      if(q->y < G.ys) q->y = q->y + G.yl;
+      else if(q->y > G.ye) q->y = q->y - G.yl;
+      q->z = q->z0 + 0.5 * dt * (q->w + q->w0);
+      if(q->z < G.zs) q->z = q->z + G.zl;
+      else if(q->z > G.ze) q->z = q->z - G.zl;
+      q->x0 = q->x; q->y0 = q->y; q->z0 = q->z;
+      q->u0 = q->u; q->v0 = q->v; q->w0 = q->w;
+      q->udot0 = q->udot; q->vdot0 = q->vdot; q->wdot0 = q->wdot;
+    }
+  }
+  if(q->rotating) {
+    double I = 0.4 * m * q->r * q->r;
+    q->oxdot = (q->Lx + q->iLx + q->aLx) / I;
+    q->oydot = (q->Ly + q->iLy + q->aLy) / I;
+    q->ozdot = (q->Lz + q->iLz + q->aLz) / I;
+    q->ox = q->ox0 + 0.5 * dt * (q->oxdot + q->oxdot0);
+    q->oy = q->oy0 + 0.5 * dt * (q->oydot + q->oydot0);
+    q->oz = q->oz0 + 0.5 * dt * (q->ozdot + q->ozdot0);
+    if(final) {
+      double mag = 0.5 * sqrt(q->ox * q->ox + q->oy * q->oy + q->oz * q->oz);
+      mag += 0.5 * sqrt(q->ox0 * q->ox0 + q->oy0 * q->oy0 + q->oz0 * q->oz0);
+      double X = 0, Y = 0, Z = 0;
+      if(mag > 0) {
+        X = 0.5 * (q->ox + q->ox0) / mag;
+        Y = 0.5 * (q->oy + q->oy0) / mag;
+        Z = 0.5 * (q->oz + q->oz0) / mag;
+      }
+      double th = mag * dt;
+      double qr = cos(0.5 * th), qi = X * sin(0.5 * th), qj = Y * sin(0.5 * th),
+             qk = Z * sin(0.5 * th);
+      d_rotate(qr, qi, qj, qk, &q->axx, &q->axy, &q->axz);
+      d_rotate(qr, qi, qj, qk, &q->ayx, &q->ayy, &q->ayz);
+      d_rotate(qr, qi, qj, qk, &q->azx, &q->azy, &q->azz);
+      q->ox0 = q->ox; q->oy0 = q->oy; q->oz0 = q->oz;
+      q->oxdot0 = q->oxdot; q->oydot0 = q->oydot; q->ozdot0 = q->ozdot;
+    }
+  }
+}
+
+__global__ void k_move_parts(part_struct *parts, int np, int final, double dt,
+  double rho_f, g_struct g, gradP_struct gp, bbb_geom G)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= np) return;
+  part_struct *q = &parts[i];
+  d_springs(q);
+  d_move(q, 0, dt, rho_f, g, gp, G);
+  d_springs(q);
+  if(final) d_move(q, 1, dt, rho_f, g, gp, G);
+}
+
+/* src/cuda_bluebottle.cu:4317-4433 */
+extern "C" void cuda_move_parts_sub(void)
+{
+  bbb_dev_require();
+  if(!g_dev.ready || nparts <= 0 || g_dev.np != nparts) return;
+  k_move_parts<<<(nparts + 127) / 128, 128, 0, g_dev.stream>>>(g_dev.parts,
+    nparts, 0, dt, rho_f, g, gradP, bbb_make_geom());
+  BBB_LAUNCHED();
+}
+
+/* src/cuda_bluebottle.cu:4435-4554 */
+extern "C" void cuda_move_parts(void)
+{
+  bbb_dev_require();
+  if(!g_dev.ready || nparts <= 0 || g_dev.np != nparts) return;
+  k_move_parts<<<(nparts + 127) / 128, 128, 0, g_dev.stream>>>(g_dev.parts,
+    nparts, 1, dt, rho_f, g, gradP, bbb_make_geom());
+  BBB_LAUNCHED();
+}

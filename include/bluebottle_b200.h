@@ -1,0 +1,237 @@
+/* bluebottle_b200.h -- C ABI of libbbb200.so.
+ *
+ * Part 1 is the drop-in boundary: the extern "C" GPU entry points that
+ * bluebottle's time loop (src/bluebottle.c:415-450 init, 528-543 pre-loop,
+ * 603-708 step) calls.  They take no arguments (or the reference's
+ * arguments) and work on the reference's global state, declared in part 2,
+ * exactly like the reference's src/cuda_*.cu implementations.  Each comment
+ * names the reference prototype it replaces.
+ *
+ * Part 3 is this library's own extension API: host-side set-up (config files
+ * in the reference's format), build-side options that the reference lacks
+ * (fixed dt, Taylor-Green start, seeded particle packs, precision mode,
+ * learned initial guess), a whole-step driver and solver statistics.
+ *
+ * Error convention: the reference exits the process when a Krylov solve fails
+ * to converge (src/cuda_bicgstab.cu:293-296, 1029-1032).  Here every entry
+ * point records a status instead; bbb_last_status() returns it, and the
+ * process exits only if bbb_set_exit_on_failure(1) was called (the default
+ * matches the reference: 1).
+ */
+#ifndef BLUEBOTTLE_B200_H
+#define BLUEBOTTLE_B200_H
+
+#include "bluebottle_b200_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ===== Part 1: drop-in GPU entry points ================================ */
+
+/* lifecycle -- src/bluebottle.h:2373-2484, src/particle.h:1097-1149 */
+void cuda_dom_malloc(void);            /* src/cuda_bluebottle.cu:36   */
+void cuda_part_malloc(void);           /* src/cuda_particle.cu:28     */
+void cuda_dom_push(void);              /* src/cuda_bluebottle.cu:299  */
+void cuda_part_push(void);             /* src/cuda_particle.cu:170    */
+void cuda_dom_pull(void);              /* src/cuda_bluebottle.cu:794  */
+void cuda_part_pull(void);             /* src/cuda_particle.cu:234    */
+void cuda_dom_free(void);              /* src/cuda_bluebottle.cu:1441 */
+void cuda_part_free(void);             /* src/cuda_particle.cu        */
+
+/* per-step -- src/bluebottle.h:2492-2943, src/cuda_bicgstab.h:55-141 */
+void cuda_compute_forcing(real *pid_int, real *pid_back, real Kp, real Ki,
+  real Kd);                            /* src/cuda_bluebottle.cu:3674 */
+void cuda_build_cages(void);           /* src/cuda_particle.cu:357    */
+void cuda_U_star_2(void);              /* src/cuda_bluebottle.cu:2930 */
+void cuda_ustar_helmholtz(int rank);   /* src/cuda_bicgstab.cu:44     */
+void cuda_vstar_helmholtz(int rank);   /* src/cuda_bicgstab.cu:319    */
+void cuda_wstar_helmholtz(int rank);   /* src/cuda_bicgstab.cu:517    */
+void cuda_ustar_rhs(int dev);          /* src/cuda_bicgstab.cu:1091   */
+void cuda_vstar_rhs(int dev);          /* src/cuda_bicgstab.cu:1119   */
+void cuda_wstar_rhs(int dev);          /* src/cuda_bicgstab.cu:1147   */
+void cuda_PP_rhs(int dev);             /* src/cuda_bicgstab.cu:1178   */
+void cuda_part_BC(void);               /* src/cuda_particle.cu:899    */
+void cuda_part_BC_star(void);          /* src/cuda_particle.cu:947    */
+void cuda_part_BC_p(int dev);          /* src/cuda_particle.cu:996    */
+void cuda_part_p_fill(void);           /* src/cuda_particle.cu:1019   */
+void cuda_dom_BC(void);                /* src/cuda_bluebottle.cu:1549 */
+void cuda_dom_BC_star(void);           /* src/cuda_bluebottle.cu:2302 */
+void cuda_dom_BC_phi(void);            /* src/cuda_bluebottle.cu:3030 */
+void cuda_dom_BC_p(void);              /* src/cuda_bluebottle.cu:3226 */
+void cuda_solvability(void);           /* src/cuda_bluebottle.cu:4122 */
+void cuda_PP_bicgstab(int rank);       /* src/cuda_bicgstab.cu:715    */
+void cuda_project(void);               /* src/cuda_bluebottle.cu:3422 */
+void cuda_update_p(void);              /* src/cuda_bluebottle.cu:3616 */
+void cuda_move_parts_sub(void);        /* src/cuda_bluebottle.cu:4317 */
+void cuda_move_parts(void);            /* src/cuda_bluebottle.cu:4435 */
+void cuda_Lamb(void);                  /* src/cuda_quadrature.cu:64   */
+real cuda_lamb_err(void);              /* src/cuda_quadrature.cu:316  */
+void cuda_parts_internal(void);        /* src/cuda_bluebottle.cu:4822 */
+void cuda_store_u(void);               /* src/cuda_bluebottle.cu:3580 */
+void cuda_store_coeffs(void);          /* src/cuda_particle.cu:1046   */
+real cuda_find_dt(void);               /* src/cuda_bluebottle.cu:3500 */
+real cuda_compute_energy(void);        /* src/cuda_bluebottle.cu:3944 */
+void cuda_div_U(void);                 /* src/bluebottle.h:2717       */
+
+/* precursor-only symbols that bluebottle.c references; the two-rank
+ * turbulence precursor is out of scope, so these are link stubs that record
+ * BBB_ERR_UNSUPPORTED -- src/bluebottle.h:2411, 2447, 2877, 2926 */
+void cuda_dom_turb_planes_push(int *bc_configs);
+void cuda_dom_turb_planes_pull(int *bc_configs);
+void cuda_compute_turb_forcing(void);
+void cuda_yank_turb_planes(int *bc_flow_configs, real *bc_plane_pos,
+  real *vel);
+
+/* ===== Part 2: the reference's global state ============================ */
+/* Defined (weakly) inside libbbb200.so; when linked under the reference's
+ * bluebottle.c, that file's definitions take precedence.  Names and types
+ * follow src/bluebottle.h:364-3329 and src/particle.h. */
+extern int dev_start, dev_end, nsubdom;
+extern dom_struct *dom;
+extern dom_struct Dom;
+extern real *p0, *p, *phi;
+extern real *u, *u0, *v, *v0, *w, *w0;
+extern real *f_x, *f_y, *f_z;
+extern real *diff0_u, *diff0_v, *diff0_w;
+extern real *conv0_u, *conv0_v, *conv0_w;
+extern real *diff_u, *diff_v, *diff_w;
+extern real *conv_u, *conv_v, *conv_w;
+extern real *u_star, *v_star, *w_star;
+extern real duration, ttime, vel_tDelay, p_tDelay, g_tDelay;
+extern real dt, dt0, CFL;
+extern int pp_max_iter;
+extern real pp_residual;
+extern int lamb_max_iter;
+extern real lamb_residual, lamb_relax, lamb_cut;
+extern int out_plane, stepnum, init_cond;
+extern g_struct g;
+extern real rho_f, mu, nu;
+extern BC bc;
+extern gradP_struct gradP;
+extern long int cpumem, gpumem;
+extern real pid_int, pid_back, Kp, Ki, Kd;
+extern int *phase, *phase_shell, *flag_u, *flag_v, *flag_w;
+extern int nparts;
+extern real interactionLengthRatio;
+extern dom_struct binDom;
+extern part_struct *parts;
+extern int coeff_stride;
+extern real *pnm_re, *pnm_im, *phinm_re, *phinm_im, *chinm_re, *chinm_im;
+extern real *pnm_re0, *pnm_im0, *phinm_re0, *phinm_im0, *chinm_re0,
+  *chinm_im0;
+extern real *pnm_re00, *pnm_im00, *phinm_re00, *phinm_im00, *chinm_re00,
+  *chinm_im00;
+
+/* ===== Part 3: extension API =========================================== */
+
+/* status codes */
+#define BBB_OK 0
+#define BBB_ERR_CUDA 1            /* a CUDA call failed                    */
+#define BBB_ERR_NOT_CONVERGED 2   /* Krylov solve hit its iteration cap    */
+#define BBB_ERR_CONFIG 3          /* bad or missing input file             */
+#define BBB_ERR_UNSUPPORTED 4     /* feature outside this library's scope  */
+#define BBB_ERR_STATE 5           /* called in the wrong order             */
+#define BBB_ERR_DIVERGED 6        /* dt left [1e-10, 1e10] (bluebottle.c:801) */
+#define BBB_ERR_TOO_LARGE 7       /* request exceeds a stated size limit   */
+#define BBB_ERR_NONFINITE 8       /* NaN/Inf met in a solver residual      */
+
+/* precision forms of the Krylov solves */
+#define BBB_PREC_FP64 0           /* plain FP64 BiCGSTAB / CG              */
+#define BBB_PREC_MIXED 1          /* FP32 inner solves inside FP64 defect
+                                     correction (FP64 outer residual,
+                                     dots, norms and accumulation)        */
+
+/* Build-side options.  The reference compiles some of these in (IMPLICIT)
+ * and lacks the rest; they live here so the reference's input files stay
+ * readable by the reference's own parser. */
+typedef struct bbb_options {
+  int implicit;            /* 1: Crank-Nicolson + Helmholtz CG (-DIMPLICIT);
+                              0: explicit AB2 (cuda_U_star_2)              */
+  real fixed_dt;           /* >0: use this dt every step instead of CFL    */
+  int precision;           /* BBB_PREC_FP64 or BBB_PREC_MIXED              */
+  real inner_tol;          /* mixed form: relative tolerance of each FP32
+                              inner solve                                  */
+  int max_outer;           /* mixed form: defect-correction sweep cap      */
+  int learned_guess;       /* 1: conv-net initial guess for the Poisson
+                              solve (requires bbb_learned_load)            */
+  int record;              /* 1: append solver_expd.rec like the reference */
+  int gravity_balance;     /* 1: set gradP.z so the box's net weight is 0  */
+  int lamb_max_iter_override; /* >0: replaces lamb_max_iter               */
+  int verbose;
+} bbb_options;
+
+void bbb_default_options(bbb_options *opt);
+void bbb_set_options(const bbb_options *opt);
+void bbb_get_options(bbb_options *opt);
+
+/* Host set-up in the reference's input format (restates domain_read_input
+ * src/domain.c:30, parts_read_input src/particle.c:79, domain_init
+ * src/domain.c:1591, parts_init src/particle.c:295). `dir` holds
+ * flow.config and part.config. Return BBB_OK or BBB_ERR_CONFIG. */
+int bbb_read_input(const char *dir);
+int bbb_domain_init(void);
+int bbb_parts_init(void);
+/* Replace the particle list by a seeded random pack: n spheres of radius a
+ * at uniform non-overlapping centres with surface gap >= min_gap*a
+ * (periodic images included), density rho, Lamb order `order`, rs/r = rsr.
+ * Returns BBB_OK or BBB_ERR_CONFIG when the pack cannot be placed. */
+int bbb_seed_particles(int n, real a, real min_gap, real rho, int order,
+  real rsr, unsigned long long seed);
+/* 3-D Taylor-Green start: u = U sin x cos y cos z, v = -U cos x sin y cos z,
+ * w = 0 on the staggered faces (domain assumed [0, 2pi)^3 scaled). */
+void bbb_init_taylor_green(real U);
+void bbb_host_free(void);
+
+/* Device set-up after the host initialisation, in the order of
+ * src/bluebottle.c:415-543: cuda_dom_malloc, cuda_part_malloc, the pushes,
+ * cuda_build_cages, cuda_part_pull, the initial cuda_find_dt (replaced by
+ * the fixed dt when one is set), particle and domain boundary conditions
+ * and the rigid-body fill.  bbb_release frees the device state. */
+int bbb_prepare(void);
+void bbb_release(void);
+/* directory that receives solver_expd.rec when options.record is set */
+void bbb_set_record_dir(const char *dir);
+
+/* one whole time step of src/bluebottle.c:603-708 (compute_forcing,
+ * vel BC ramps, cage build, Lamb sub-iterations, particle update, history
+ * store, next dt).  Returns BBB_OK or an error code. */
+int bbb_step(void);
+/* ttime/dt/stepnum bookkeeping before the step, as bluebottle.c:603-609 */
+void bbb_advance_clock(void);
+
+/* solver statistics of the most recent step */
+typedef struct bbb_stats {
+  int pp_solves;           /* Poisson solves in the step (Lamb iterations) */
+  int pp_iters_total;      /* BiCGSTAB iterations summed over those solves */
+  int pp_iters_last;       /* iterations of the latest solve               */
+  real pp_resid_last;      /* final residual (normalised) of latest solve  */
+  int pp_outer_last;       /* defect-correction sweeps of latest solve     */
+  int helm_iters_total;    /* CG iterations summed over Helmholtz solves   */
+  int lamb_iters;          /* Lamb sub-iterations in the step              */
+  real lamb_err;           /* final Lamb coefficient error                 */
+  int guess_used;          /* learned guess accepted (1) / rejected (0)    */
+  real guess_r0;           /* initial residual norm from the chosen guess  */
+  real extrap_r0;          /* initial residual norm of the extrapolation   */
+} bbb_stats;
+void bbb_get_stats(bbb_stats *st);
+
+int bbb_last_status(void);
+const char *bbb_status_string(int status);
+void bbb_clear_status(void);
+void bbb_set_exit_on_failure(int on);
+
+/* device diagnostics */
+int bbb_device_count(void);
+/* divergence of (u, v, w) over the interior cells: max |div| and the
+ * L2 norm; computed on the device from the current fields */
+void bbb_divergence(real *max_abs, real *l2);
+
+/* kernel launch counter (this library's kernels only), for benchmarks */
+long long bbb_kernel_launches(void);
+void bbb_reset_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
