@@ -122,7 +122,9 @@ bbb_read_input bbb_domain_init bbb_parts_init bbb_seed_particles
 bbb_init_taylor_green bbb_host_free bbb_prepare bbb_release
 bbb_set_record_dir bbb_step bbb_advance_clock bbb_get_stats bbb_last_status
 bbb_status_string bbb_clear_status bbb_set_exit_on_failure bbb_device_count
-bbb_divergence bbb_kernel_launches bbb_reset_kernel_launches""".split()
+bbb_divergence bbb_kernel_launches bbb_reset_kernel_launches
+bbb_profile_enable bbb_profile_reset bbb_profile_get bbb_part_state_push
+bbb_part_state_pull bbb_mark bbb_mark_elapsed""".split()
 
 _lib = None
 
@@ -159,6 +161,12 @@ def load():
     lib.bbb_get_stats.argtypes = [C.POINTER(Stats)]
     lib.bbb_divergence.argtypes = [C.POINTER(R), C.POINTER(R)]
     lib.cuda_compute_forcing.argtypes = [C.POINTER(R), C.POINTER(R), R, R, R]
+    lib.bbb_profile_enable.argtypes = [C.c_int]
+    lib.bbb_mark.argtypes = [C.c_int]
+    lib.bbb_mark_elapsed.argtypes = [C.c_int, C.c_int]
+    lib.bbb_mark_elapsed.restype = R
+    lib.bbb_profile_get.argtypes = [C.POINTER(R), C.POINTER(C.c_longlong),
+                                    C.POINTER(R)]
     for name in ("cuda_ustar_helmholtz", "cuda_vstar_helmholtz",
                  "cuda_wstar_helmholtz", "cuda_PP_bicgstab", "cuda_PP_rhs",
                  "cuda_part_BC_p", "cuda_ustar_rhs", "cuda_vstar_rhs",

@@ -230,6 +230,53 @@ extern "C" void cuda_part_pull(void)
   BBB_CK(cudaStreamSynchronize(g_dev.stream));
 }
 
+/* the host particle array is page-locked on first use so that the
+ * per-step exchange runs as a DMA from pinned memory */
+static part_struct *g_pinned_parts = NULL;
+static void pin_parts(void)
+{
+  if(nparts <= 0 || parts == g_pinned_parts) return;
+  if(g_pinned_parts) cudaHostUnregister(g_pinned_parts);
+  g_pinned_parts = NULL;
+  if(cudaHostRegister(parts, sizeof(part_struct) * nparts, cudaHostRegisterDefault)
+    == cudaSuccess) g_pinned_parts = parts;
+  else cudaGetLastError();
+}
+
+extern "C" void bbb_part_state_push(void)
+{
+  bbb_dev_require();
+  pin_parts();
+  if(nparts > 0 && g_dev.np == nparts)
+    h2d(g_dev.parts, parts, sizeof(part_struct) * nparts);
+}
+
+/* device-side time marks on the library stream */
+static cudaEvent_t g_marks[8];
+extern "C" void bbb_mark(int i)
+{
+  if(i < 0 || i >= 8) return;
+  if(!g_marks[i]) BBB_CK(cudaEventCreate(&g_marks[i]));
+  BBB_CK(cudaEventRecord(g_marks[i], g_dev.stream));
+}
+
+extern "C" double bbb_mark_elapsed(int a, int b)
+{
+  if(a < 0 || a >= 8 || b < 0 || b >= 8 || !g_marks[a] || !g_marks[b]) return -1.;
+  BBB_CK(cudaEventSynchronize(g_marks[b]));
+  float ms = 0.f;
+  if(cudaEventElapsedTime(&ms, g_marks[a], g_marks[b]) != cudaSuccess) return -1.;
+  return ms;
+}
+
+extern "C" void bbb_part_state_pull(void)
+{
+  bbb_dev_require();
+  if(nparts > 0 && g_dev.np == nparts)
+    d2h(parts, g_dev.parts, sizeof(part_struct) * nparts);
+  BBB_CK(cudaStreamSynchronize(g_dev.stream));
+}
+
 extern "C" void cuda_dom_free(void)
 {
   if(!g_dev.ready) return;
@@ -250,7 +297,8 @@ extern "C" void cuda_dom_free(void)
   float **fs[] = {&g_dev.fb, &g_dev.fx, &g_dev.fr, &g_dev.frh, &g_dev.fp[0],
     &g_dev.fp[1], &g_dev.fv[0], &g_dev.fv[1], &g_dev.fs, &g_dev.ft};
   for(size_t a = 0; a < sizeof(fs) / sizeof(fs[0]); a++) dfree(*fs[a]);
-  dfree(g_dev.kry); dfree(g_dev.red_ticket);
+  dfree(g_dev.kry); dfree(g_dev.kry_inner); dfree(g_dev.red_ticket);
+  if(g_pinned_parts) { cudaHostUnregister(g_pinned_parts); g_pinned_parts = NULL; }
   if(g_dev.kry_host) cudaFreeHost(g_dev.kry_host);
   if(g_dev.red_host) cudaFreeHost(g_dev.red_host);
   g_dev.kry_host = NULL; g_dev.red_host = NULL;

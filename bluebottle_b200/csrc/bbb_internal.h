@@ -79,6 +79,7 @@ struct bbb_dev {
   double *partials;                /* per-block reduction partials       */
   int max_blocks;
   bbb_kry *kry;                    /* device scalars                     */
+  bbb_kry *kry_inner;              /* scalars of the FP32 inner solve    */
   bbb_kry *kry_host;               /* pinned mirror                      */
   /* particles */
   int np, stride;
@@ -127,6 +128,7 @@ void bbb_record_solver(const char *name, int niter, real resid);
 void bbb_dev_require(void);
 void bbb_build_masks(void);
 int bbb_poisson_solve(int record);
+int bbb_poisson_solve_mixed(int record);
 int bbb_helmholtz_solve(int comp);
 void bbb_part_BC_fields(real *uu, real *vv, real *ww);
 void bbb_star_rhs(int comp_mask, int explicit_ab2);

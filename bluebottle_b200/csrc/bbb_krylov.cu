@@ -530,6 +530,64 @@ __global__ void k_pp_writeback(const double *x, real *ph, bbb_geom G,
   }
 }
 
+/* ------------------------------------------------ live iteration timing
+ * CUDA events on the solver stream bracket each BiCGSTAB iteration (K1 to
+ * K3) while enabled; after a solve only the iterations the device really
+ * executed are summed, with their algorithmic bytes. */
+#define BBB_PROF_EV 8192
+static struct {
+  int on, n;
+  cudaEvent_t ev[2 * BBB_PROF_EV];
+  double bytes[BBB_PROF_EV];
+  double ms, tot_bytes;
+  long long iters;
+} g_prof;
+
+static void prof_begin(double bytes)
+{
+  if(!g_prof.on || g_prof.n >= BBB_PROF_EV) return;
+  int i = g_prof.n;
+  if(!g_prof.ev[2 * i]) {
+    cudaEventCreate(&g_prof.ev[2 * i]);
+    cudaEventCreate(&g_prof.ev[2 * i + 1]);
+  }
+  g_prof.bytes[i] = bytes;
+  cudaEventRecord(g_prof.ev[2 * i], g_dev.stream);
+}
+
+static void prof_end(void)
+{
+  if(!g_prof.on || g_prof.n >= BBB_PROF_EV) return;
+  cudaEventRecord(g_prof.ev[2 * g_prof.n + 1], g_dev.stream);
+  g_prof.n++;
+}
+
+/* the stream has been synchronised; `executed` iterations really ran */
+static void prof_collect(int executed)
+{
+  if(!g_prof.on) return;
+  int m = executed < g_prof.n ? executed : g_prof.n;
+  for(int i = 0; i < m; i++) {
+    float t = 0.f;
+    if(cudaEventElapsedTime(&t, g_prof.ev[2 * i], g_prof.ev[2 * i + 1]) == cudaSuccess) {
+      g_prof.ms += t;
+      g_prof.tot_bytes += g_prof.bytes[i];
+      g_prof.iters++;
+    }
+  }
+  g_prof.n = 0;
+}
+
+extern "C" void bbb_profile_enable(int on) { g_prof.on = on; g_prof.n = 0; }
+extern "C" void bbb_profile_reset(void)
+{
+  g_prof.ms = 0.; g_prof.tot_bytes = 0.; g_prof.iters = 0; g_prof.n = 0;
+}
+extern "C" void bbb_profile_get(double *ms, long long *iters, double *bytes)
+{
+  *ms = g_prof.ms; *iters = g_prof.iters; *bytes = g_prof.tot_bytes;
+}
+
 /* run iterations until the device says done; host polls in growing
  * batches so that a converged solve costs at most a few no-op launches */
 template <typename LaunchIter>
@@ -572,8 +630,10 @@ int bbb_poisson_solve(int record)
     pp_residual, pp_max_iter);
   BBB_LAUNCHED();
   int cur = 0;
+  double it_bytes = (double)n * (17. * sizeof(double) + 3.);
   int it = drive([&](int q) {
     (void)q;
+    prof_begin(it_bytes);
     k_bicg1<double><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
       g_dev.kr, g_dev.kp[cur], g_dev.kv[cur], g_dev.krh, g_dev.kp[cur ^ 1],
       g_dev.kv[cur ^ 1], s, g_dev.partials);
@@ -585,8 +645,10 @@ int bbb_poisson_solve(int record)
       g_dev.kx, g_dev.kp[cur ^ 1], g_dev.ks, g_dev.kt, g_dev.kr, g_dev.krh,
       s, g_dev.partials);
     BBB_LAUNCHED();
+    prof_end();
     cur ^= 1;
   }, pp_max_iter);
+  prof_collect(g_dev.kry_host->iter + (g_dev.kry_host->s_conv ? 1 : 0));
   k_pp_writeback<<<1184, 256, 0, g_dev.stream>>>(g_dev.kx, g_dev.phi, G, s);
   BBB_LAUNCHED();
   BBB_CK(cudaMemcpyAsync(g_dev.kry_host, s, sizeof(bbb_kry),
@@ -611,11 +673,236 @@ int bbb_poisson_solve(int record)
   return it;
 }
 
+/* ------------------------------------------------ mixed precision
+ * Defect correction: the FP64 outer loop forms r = b - A x in FP64 (with
+ * ||r||, the stopping test of the FP64 form, and sum x for the mean),
+ * hands r to an FP32 Jacobi-BiCGSTAB that solves A e = r from e = 0 to
+ * `inner_tol` relative, and accumulates x += e in FP64.  Stops when the
+ * FP64 residual meets pp_residual * ||b||, the same test as the FP64 form.
+ * Without particle rows the periodic/Neumann operator is singular; the
+ * inner right-hand side is then projected onto zero mean. */
+
+template <typename T>
+struct epi_res64 {
+  const double *b; float *rf;
+  __device__ __forceinline__ void at(long long c, double xr, double Ax, double (&red)[3]) const
+  {
+    double rv = b[c] - Ax;
+    rf[c] = (float)rv;
+    red[0] += rv * rv;
+    red[1] += xr;
+    red[2] += rv;
+  }
+};
+
+/* outer residual; finaliser decides convergence and the inner tolerance */
+__global__ void __launch_bounds__(NTHR) k_outer_resid(boxc B, opc O,
+  const uint8_t *__restrict__ mask, const double *__restrict__ b,
+  const double *x, float *rf, bbb_kry *s, bbb_kry *si, double *partials,
+  double inner_tol, int inner_maxit, int project_mean, long long n)
+{
+  __shared__ double sh[32 * 3];
+  prod_x<double> P{x};
+  epi_res64<double> E{b, rf};
+  double red[3] = {0., 0., 0.};
+  tile_stencil<double>(B, O, mask, P, E, red);
+  if(bbb_grid_partial<3>(red, partials, &s->ticket, sh)) {
+    bbb_grid_finish_sum<3>(red, partials, &s->ticket, sh);
+    if(threadIdx.x == 0 && threadIdx.y == 0) {
+      double rn = sqrt(red[0]);
+      s->rnorm = rn;
+      s->sumx = red[1];
+      s->converged = (rn <= s->tol);
+      s->s_conv = 0;
+      if(!isfinite(rn)) { s->status = BBB_ERR_NONFINITE; s->done = 1; }
+      if(s->converged || s->iter >= s->maxit) s->done = 1;
+      /* inner solve set-up scalars */
+      double mean = project_mean ? red[2] / (double)n : 0.;
+      si->sumx = mean;                 /* subtracted by the inner set-up */
+      si->tol = inner_tol * rn;
+      si->maxit = inner_maxit;
+      si->done = s->done;
+    }
+  }
+}
+
+/* inner set-up from e = 0: r = rh = p = rf - mean, e = 0, (r, r) */
+template <typename T>
+__global__ void __launch_bounds__(256) k_inner_setup(long long n, T *rf,
+  T *e, T *rh, T *p, bbb_kry *si, double *partials)
+{
+  if(((volatile bbb_kry *)si)->done) return;
+  __shared__ double sh[32];
+  T mean = (T)si->sumx;
+  double red[1] = {0.};
+  for(long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+      c += (long long)gridDim.x * blockDim.x) {
+    T rv = rf[c] - mean;
+    rf[c] = rv; rh[c] = rv; p[c] = rv; e[c] = (T)0.;
+    red[0] += (double)rv * (double)rv;
+  }
+  if(bbb_grid_partial<1>(red, partials, &si->ticket, sh)) {
+    bbb_grid_finish_sum<1>(red, partials, &si->ticket, sh);
+    if(threadIdx.x == 0) {
+      double rn = sqrt(red[0]);
+      si->rho = red[0];
+      si->rnorm = rn;
+      si->iter = 0;
+      si->first = 1;
+      si->s_conv = 0;
+      si->alpha = si->omega = si->beta = 0.;
+      si->converged = (rn <= si->tol);
+      si->done = si->converged || si->maxit <= 0 || !isfinite(rn);
+      si->status = isfinite(rn) ? 0 : BBB_ERR_NONFINITE;
+    }
+  }
+}
+
+/* x += e; count the inner iterations into the outer scalars */
+__global__ void __launch_bounds__(256) k_accumulate(long long n, double *x,
+  const float *__restrict__ e, bbb_kry *s, const bbb_kry *si)
+{
+  if(((volatile bbb_kry *)s)->done) return;
+  for(long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+      c += (long long)gridDim.x * blockDim.x)
+    x[c] = x[c] + (double)e[c];
+  if(blockIdx.x == 0 && threadIdx.x == 0) s->iter += 1;   /* outer sweeps */
+  (void)si;
+}
+
+static void ensure_fp32(void)
+{
+  if(g_dev.fb) return;
+  long long n = g_dev.nmax;
+  float **fs[] = {&g_dev.fb, &g_dev.fx, &g_dev.fr, &g_dev.frh, &g_dev.fp[0],
+    &g_dev.fp[1], &g_dev.fv[0], &g_dev.fv[1], &g_dev.fs, &g_dev.ft};
+  for(size_t a = 0; a < sizeof(fs) / sizeof(fs[0]); a++) {
+    if(cudaMalloc((void **)fs[a], sizeof(float) * (size_t)n) != cudaSuccess)
+      bbb_set_status(BBB_ERR_CUDA, "cudaMalloc fp32 workspace");
+    else
+      cudaMemsetAsync(*fs[a], 0, sizeof(float) * (size_t)n, g_dev.stream);
+  }
+  if(!g_dev.kry_inner) {
+    if(cudaMalloc((void **)&g_dev.kry_inner, sizeof(bbb_kry)) != cudaSuccess)
+      bbb_set_status(BBB_ERR_CUDA, "cudaMalloc inner scalars");
+    cudaMemsetAsync(g_dev.kry_inner, 0, sizeof(bbb_kry), g_dev.stream);
+  }
+}
+
+/* runs after k_pp_rhs has filled b, x and s->bnorm */
+static int poisson_mixed(const boxc &B, const opc &O, long long n, int record)
+{
+  ensure_fp32();
+  bbb_kry *s = g_dev.kry, *si = g_dev.kry_inner;
+  dim3 grd = box_grid(B), blk(TX, TY);
+  /* outer scalars: tol, iteration counters */
+  bbb_kry init;
+  memset(&init, 0, sizeof(init));
+  BBB_CK(cudaMemcpyAsync(g_dev.kry_host, s, sizeof(bbb_kry),
+    cudaMemcpyDeviceToHost, g_dev.stream));
+  BBB_CK(cudaStreamSynchronize(g_dev.stream));
+  init.bnorm = g_dev.kry_host->bnorm;
+  init.tol = pp_residual * init.bnorm;
+  init.maxit = g_opt.max_outer > 0 ? g_opt.max_outer : 20;
+  BBB_CK(cudaMemcpyAsync(s, &init, sizeof(bbb_kry), cudaMemcpyHostToDevice,
+    g_dev.stream));
+  int project = (nparts == 0) && (bc.pW == bc.pE) && (bc.pS == bc.pN)
+    && (bc.pB == bc.pT);
+  double itol = g_opt.inner_tol > 0 ? g_opt.inner_tol : 1e-4;
+  int inner_total = 0;
+  for(int outer = 0; outer <= init.maxit; outer++) {
+    k_outer_resid<<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p, g_dev.kb,
+      g_dev.kx, g_dev.fb, s, si, g_dev.partials, itol, pp_max_iter, project, n);
+    BBB_LAUNCHED();
+    k_inner_setup<float><<<1184, 256, 0, g_dev.stream>>>(n, g_dev.fb, g_dev.fx,
+      g_dev.frh, g_dev.fp[0], si, g_dev.partials);
+    BBB_LAUNCHED();
+    int cur = 0;
+    /* the inner loop polls the inner scalars */
+    int batch = 4, total = 0;
+    double it_bytes = (double)n * (17. * sizeof(float) + 3.);
+    for(;;) {
+      for(int q = 0; q < batch; q++) {
+        prof_begin(it_bytes);
+        k_bicg1<float><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
+          g_dev.fb, g_dev.fp[cur], g_dev.fv[cur], g_dev.frh, g_dev.fp[cur ^ 1],
+          g_dev.fv[cur ^ 1], si, g_dev.partials);
+        BBB_LAUNCHED();
+        k_bicg2<float><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
+          g_dev.fb, g_dev.fv[cur ^ 1], g_dev.fs, g_dev.ft, si, g_dev.partials);
+        BBB_LAUNCHED();
+        k_bicg3<float><<<1184, 256, 0, g_dev.stream>>>(n, O, g_dev.mask_p,
+          g_dev.fx, g_dev.fp[cur ^ 1], g_dev.fs, g_dev.ft, g_dev.fb, g_dev.frh,
+          si, g_dev.partials);
+        BBB_LAUNCHED();
+        prof_end();
+        cur ^= 1;
+      }
+      total += batch;
+      BBB_CK(cudaMemcpyAsync(g_dev.kry_host, si, sizeof(bbb_kry),
+        cudaMemcpyDeviceToHost, g_dev.stream));
+      BBB_CK(cudaStreamSynchronize(g_dev.stream));
+      if(bbb_last_status() == BBB_ERR_CUDA) return -1;
+      if(g_dev.kry_host->done || total > pp_max_iter + 4) break;
+      if(batch < 16) batch *= 2;
+    }
+    prof_collect(g_dev.kry_host->iter + (g_dev.kry_host->s_conv ? 1 : 0));
+    inner_total += g_dev.kry_host->iter;
+    k_accumulate<<<1184, 256, 0, g_dev.stream>>>(n, g_dev.kx, g_dev.fx, s, si);
+    BBB_LAUNCHED();
+    BBB_CK(cudaMemcpyAsync(g_dev.kry_host, s, sizeof(bbb_kry),
+      cudaMemcpyDeviceToHost, g_dev.stream));
+    BBB_CK(cudaStreamSynchronize(g_dev.stream));
+    if(g_dev.kry_host->done) break;
+  }
+  bbb_kry *h = g_dev.kry_host;
+  real resid = h->bnorm > 0 ? h->rnorm / h->bnorm : h->rnorm;
+  g_stats.pp_solves++;
+  g_stats.pp_iters_total += inner_total;
+  g_stats.pp_iters_last = inner_total;
+  g_stats.pp_resid_last = resid;
+  g_stats.pp_outer_last = h->iter;
+  if(record) bbb_record_solver("solver_expd.rec", inner_total, resid);
+  return h->converged ? inner_total : -inner_total;
+}
+
+int bbb_poisson_solve_mixed(int record)
+{
+  bbb_dev_require();
+  if(!g_dev.ready) return -1;
+  bbb_build_masks();
+  bbb_geom G = bbb_make_geom();
+  boxc B = make_box(G.nx, G.ny, G.nz, bc.pW == BBB_PERIODIC,
+    bc.pS == BBB_PERIODIC, bc.pB == BBB_PERIODIC, 0, 0, 0);
+  opc O;
+  O.wx = 1. / (G.dx * G.dx); O.wy = 1. / (G.dy * G.dy); O.wz = 1. / (G.dz * G.dz);
+  O.helm = 0;
+  long long n = (long long)G.nx * G.ny * G.nz;
+  k_pp_rhs<<<1184, 256, 0, g_dev.stream>>>(g_dev.us, g_dev.vs, g_dev.ws,
+    g_dev.phi, g_dev.phase, G, rho_f / dt, g_dev.kb, g_dev.kx, g_dev.kry,
+    g_dev.partials);
+  BBB_LAUNCHED();
+  int it = poisson_mixed(B, O, n, record);
+  k_pp_writeback<<<1184, 256, 0, g_dev.stream>>>(g_dev.kx, g_dev.phi, G, g_dev.kry);
+  BBB_LAUNCHED();
+  bbb_kry *h = g_dev.kry_host;
+  if(h->status == BBB_ERR_NONFINITE) bbb_set_status(BBB_ERR_NONFINITE, "pressure-Poisson");
+  if(!h->converged) {
+    bbb_set_status(BBB_ERR_NOT_CONVERGED, "pressure-Poisson (mixed)");
+    if(bbb_fail_exit()) {
+      printf("The pressure-Poisson equation did not converge.              \n");
+      exit(EXIT_FAILURE);
+    }
+  }
+  return it;
+}
+
 /* src/cuda_bicgstab.cu:715-1073 */
 extern "C" void cuda_PP_bicgstab(int rank)
 {
   (void)rank;
-  bbb_poisson_solve(1);
+  if(g_opt.precision == BBB_PREC_MIXED) bbb_poisson_solve_mixed(1);
+  else bbb_poisson_solve(1);
 }
 
 /* src/cuda_bicgstab.cu:1178-1204: the un-ghosted Poisson right-hand side

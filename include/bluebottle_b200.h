@@ -231,6 +231,26 @@ void bbb_divergence(real *max_abs, real *l2);
 long long bbb_kernel_launches(void);
 void bbb_reset_kernel_launches(void);
 
+/* Live timing of the pressure solver's BiCGSTAB iteration (its three fused
+ * passes), by CUDA events on the solver stream, over the iterations the
+ * device executed while enabled: total milliseconds, iteration count and
+ * algorithmic bytes (17 vector words + 3 mask bytes per unknown). */
+void bbb_profile_enable(int on);
+void bbb_profile_reset(void);
+void bbb_profile_get(double *ms, long long *iters, double *bytes);
+
+/* Copy only the particle records (part_struct array) between the host
+ * `parts` and the device: the per-step exchange of a caller that moves
+ * particle state, without the phase/flag arrays cuda_part_push/pull also
+ * carry. */
+void bbb_part_state_push(void);
+void bbb_part_state_pull(void);
+
+/* CUDA-event time marks (0..7) on the library's stream; elapsed waits for
+ * mark b and returns milliseconds between marks a and b (-1 on error) */
+void bbb_mark(int i);
+double bbb_mark_elapsed(int a, int b);
+
 #ifdef __cplusplus
 }
 #endif

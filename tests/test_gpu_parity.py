@@ -50,6 +50,27 @@ def test_taylor_green_steps(gpu):
         orc.close()
 
 
+def test_mixed_precision_matches_fp64_oracle(gpu):
+    """FP32 inner solves inside FP64 defect correction reach the same FP64
+    residual test; fields agree with the FP64 oracle to within what that
+    tolerance allows (cond * tol, here < 1e-7)."""
+    wl = configs.taylor_green(32)
+    sim, orc, stats = _run_pair(wl, 3, options=dict(precision=1,
+                                                     inner_tol=1e-4))
+    try:
+        d = sim.dom
+        for name in ("u", "v", "w", "p"):
+            e = rel_err(field_interior(d, name, sim.array(name)),
+                        field_interior(d, name, orc.field(name)))
+            assert e < 1e-7, (name, e)
+        for g, _ in stats:
+            assert g.pp_resid_last <= 1e-10
+            assert g.pp_outer_last >= 1
+    finally:
+        sim.close()
+        orc.close()
+
+
 def test_explicit_ab2_steps(gpu):
     wl = configs.taylor_green(32)
     wl.options["implicit"] = 0
