@@ -124,7 +124,7 @@ bbb_set_record_dir bbb_step bbb_advance_clock bbb_get_stats bbb_last_status
 bbb_status_string bbb_clear_status bbb_set_exit_on_failure bbb_device_count
 bbb_divergence bbb_kernel_launches bbb_reset_kernel_launches
 bbb_profile_enable bbb_profile_reset bbb_profile_get bbb_part_state_push
-bbb_part_state_pull bbb_mark bbb_mark_elapsed""".split()
+bbb_part_state_pull bbb_mark bbb_mark_elapsed bbb_PP_bicgstab_static""".split()
 
 _lib = None
 
@@ -163,6 +163,12 @@ def load():
     lib.cuda_compute_forcing.argtypes = [C.POINTER(R), C.POINTER(R), R, R, R]
     lib.bbb_profile_enable.argtypes = [C.c_int]
     lib.bbb_mark.argtypes = [C.c_int]
+    vp = C.c_void_p
+    lib.bbb_PP_bicgstab_static.restype = C.c_int
+    lib.bbb_PP_bicgstab_static.argtypes = [
+        C.c_int, C.c_int, C.c_int, R, R, R, C.c_int, C.c_int, C.c_int,
+        vp, vp, vp, vp, vp, vp, vp, R, R, R, C.c_int, vp,
+        C.POINTER(C.c_int), C.POINTER(R), vp]
     lib.bbb_mark_elapsed.argtypes = [C.c_int, C.c_int]
     lib.bbb_mark_elapsed.restype = R
     lib.bbb_profile_get.argtypes = [C.POINTER(R), C.POINTER(C.c_longlong),

@@ -1119,3 +1119,115 @@ static void helmholtz_entry(int comp)
 extern "C" void cuda_ustar_helmholtz(int rank) { (void)rank; helmholtz_entry(0); }
 extern "C" void cuda_vstar_helmholtz(int rank) { (void)rank; helmholtz_entry(1); }
 extern "C" void cuda_wstar_helmholtz(int rank) { (void)rank; helmholtz_entry(2); }
+
+/* ------------------------------------------------ allocation-free solve
+ * bbb_PP_bicgstab_static: the FP64 pressure-Poisson solve of
+ * cuda_PP_bicgstab for callers that cannot allocate device memory -- for
+ * example a host application whose own pool allocator owns all of the
+ * GPU's memory, or a time-critical loop that cannot afford the implicit
+ * device synchronisation cudaMalloc/cudaFree bring.  The caller passes the
+ * inputs and the output as device pointers; everything else (operator
+ * mask, Krylov vectors, reduction partials, solver scalars) lives in the
+ * fixed array below, which every GPU that loads this library holds until
+ * the process exits.  No cudaMalloc, cudaFree or allocating library call
+ * is made. */
+#define BBB_STATIC_MAX_CELLS (64LL * 64LL * 64LL)
+#define BBB_STATIC_PARTIALS (16384LL * 4LL)
+#define BBB_STATIC_SCRATCH_BYTES \
+  (256LL + 256LL * ((BBB_STATIC_PARTIALS * 8LL + 255LL) / 256LL) \
+   + 256LL * ((BBB_STATIC_MAX_CELLS + 255LL) / 256LL) \
+   + 10LL * 256LL * ((BBB_STATIC_MAX_CELLS * 8LL + 255LL) / 256LL))
+
+static __device__ __align__(256) unsigned char
+  g_static_scratch[BBB_STATIC_SCRATCH_BYTES];
+
+/* device address of g_static_scratch per device, looked up once with that
+ * device current */
+static unsigned char *g_static_addr[64];
+
+extern "C" int bbb_PP_bicgstab_static(int nx, int ny, int nz, double dx,
+  double dy, double dz, int perx, int pery, int perz, const double *u_star_d,
+  const double *v_star_d, const double *w_star_d, const int *phase_d,
+  const int *flag_u_d, const int *flag_v_d, const int *flag_w_d,
+  double rho_f_, double dt_, double tol, int maxit, double *phi_d,
+  int *iters, double *resid, void *stream)
+{
+  if(nx < 1 || ny < 1 || nz < 1) return BBB_ERR_CONFIG;
+  long long n = (long long)nx * ny * nz;
+  if(n > BBB_STATIC_MAX_CELLS) return BBB_ERR_TOO_LARGE;
+  int dev = 0;
+  if(cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return BBB_ERR_CUDA;
+  if(!g_static_addr[dev]) {
+    unsigned char *p = NULL;
+    if(cudaGetSymbolAddress((void **)&p, g_static_scratch) != cudaSuccess || !p)
+      return BBB_ERR_CUDA;
+    g_static_addr[dev] = p;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  /* carve the scratch */
+  unsigned char *base = g_static_addr[dev];
+  long long off = 0;
+#define CARVE(T, ptr, bytes) do { ptr = (T *)(base + off); \
+  off += 256LL * (((long long)(bytes) + 255LL) / 256LL); } while(0)
+  bbb_kry *s; double *partials; uint8_t *mask;
+  double *b, *x, *r, *rh, *pp[2], *vv[2], *sv, *tv;
+  CARVE(bbb_kry, s, 256);
+  CARVE(double, partials, BBB_STATIC_PARTIALS * 8LL);
+  CARVE(uint8_t, mask, BBB_STATIC_MAX_CELLS);
+  size_t vb = (size_t)BBB_STATIC_MAX_CELLS * 8;
+  CARVE(double, b, vb); CARVE(double, x, vb); CARVE(double, r, vb);
+  CARVE(double, rh, vb); CARVE(double, pp[0], vb); CARVE(double, pp[1], vb);
+  CARVE(double, vv[0], vb); CARVE(double, vv[1], vb); CARVE(double, sv, vb);
+  CARVE(double, tv, vb);
+#undef CARVE
+  /* geometry of the reference's ghosted layouts */
+  bbb_geom G;
+  memset(&G, 0, sizeof(G));
+  G.nx = nx; G.ny = ny; G.nz = nz;
+  G.cc_s1 = nx + 2; G.cc_s2 = (nx + 2) * (ny + 2);
+  G.fx_s1 = nx + 3; G.fx_s2 = (nx + 3) * (ny + 2);
+  G.fy_s1 = nx + 2; G.fy_s2 = (nx + 2) * (ny + 3);
+  G.fz_s1 = nx + 2; G.fz_s2 = (nx + 2) * (ny + 2);
+  G.dx = dx; G.dy = dy; G.dz = dz;
+  boxc B = make_box(nx, ny, nz, perx, pery, perz, 0, 0, 0);
+  dim3 grd = box_grid(B), blk(TX, TY);
+  if((long long)grd.x * grd.y * grd.z > BBB_STATIC_PARTIALS / 4) return BBB_ERR_TOO_LARGE;
+  opc O;
+  O.wx = 1. / (dx * dx); O.wy = 1. / (dy * dy); O.wz = 1. / (dz * dz);
+  O.helm = 0;
+  /* the reduction ticket and the scalars start from zero on every call */
+  if(cudaMemsetAsync(s, 0, sizeof(bbb_kry), st) != cudaSuccess) return BBB_ERR_CUDA;
+  k_mask_p<<<1184, 256, 0, st>>>(flag_u_d, flag_v_d, flag_w_d, phase_d, G, mask);
+  k_pp_rhs<<<1184, 256, 0, st>>>(u_star_d, v_star_d, w_star_d, phi_d, phase_d,
+    G, rho_f_ / dt_, b, x, s, partials);
+  k_bicg_setup<double><<<grd, blk, 0, st>>>(B, O, mask, b, x, r, rh, pp[0],
+    s, partials, tol, maxit);
+  if(cudaPeekAtLastError() != cudaSuccess) return BBB_ERR_CUDA;
+  bbb_kry h;
+  int cur = 0, batch = 1, total = 0;
+  for(;;) {
+    for(int q = 0; q < batch; q++) {
+      k_bicg1<double><<<grd, blk, 0, st>>>(B, O, mask, r, pp[cur], vv[cur], rh,
+        pp[cur ^ 1], vv[cur ^ 1], s, partials);
+      k_bicg2<double><<<grd, blk, 0, st>>>(B, O, mask, r, vv[cur ^ 1], sv, tv,
+        s, partials);
+      k_bicg3<double><<<1184, 256, 0, st>>>(n, O, mask, x, pp[cur ^ 1], sv, tv,
+        r, rh, s, partials);
+      cur ^= 1;
+    }
+    total += batch;
+    if(cudaMemcpyAsync(&h, s, sizeof(bbb_kry), cudaMemcpyDeviceToHost, st)
+      != cudaSuccess) return BBB_ERR_CUDA;
+    if(cudaStreamSynchronize(st) != cudaSuccess) return BBB_ERR_CUDA;
+    if(h.done || total > maxit + 4) break;
+    if(batch < 16) batch *= 2;
+  }
+  k_pp_writeback<<<1184, 256, 0, st>>>(x, phi_d, G, s);
+  if(cudaMemcpyAsync(&h, s, sizeof(bbb_kry), cudaMemcpyDeviceToHost, st)
+    != cudaSuccess) return BBB_ERR_CUDA;
+  if(cudaStreamSynchronize(st) != cudaSuccess) return BBB_ERR_CUDA;
+  if(iters) *iters = h.iter;
+  if(resid) *resid = h.bnorm > 0 ? h.rnorm / h.bnorm : h.rnorm;
+  if(h.status == BBB_ERR_NONFINITE) return BBB_ERR_NONFINITE;
+  return h.converged ? BBB_OK : BBB_ERR_NOT_CONVERGED;
+}

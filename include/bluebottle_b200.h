@@ -251,6 +251,41 @@ void bbb_part_state_pull(void);
 void bbb_mark(int i);
 double bbb_mark_elapsed(int a, int b);
 
+/* Allocation-free pressure-Poisson solve.  No counterpart in the
+ * reference: it is the FP64 solve of cuda_PP_bicgstab for callers that
+ * cannot allocate device memory (a host application whose pool allocator
+ * owns all GPU memory, or a time-critical loop that cannot take the
+ * device-wide synchronisation of cudaMalloc/cudaFree).  It calls no
+ * cudaMalloc, cudaFree or allocating library routine.
+ *   - Inputs and output are device pointers in the reference's ghosted
+ *     layouts: u_star/v_star/w_star (Gfx/Gfy/Gfz), phase and flag_u/v/w,
+ *     and phi, read as the initial guess and overwritten on the interior
+ *     with the mean-free solution (its ghosts are left to the caller's
+ *     boundary-condition pass, as with cuda_PP_bicgstab).
+ *   - Scratch lives in one file-scope device array of about 22 MB, held by
+ *     every GPU that loads the library until the process exits; it limits
+ *     the grid to nx*ny*nz <= 64^3 cells, and larger requests return
+ *     BBB_ERR_TOO_LARGE.
+ *   - The first call on a device looks up that array's device address
+ *     (with that device current); make that first call before any stream
+ *     capture.
+ *   - Every call shares the array and it keeps the last call's contents:
+ *     calls that overlap on the GPU (other streams, other host threads)
+ *     race and must be serialised by the caller.
+ * perx/pery/perz select periodic wrap per axis; tol is the relative
+ * residual ||b - A x|| <= tol ||b||.  Returns BBB_OK,
+ * BBB_ERR_NOT_CONVERGED, BBB_ERR_NONFINITE, BBB_ERR_TOO_LARGE,
+ * BBB_ERR_CONFIG or BBB_ERR_CUDA; iters/resid (may be NULL) receive the
+ * iteration count and the final relative residual.  `stream` is a
+ * cudaStream_t (NULL for the default stream); the call returns after the
+ * solve has finished on it. */
+int bbb_PP_bicgstab_static(int nx, int ny, int nz, double dx, double dy,
+  double dz, int perx, int pery, int perz, const double *u_star,
+  const double *v_star, const double *w_star, const int *phase,
+  const int *flag_u, const int *flag_v, const int *flag_w, double rho_f,
+  double dt, double tol, int maxit, double *phi, int *iters, double *resid,
+  void *stream);
+
 #ifdef __cplusplus
 }
 #endif
