@@ -209,6 +209,7 @@ extern "C" void cuda_part_push(void)
   h2d(g_dev.flag_v, flag_v, sizeof(int) * d->Gfy.s3b);
   h2d(g_dev.flag_w, flag_w, sizeof(int) * d->Gfz.s3b);
   g_dev.masks_valid = 0;
+  g_dev.lf_valid = 0;
   BBB_CK(cudaStreamSynchronize(g_dev.stream));
 }
 
@@ -249,6 +250,7 @@ extern "C" void bbb_part_state_push(void)
   pin_parts();
   if(nparts > 0 && g_dev.np == nparts)
     h2d(g_dev.parts, parts, sizeof(part_struct) * nparts);
+  g_dev.lf_geo_valid = 0;
 }
 
 /* device-side time marks on the library stream */
@@ -312,6 +314,9 @@ extern "C" void cuda_part_free(void)
   for(int a = 0; a < 18; a++) dfree(g_dev.coef[a]);
   dfree(g_dev.node_pp); dfree(g_dev.node_ur); dfree(g_dev.node_ut);
   dfree(g_dev.node_up); dfree(g_dev.perr);
+  dfree(g_dev.lf_idx); dfree(g_dev.lf_part); dfree(g_dev.lf_geo);
+  dfree(g_dev.lf_count);
+  g_dev.lf_cap = 0; g_dev.lf_n = 0; g_dev.lf_valid = 0; g_dev.lf_geo_valid = 0;
   g_dev.np = 0;
 }
 

@@ -87,6 +87,14 @@ struct bbb_dev {
   real *coef[18];
   real *node_pp, *node_ur, *node_ut, *node_up;   /* nparts*26 each */
   real *perr;                      /* per-particle Lamb error            */
+  /* faces whose velocity the particle boundary condition sets: packed
+   * (component << 30 | ghosted face index), owning particle, and the
+   * face geometry in the particle frame (LF_NGEO arrays of lf_cap) */
+  long long lf_cap, lf_n;
+  int *lf_idx, *lf_part;
+  double *lf_geo;
+  unsigned int *lf_count;
+  int lf_valid, lf_geo_valid;
   real *red_host;                  /* pinned scratch for host reductions */
   double *red_dev;                 /* device scratch for small reductions */
   unsigned int *red_ticket;

@@ -317,6 +317,7 @@ extern "C" void cuda_build_cages(void)
     }
   }
   g_dev.masks_valid = 0;
+  g_dev.lf_valid = 0;
 }
 
 /* ------------------------------------------------ Lamb's series */
@@ -483,33 +484,92 @@ __device__ __forceinline__ double d_wrap_rel(double x, double a, double L)
   return x;
 }
 
-/* part_BC_u/v/w (src/particle_kernel.cu:535-838): every interior face of
- * each component, ghost rows included.  Faces that neither border a
- * particle cell nor carry flag < 1 are left untouched without evaluating
- * the series. */
-__global__ void k_part_BC(real *uu, real *vv, real *ww, const int *phs,
-  const int *fu, const int *fv, const int *fw, const part_struct *parts,
-  coef_ptrs cf, int stride, double nu, bbb_geom G)
+/* ------------------------------------------------ particle BC faces
+ * part_BC_u/v/w (src/particle_kernel.cu:535-838) visit every interior
+ * face of each component, ghost rows included, and overwrite those with
+ * flag < 1 that border a particle cell with the Lamb velocity plus the
+ * rigid-body motion.  Those faces depend only on phase and flags, which
+ * change only in the cage build, and their positions relative to the
+ * particle change only when particles move; the Lamb loop applies the
+ * condition about seven times per sub-iteration.  So the faces are listed
+ * once per cage build, their particle-frame geometry (r, cos/sin theta,
+ * cos/sin m phi) once per particle move, and each application evaluates
+ * the series from that list with no transcendental calls. */
+
+#define LF_NGEO 14   /* x y z r ct st cp1 sp1 cp2 sp2 cp3 sp3 cp4 sp4 */
+__constant__ double c_Nnm[6][6];
+static int g_nnm_ready = 0;
+
+static void upload_nnm(void)
+{
+  if(g_nnm_ready) return;
+  double t[6][6];
+  for(int n = 0; n < 6; n++) for(int m = 0; m < 6; m++) {
+    double top = 1, bot = 1;
+    for(int i = 1; i <= (n - m); i++) top *= (double)i;
+    for(int i = 1; i <= (n + m); i++) bot *= (double)i;
+    t[n][m] = m <= n ? sqrt((2. * n + 1.) / 4. / PI * top / bot) : 0.;
+  }
+  BBB_CK(cudaMemcpyToSymbol(c_Nnm, t, sizeof(t)));
+  g_nnm_ready = 1;
+}
+
+/* the faces part_BC would change: flag < 1 and a particle cell on either
+ * side (the first side wins, as in the reference) */
+__device__ __forceinline__ int lf_owner(int comp, int i, int j, int k,
+  const int *phs, const int *fu, const int *fv, const int *fw,
+  const bbb_geom &G, long long *Cout)
+{
+  int s1 = comp == 0 ? G.fx_s1 : (comp == 1 ? G.fy_s1 : G.fz_s1);
+  int s2 = comp == 0 ? G.fx_s2 : (comp == 1 ? G.fy_s2 : G.fz_s2);
+  long long C = i + (long long)j * s1 + (long long)k * s2;
+  const int *flag = comp == 0 ? fu : (comp == 1 ? fv : fw);
+  if(flag[C] >= 1) return -1;
+  long long cc = i + (long long)j * G.cc_s1 + (long long)k * G.cc_s2;
+  long long cstep = comp == 0 ? 1 : (comp == 1 ? G.cc_s1 : G.cc_s2);
+  int P0 = phs[cc - cstep], P1 = phs[cc];
+  *Cout = C;
+  return P0 > -1 ? P0 : (P1 > -1 ? P1 : -1);
+}
+
+/* pass 0 counts, pass 1 fills (slot order is irrelevant: every face is
+ * written by exactly one entry) */
+__global__ void k_lf_collect(const int *phs, const int *fu, const int *fv,
+  const int *fw, bbb_geom G, int pass, unsigned int *count, int *idx,
+  int *part, long long cap)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
   int k = blockIdx.z;
+  if(i > G.nx + 1 || j > G.ny + 1 || k > G.nz + 1) return;
   for(int comp = 0; comp < 3; comp++) {
-    int ilo = comp == 0 ? 1 : 0, ihi = comp == 0 ? G.nx + 2 : G.nx + 2;
-    int jlo = comp == 1 ? 1 : 0, jhi = comp == 1 ? G.ny + 2 : G.ny + 2;
-    int klo = comp == 2 ? 1 : 0, khi = comp == 2 ? G.nz + 2 : G.nz + 2;
-    if(i < ilo || i >= ihi || j < jlo || j >= jhi || k < klo || k >= khi) continue;
+    if((comp == 0 && i < 1) || (comp == 1 && j < 1) || (comp == 2 && k < 1)) continue;
+    long long C;
+    int P = lf_owner(comp, i, j, k, phs, fu, fv, fw, G, &C);
+    if(P < 0) continue;
+    unsigned int slot = atomicAdd(count, 1u);
+    if(pass == 1 && slot < cap) {
+      idx[slot] = (int)(((unsigned int)comp << 30) | (unsigned int)C);
+      part[slot] = P;
+    }
+  }
+}
+
+/* particle-frame geometry of every listed face, from the current
+ * particle positions */
+__global__ void k_lf_geom(long long n, const int *idx, const int *part,
+  const part_struct *parts, bbb_geom G, double *geo, long long cap)
+{
+  for(long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+      e += (long long)gridDim.x * blockDim.x) {
+    unsigned int pk = (unsigned int)idx[e];
+    int comp = (int)(pk >> 30);
+    long long C = (long long)(pk & 0x3fffffffu);
     int s1 = comp == 0 ? G.fx_s1 : (comp == 1 ? G.fy_s1 : G.fz_s1);
     int s2 = comp == 0 ? G.fx_s2 : (comp == 1 ? G.fy_s2 : G.fz_s2);
-    long long C = i + (long long)j * s1 + (long long)k * s2;
-    const int *flag = comp == 0 ? fu : (comp == 1 ? fv : fw);
-    if(flag[C] >= 1) continue;
-    long long cc = i + (long long)j * G.cc_s1 + (long long)k * G.cc_s2;
-    long long cstep = comp == 0 ? 1 : (comp == 1 ? G.cc_s1 : G.cc_s2);
-    int P0 = phs[cc - cstep], P1 = phs[cc];
-    int P = P0 > -1 ? P0 : (P1 > -1 ? P1 : -1);
-    if(P < 0) continue;
-    const part_struct *q = &parts[P];
+    int k = (int)(C / s2), rem = (int)(C % s2);
+    int j = rem / s1, i = rem % s1;
+    const part_struct *q = &parts[part[e]];
     double a = q->r;
     double x = (comp == 0 ? (i - BBB_DOM_BUF) * G.dx : (i - 0.5) * G.dx) + G.xs - q->x;
     double y = (comp == 1 ? (j - BBB_DOM_BUF) * G.dy : (j - 0.5) * G.dy) + G.ys - q->y;
@@ -519,24 +579,195 @@ __global__ void k_part_BC(real *uu, real *vv, real *ww, const int *phs,
     z = d_wrap_rel(z, a, G.zl);
     double r, theta, phi;
     d_xyz2rtp(x, y, z, &r, &theta, &phi);
-    double Ux, Uy, Uz;
-    d_lamb_vel(q->order, a, r, theta, phi, nu, cf, P, stride, &Ux, &Uy, &Uz);
+    double g[LF_NGEO];
+    g[0] = x; g[1] = y; g[2] = z; g[3] = r;
+    g[4] = cos(theta); g[5] = sin(theta);
+    for(int m = 1; m <= 4; m++) { g[4 + 2 * m] = cos(m * phi); g[5 + 2 * m] = sin(m * phi); }
+#pragma unroll
+    for(int a2 = 0; a2 < LF_NGEO; a2++) geo[a2 * cap + e] = g[a2];
+  }
+}
+
+/* associated Legendre P_n^m from x = cos theta, y = sin theta (n <= 5) */
+__device__ __forceinline__ double lf_P(int n, int m, double x, double y)
+{
+  switch(n * 10 + m) {
+    case 0: return 1;
+    case 10: return x;
+    case 11: return -y;
+    case 20: return 0.5 * (3. * x * x - 1.);
+    case 21: return -3. * x * y;
+    case 22: return 3. * y * y;
+    case 30: return 0.5 * x * (5. * x * x - 3.);
+    case 31: return -1.5 * (5. * x * x - 1.) * y;
+    case 32: return 15. * x * y * y;
+    case 33: return -15. * y * y * y;
+    case 40: return 0.125 * (35. * x * x * x * x - 30. * x * x + 3.);
+    case 41: return -2.5 * (7. * x * x - 3.) * x * y;
+    case 42: return 7.5 * (7. * x * x - 1.) * y * y;
+    case 43: return -105. * x * y * y * y;
+    case 44: return 105. * y * y * y * y;
+    case 50: return 0.125 * x * (63. * x * x * x * x - 70. * x * x + 15.);
+    case 51: return -1.875 * y * (21. * x * x * x * x - 14. * x * x + 1.);
+    case 52: return 52.5 * x * y * y * (3. * x * x - 1.);
+    case 53: return -52.5 * y * y * y * (9. * x * x - 1.);
+    case 54: return 945. * x * y * y * y * y;
+    case 55: return -945. * y * y * y * y * y;
+  }
+  return 0;
+}
+
+/* Lamb velocity (src/particle_kernel.cu:1311-1369) from the stored face
+ * geometry; the X/Y/Z angular sums of :1107-1309 with cos(m phi),
+ * sin(m phi), cos theta, sin theta precomputed and powers of r/a formed
+ * by multiplication */
+__global__ void __launch_bounds__(256) k_lf_eval(long long n, const int *idx,
+  const int *part, const double *__restrict__ geo, long long cap,
+  const part_struct *parts, coef_ptrs cf, int stride, double nu, real *uu,
+  real *vv, real *ww)
+{
+  for(long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+      e += (long long)gridDim.x * blockDim.x) {
+    unsigned int pk = (unsigned int)idx[e];
+    int comp = (int)(pk >> 30);
+    long long C = (long long)(pk & 0x3fffffffu);
+    int P = part[e];
+    const part_struct *q = &parts[P];
+    double x = geo[0 * cap + e], y = geo[1 * cap + e], z = geo[2 * cap + e];
+    double r = geo[3 * cap + e], ct = geo[4 * cap + e], st = geo[5 * cap + e];
+    double cm[5], sm[5];
+    cm[0] = 1.; sm[0] = 0.;
+#pragma unroll
+    for(int m = 1; m <= 4; m++) { cm[m] = geo[(4 + 2 * m) * cap + e]; sm[m] = geo[(5 + 2 * m) * cap + e]; }
+    double stc = st;
+    if(stc >= 0 && stc < DIV_ST) stc = DIV_ST;
+    else if(stc < 0 && stc > -DIV_ST) stc = -DIV_ST;
+    double a = q->r;
+    double ar = a / r, ra = r / a;
+    int order = q->order;
+    const double *pre = cf.c[0], *pim = cf.c[1], *fre = cf.c[2], *fim = cf.c[3],
+                 *cre = cf.c[4], *cim = cf.c[5];
+    int base = P * stride;
+    /* n = 0 terms */
+    double Y0 = c_Nnm[0][0] * (-1. * ct / stc * 1. + 1. / stc * lf_P(1, 0, ct, st)) * pre[base];
+    double ur = 0.;
+    double ut = 0.5 * ra * Y0;
+    double up = 0.;
+    double ran = 1., arn = 1.;   /* ra^(n-1), ar^n at the loop head */
+    int c0 = 1;
+    for(int nn_ = 1; nn_ <= order; nn_++) {
+      double n = nn_;
+      arn *= ar;
+      double powranm1 = ran;
+      double powranp1 = ran * ra * ra;
+      double powarn = arn;
+      double powarnp1 = arn * ar;
+      double powarnp2 = powarnp1 * ar;
+      double od2np3 = 1. / (2. * n + 3.);
+      double odnp1 = 1. / (n + 1.);
+      double Xp = 0., Xf = 0., Yp = 0., Yf = 0., Yc = 0., Zp = 0., Zf = 0., Zc = 0.;
+      for(int m = 0; m <= nn_; m++) {
+        int c = base + c0 + m;
+        double N = c_Nnm[nn_][m];
+        double Pn = lf_P(nn_, m, ct, st);
+        double dY = -(n + 1) * ct / stc * Pn + (nn_ - m + 1) / stc * lf_P(nn_ + 1, m, ct, st);
+        double w = m == 0 ? 1. : 2.;
+        double Rp = pre[c] * cm[m] - pim[c] * sm[m];
+        double Rf = fre[c] * cm[m] - fim[c] * sm[m];
+        double Rc = cre[c] * cm[m] - cim[c] * sm[m];
+        Xp += w * N * Pn * Rp;
+        Xf += w * N * Pn * Rf;
+        Yp += w * N * dY * Rp;
+        Yf += w * N * dY * Rf;
+        Yc += w * N * dY * Rc;
+        if(m > 0) {
+          double zf = -2. * m / stc * N * Pn;
+          Zp += zf * (pre[c] * sm[m] + pim[c] * cm[m]);
+          Zf += zf * (fre[c] * sm[m] + fim[c] * cm[m]);
+          Zc += zf * (cre[c] * sm[m] + cim[c] * cm[m]);
+        }
+      }
+      ur += (0.5 * n * od2np3 * powranp1
+        + 0.25 * n * ((2. * n + 1.) * od2np3 * ar * ar - 1.) * powarn) * Xp;
+      ur += (n * powranm1
+        + 0.5 * n * (2. * n - 1. - (2. * n + 1.) * ra * ra) * powarnp2) * Xf;
+      ut += (0.5 * (n + 3.) * odnp1 * od2np3 * powranp1
+        + 0.25 * odnp1 * (n - 2. - n * (2. * n + 1.) * od2np3 * ar * ar) * powarn) * Yp;
+      ut += (powranm1
+        + 0.5 * odnp1 * ((n - 2.) * (2. * n + 1.) * ra * ra - n * (2. * n - 1.)) * powarnp2) * Yf;
+      ut += (powranm1 - powarnp1) * Zc;
+      up += (0.5 * (n + 3.) * odnp1 * od2np3 * powranp1
+        + 0.25 * odnp1 * (n - 2. - n * (2. * n + 1.) * od2np3 * ar * ar) * powarn) * Zp;
+      up += (powranm1
+        + 0.5 * odnp1 * ((n - 2.) * (2. * n + 1.) * ra * ra - n * (2. * n - 1.)) * powarnp2) * Zf;
+      up += (-powranm1 + powarnp1) * Yc;
+      ran *= ra;
+      c0 += nn_ + 1;
+    }
+    ur *= nu / a;
+    ut *= nu / a;
+    up *= nu / a;
     double rr = 0.1 / nu * (r * r * r * r * r - a * a * a * a * a) / (r * r * r);
-    double val;
     if(comp == 0) {
-      val = Ux + q->u + (q->oy * z - q->oz * y);
+      double Ux = ur * st * cm[1] + ut * ct * cm[1] - up * sm[1];
+      double val = Ux + q->u + (q->oy * z - q->oz * y);
       val += rr * (q->oydot * z - q->ozdot * y);
       uu[C] = val;
     } else if(comp == 1) {
-      val = Uy + q->v + (-(q->ox * z - q->oz * x));
+      double Uy = ur * st * sm[1] + ut * ct * sm[1] + up * cm[1];
+      double val = Uy + q->v + (-(q->ox * z - q->oz * x));
       val += rr * (-(q->oxdot * z - q->ozdot * x));
       vv[C] = val;
     } else {
-      val = Uz + q->w + (q->ox * y - q->oy * x);
+      double Uz = ur * ct - ut * st;
+      double val = Uz + q->w + (q->ox * y - q->oy * x);
       val += rr * (q->oxdot * y - q->oydot * x);
       ww[C] = val;
     }
   }
+}
+
+static void lf_build(void)
+{
+  bbb_geom G = bbb_make_geom();
+  dim3 blk(32, 8), grd((G.nx + 2 + 31) / 32, (G.ny + 2 + 7) / 8, G.nz + 2);
+  if(!g_dev.lf_count) {
+    if(cudaMalloc((void **)&g_dev.lf_count, sizeof(unsigned int)) != cudaSuccess) {
+      bbb_set_status(BBB_ERR_CUDA, "cudaMalloc face list");
+      return;
+    }
+  }
+  for(int pass = 0; pass < 2; pass++) {
+    BBB_CK(cudaMemsetAsync(g_dev.lf_count, 0, sizeof(unsigned int), g_dev.stream));
+    k_lf_collect<<<grd, blk, 0, g_dev.stream>>>(g_dev.phase, g_dev.flag_u,
+      g_dev.flag_v, g_dev.flag_w, G, pass, g_dev.lf_count, g_dev.lf_idx,
+      g_dev.lf_part, g_dev.lf_cap);
+    BBB_LAUNCHED();
+    if(pass == 0) {
+      unsigned int cnt = 0;
+      BBB_CK(cudaMemcpyAsync(&cnt, g_dev.lf_count, sizeof(cnt),
+        cudaMemcpyDeviceToHost, g_dev.stream));
+      BBB_CK(cudaStreamSynchronize(g_dev.stream));
+      g_dev.lf_n = cnt;
+      if((long long)cnt > g_dev.lf_cap) {
+        long long cap = (long long)cnt + cnt / 4 + 1024;
+        if(g_dev.lf_idx) cudaFree(g_dev.lf_idx);
+        if(g_dev.lf_part) cudaFree(g_dev.lf_part);
+        if(g_dev.lf_geo) cudaFree(g_dev.lf_geo);
+        g_dev.lf_idx = NULL; g_dev.lf_part = NULL; g_dev.lf_geo = NULL;
+        if(cudaMalloc((void **)&g_dev.lf_idx, sizeof(int) * cap) != cudaSuccess
+          || cudaMalloc((void **)&g_dev.lf_part, sizeof(int) * cap) != cudaSuccess
+          || cudaMalloc((void **)&g_dev.lf_geo, sizeof(double) * LF_NGEO * cap) != cudaSuccess) {
+          bbb_set_status(BBB_ERR_CUDA, "cudaMalloc face list");
+          g_dev.lf_cap = 0;
+          return;
+        }
+        g_dev.lf_cap = cap;
+      }
+    }
+  }
+  g_dev.lf_valid = 1;
+  g_dev.lf_geo_valid = 0;
 }
 
 static coef_ptrs cur_coefs(void)
@@ -550,11 +781,22 @@ void bbb_part_BC_fields(real *uu, real *vv, real *ww)
 {
   bbb_dev_require();
   if(!g_dev.ready || nparts <= 0 || g_dev.np != nparts) return;
-  bbb_geom G = bbb_make_geom();
-  dim3 blk(32, 8), grd((G.nx + 2 + 31) / 32, (G.ny + 2 + 7) / 8, G.nz + 2);
-  k_part_BC<<<grd, blk, 0, g_dev.stream>>>(uu, vv, ww, g_dev.phase,
-    g_dev.flag_u, g_dev.flag_v, g_dev.flag_w, g_dev.parts, cur_coefs(),
-    coeff_stride, nu, G);
+  upload_nnm();
+  if(!g_dev.lf_valid) lf_build();
+  if(bbb_last_status() == BBB_ERR_CUDA) return;
+  long long n = g_dev.lf_n;
+  if(n <= 0) return;
+  int blocks = (int)((n + 255) / 256);
+  if(blocks > 148 * 16) blocks = 148 * 16;
+  if(!g_dev.lf_geo_valid) {
+    k_lf_geom<<<blocks, 256, 0, g_dev.stream>>>(n, g_dev.lf_idx, g_dev.lf_part,
+      g_dev.parts, bbb_make_geom(), g_dev.lf_geo, g_dev.lf_cap);
+    BBB_LAUNCHED();
+    g_dev.lf_geo_valid = 1;
+  }
+  k_lf_eval<<<blocks, 256, 0, g_dev.stream>>>(n, g_dev.lf_idx, g_dev.lf_part,
+    g_dev.lf_geo, g_dev.lf_cap, g_dev.parts, cur_coefs(), coeff_stride, nu,
+    uu, vv, ww);
   BBB_LAUNCHED();
 }
 
@@ -1142,4 +1384,5 @@ extern "C" void cuda_move_parts(void)
   k_move_parts<<<(nparts + 127) / 128, 128, 0, g_dev.stream>>>(g_dev.parts,
     nparts, 1, dt, rho_f, g, gradP, bbb_make_geom());
   BBB_LAUNCHED();
+  g_dev.lf_geo_valid = 0;   /* positions moved */
 }
