@@ -4,12 +4,13 @@
  * the 13-diagonal DIA matrices it rebuilds every call (13 words per row,
  * src/bicgstab_kernel.cu:643-1856) are never formed.  One byte per unknown
  * holds the six face weights |flag| and the identity-row bit; the operator
- * is applied from that byte inside the fused kernels.
+ * is applied from that byte inside the fused kernels, with the diagonal and
+ * the Jacobi scale of the 128 possible bytes tabulated in shared memory.
  *
  * BiCGSTAB (right-preconditioned, as CUSP's krylov::bicgstab) runs as three
  * fused passes per iteration, with all scalars kept on the device:
- *   K1  p = r + beta (p - omega v);  v = A M p;   (rh, v)      -> alpha
- *   K2  s = r - alpha v;             t = A M s;   (t,s) (t,t) (s,s)
+ *   K1  p = r + beta p - beta omega v;  v = A M p;   (rh, v)   -> alpha
+ *   K2  s = r - alpha v;                t = A M s;   (t,s) (t,t) (s,s)
  *   K3  x += alpha M p + omega M s;  r = s - omega t;  (rh,r) (r,r) sum x
  * 17 vector words + 3 mask bytes per unknown and iteration.  CG (CUSP's
  * krylov::cg, used for the Crank-Nicolson Helmholtz solves) runs as two:
@@ -18,10 +19,12 @@
  * Stopping rule of CUSP's monitor: ||r|| <= rtol ||b||, iteration count
  * advanced once per full iteration, early exit when ||s|| meets it.
  *
- * Stencil kernels tile x-y as 32x8 (one thread per column) and march along
- * z through a slab; the x-y halo of the producer values sits in a
- * three-plane shared-memory ring (one barrier per plane), the z neighbours
- * of a column stay in registers.
+ * Stencil kernels tile x-y with 32x8 threads and march along z through a
+ * slab.  Where the row length allows, each thread owns V consecutive cells
+ * in x (V = 4 for FP32, 2 for FP64: one 128-bit access per array); x
+ * neighbours come from registers and warp shuffles, y neighbours from a
+ * three-plane shared-memory ring (one barrier per plane), z neighbours
+ * from registers.  Rows of other lengths use a one-cell-per-thread tile.
  */
 #include <math.h>
 #include <stdio.h>
@@ -34,6 +37,7 @@
 #define HX (TX + 2)
 #define HY (TY + 2)
 #define NTHR (TX * TY)
+#define NPW 1184          /* blocks of the pointwise passes (8 per SM) */
 
 /* operator constants in the form the kernels use */
 struct opc {
@@ -45,10 +49,19 @@ struct boxc {
   int nx, ny, nz;
   int wW, wE, wS, wN, wB, wT;   /* wrapped neighbour index at each edge */
   int slab;                     /* planes per block                    */
+  int vec;                      /* cells per thread along x            */
 };
 
+/* vector width usable for a row of nx cells of element size `esz` */
+static int pick_vec(int nx, int esz)
+{
+  int v = 16 / esz;
+  if(nx % (TX * v) == 0) return v;
+  return 1;
+}
+
 static boxc make_box(int nx, int ny, int nz, int perx, int pery, int perz,
-  int dupx, int dupy, int dupz)
+  int dupx, int dupy, int dupz, int vec)
 {
   boxc b;
   b.nx = nx; b.ny = ny; b.nz = nz;
@@ -58,9 +71,11 @@ static boxc make_box(int nx, int ny, int nz, int perx, int pery, int perz,
   b.wN = pery ? (dupy ? 1 : 0) : ny - 1;
   b.wB = perz ? (dupz ? nz - 2 : nz - 1) : 0;
   b.wT = perz ? (dupz ? 1 : 0) : nz - 1;
-  /* blocks: ~8 per SM resident; aim for several waves of x-y tiles */
-  long long tiles = (long long)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY);
-  int slabs = (int)((148LL * 8 * 4 + tiles - 1) / tiles);
+  b.vec = vec;
+  /* about two waves of 4 resident blocks per SM; long slabs keep the
+   * re-read of the two z-halo planes small */
+  long long tiles = (long long)((nx + TX * vec - 1) / (TX * vec)) * ((ny + TY - 1) / TY);
+  int slabs = (int)((148LL * 8 + tiles - 1) / tiles);
   if(slabs < 1) slabs = 1;
   int kz = (nz + slabs - 1) / slabs;
   if(kz < 4) kz = 4;
@@ -71,7 +86,7 @@ static boxc make_box(int nx, int ny, int nz, int perx, int pery, int perz,
 
 static dim3 box_grid(const boxc &b)
 {
-  return dim3((b.nx + TX - 1) / TX, (b.ny + TY - 1) / TY,
+  return dim3((b.nx + TX * b.vec - 1) / (TX * b.vec), (b.ny + TY - 1) / TY,
     (b.nz + b.slab - 1) / b.slab);
 }
 
@@ -83,7 +98,7 @@ __device__ __forceinline__ int mapz(const boxc &b, int g)
 { return g < 0 ? b.wB : (g >= b.nz ? (g == b.nz ? b.wT : b.nz - 1) : g); }
 
 /* diagonal of the row with mask m, in the reference's summation order */
-__device__ __forceinline__ double op_diag(uint8_t m, const opc &O)
+__host__ __device__ __forceinline__ double op_diag(unsigned m, const opc &O)
 {
   if(m & BBB_MID) return 1.;
   double fW = (m & BBB_MW) ? 1. : 0., fE = (m & BBB_ME) ? 1. : 0.;
@@ -103,16 +118,35 @@ __device__ __forceinline__ double op_diag(uint8_t m, const opc &O)
   return d;
 }
 
+/* per-block tables of diagonal and Jacobi scale for the 128 mask bytes */
+template <typename T>
+struct optab {
+  T diag[128];
+  T dinv[128];
+};
+
+template <typename T>
+__device__ __forceinline__ void optab_fill(optab<T> &t, const opc &O)
+{
+  int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  int nthr = blockDim.x * blockDim.y;
+  for(int m = tid; m < 128; m += nthr) {
+    double d = op_diag((unsigned)m, O);
+    t.diag[m] = (T)d;
+    t.dinv[m] = (T)(1. / d);
+  }
+  __syncthreads();
+}
+
 /* y = (A q)_c from the centre value, its six neighbours and the row mask;
  * neighbours in the order of the DIA diagonals: B, S, W, C, E, N, T */
 template <typename T>
-__device__ __forceinline__ T op_apply(uint8_t m, const opc &O, T qB, T qS,
-  T qW, T qC, T qE, T qN, T qT)
+__device__ __forceinline__ T op_apply(unsigned m, const opc &O, T d, T qB,
+  T qS, T qW, T qC, T qE, T qN, T qT)
 {
   if(m & BBB_MID) return qC;
   T sg = O.helm ? (T)-1. : (T)1.;
   T wx = (T)O.wx * sg, wy = (T)O.wy * sg, wz = (T)O.wz * sg;
-  T d = (T)op_diag(m, O);
   T acc = (T)0.;
   acc += ((m & BBB_MB) ? wz : (T)0.) * qB;
   acc += ((m & BBB_MS) ? wy : (T)0.) * qS;
@@ -127,14 +161,57 @@ __device__ __forceinline__ T op_apply(uint8_t m, const opc &O, T qB, T qS,
 __device__ __forceinline__ long long lin(const boxc &b, int i, int j, int k)
 { return i + (long long)b.nx * (j + (long long)b.ny * k); }
 
-/* ------------------------------------------------ tiled stencil driver
- * P: producer, evaluated at any (mapped) cell: raw value and the value the
- *    operator is applied to.  E: epilogue at each owned cell.  The driver
- *    fills the shared ring for every plane of the slab and calls E with
- *    (A q) at the owned cell. */
+/* ------------------------------------------------ vector access */
+template <typename T, int V> struct VT;
+template <> struct VT<float, 1> { typedef float t; };
+template <> struct VT<float, 2> { typedef float2 t; };
+template <> struct VT<float, 4> { typedef float4 t; };
+template <> struct VT<double, 1> { typedef double t; };
+template <> struct VT<double, 2> { typedef double2 t; };
+template <int V> struct VM;
+template <> struct VM<1> { typedef unsigned char t; };
+template <> struct VM<2> { typedef uchar2 t; };
+template <> struct VM<4> { typedef uchar4 t; };
+
+template <typename T, int V>
+__device__ __forceinline__ void ldv(const T *p, long long c, T (&o)[V])
+{
+  typename VT<T, V>::t x = *reinterpret_cast<const typename VT<T, V>::t *>(p + c);
+  const T *e = reinterpret_cast<const T *>(&x);
+#pragma unroll
+  for(int v = 0; v < V; v++) o[v] = e[v];
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void stv(T *p, long long c, const T (&o)[V])
+{
+  typename VT<T, V>::t x;
+  T *e = reinterpret_cast<T *>(&x);
+#pragma unroll
+  for(int v = 0; v < V; v++) e[v] = o[v];
+  *reinterpret_cast<typename VT<T, V>::t *>(p + c) = x;
+}
+
+template <int V>
+__device__ __forceinline__ void ldm(const uint8_t *p, long long c, unsigned (&o)[V])
+{
+  typename VM<V>::t x = *reinterpret_cast<const typename VM<V>::t *>(p + c);
+  const unsigned char *e = reinterpret_cast<const unsigned char *>(&x);
+#pragma unroll
+  for(int v = 0; v < V; v++) o[v] = e[v];
+}
+
+/* ------------------------------------------------ tiled stencil drivers
+ * P: producer; P::ev<V>(c, raw, q, dinv) gives at V consecutive cells the
+ * raw value and the value the operator is applied to.  E: epilogue;
+ * E::at<V>(c, raw, Aq, red) at the owned cells.  Both drivers fill the
+ * shared ring for every plane of the slab. */
+
+/* one cell per thread; any row length (partial tiles wrap by index) */
 template <typename T, class P, class E, int NRED>
-__device__ __forceinline__ void tile_stencil(const boxc &B, const opc &O,
-  const uint8_t *__restrict__ mask, P &prod, E &epi, double (&red)[NRED])
+__device__ __forceinline__ void tile_stencil1(const boxc &B, const opc &O,
+  const uint8_t *__restrict__ mask, const optab<T> &tab, P &prod, E &epi,
+  double (&red)[NRED])
 {
   __shared__ T ring[3][HY][HX];
   int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
@@ -143,7 +220,6 @@ __device__ __forceinline__ void tile_stencil(const boxc &B, const opc &O,
   int i = i0 + tx, j = j0 + ty;
   bool valid = (i < B.nx) && (j < B.ny);
   int gi = mapx(B, i), gj = mapy(B, j);
-  /* halo cell of this thread (80 of them; corners are not needed) */
   int hsx = -1, hsy = -1, hgi = 0, hgj = 0;
   if(tid < 32) { hsx = tid + 1; hsy = 0; }
   else if(tid < 64) { hsx = tid - 32 + 1; hsy = HY - 1; }
@@ -151,55 +227,139 @@ __device__ __forceinline__ void tile_stencil(const boxc &B, const opc &O,
   else if(tid < 80) { hsx = HX - 1; hsy = tid - 72 + 1; }
   if(hsx >= 0) { hgi = mapx(B, i0 - 1 + hsx); hgj = mapy(B, j0 - 1 + hsy); }
 
-  T raw_prev, raw_cur, raw_next, q_prev, q_cur, q_next;
-  uint8_t m_cur = 0, m_next = 0;
-  {
-    int kk = mapz(B, k0 - 1);
-    prod.eval(lin(B, gi, gj, kk), raw_prev, q_prev);
-  }
+  T raw_cur[1], raw_next[1], q_prev[1], q_cur[1], q_next[1], hr[1], hq[1];
+  unsigned m_cur[1], m_next[1];
+  prod.template ev<1>(lin(B, gi, gj, mapz(B, k0 - 1)), hr, q_prev, tab.dinv);
   {
     long long c = lin(B, gi, gj, k0);
-    prod.eval(c, raw_cur, q_cur);
-    m_cur = mask[c];
-    ring[0][ty + 1][tx + 1] = q_cur;
+    prod.template ev<1>(c, raw_cur, q_cur, tab.dinv);
+    ldm<1>(mask, c, m_cur);
+    ring[0][ty + 1][tx + 1] = q_cur[0];
     if(hsx >= 0) {
-      T hr, hq;
-      prod.eval(lin(B, hgi, hgj, k0), hr, hq);
-      ring[0][hsy][hsx] = hq;
+      prod.template ev<1>(lin(B, hgi, hgj, k0), hr, hq, tab.dinv);
+      ring[0][hsy][hsx] = hq[0];
     }
   }
   for(int k = k0; k < k1; k++) {
     int slot = (k - k0) % 3, nslot = (k - k0 + 1) % 3;
-    int kn = mapz(B, k + 1);
-    long long cn = lin(B, gi, gj, kn);
-    prod.eval(cn, raw_next, q_next);
-    m_next = mask[cn];
+    long long cn = lin(B, gi, gj, mapz(B, k + 1));
+    prod.template ev<1>(cn, raw_next, q_next, tab.dinv);
+    ldm<1>(mask, cn, m_next);
     if(k + 1 < k1) {
-      ring[nslot][ty + 1][tx + 1] = q_next;
+      ring[nslot][ty + 1][tx + 1] = q_next[0];
       if(hsx >= 0) {
-        T hr, hq;
-        prod.eval(lin(B, hgi, hgj, k + 1), hr, hq);
-        ring[nslot][hsy][hsx] = hq;
+        prod.template ev<1>(lin(B, hgi, hgj, k + 1), hr, hq, tab.dinv);
+        ring[nslot][hsy][hsx] = hq[0];
       }
     }
     __syncthreads();
     if(valid) {
-      T Aq = op_apply<T>(m_cur, O, q_prev, ring[slot][ty][tx + 1],
-        ring[slot][ty + 1][tx], q_cur, ring[slot][ty + 1][tx + 2],
-        ring[slot][ty + 2][tx + 1], q_next);
-      epi.at(lin(B, i, j, k), raw_cur, Aq, red);
+      T Aq[1];
+      Aq[0] = op_apply<T>(m_cur[0], O, tab.diag[m_cur[0]], q_prev[0],
+        ring[slot][ty][tx + 1], ring[slot][ty + 1][tx], q_cur[0],
+        ring[slot][ty + 1][tx + 2], ring[slot][ty + 2][tx + 1], q_next[0]);
+      epi.template at<1>(lin(B, i, j, k), raw_cur, Aq, red);
     }
-    raw_prev = raw_cur; q_prev = q_cur;
-    raw_cur = raw_next; q_cur = q_next;
-    m_cur = m_next;
+    q_prev[0] = q_cur[0];
+    raw_cur[0] = raw_next[0]; q_cur[0] = q_next[0];
+    m_cur[0] = m_next[0];
   }
-  (void)raw_prev;
 }
 
-template <typename T>
-__device__ __forceinline__ T dinv_of(uint8_t m, const opc &O)
+/* V cells per thread; requires nx % (32 V) == 0 (full tiles in x) */
+template <typename T, int V, class P, class E, int NRED>
+__device__ __forceinline__ void tile_stencilV(const boxc &B, const opc &O,
+  const uint8_t *__restrict__ mask, const optab<T> &tab, P &prod, E &epi,
+  double (&red)[NRED])
 {
-  return (T)(1. / op_diag(m, O));
+  constexpr int W = TX * V;
+  __shared__ __align__(16) T ring[3][HY][W];
+  __shared__ T hw[3][TY], he[3][TY];
+  int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
+  int i0 = blockIdx.x * W, j0 = blockIdx.y * TY;
+  int k0 = blockIdx.z * B.slab, k1 = min(k0 + B.slab, B.nz);
+  int ib = i0 + tx * V, j = j0 + ty;
+  bool valid = j < B.ny;
+  int gj = mapy(B, j);
+  /* halo: two rows of W cells (vectors) and two columns of TY cells */
+  int hrow = -1, hcol = -1, hgi = 0, hgj = 0;
+  if(tid < 64) {
+    hrow = tid < 32 ? 0 : HY - 1;
+    hgi = i0 + (tid & 31) * V;
+    hgj = mapy(B, hrow == 0 ? j0 - 1 : j0 + TY);
+  } else if(tid < 80) {
+    hcol = tid < 72 ? 0 : 1;
+    int r = (tid - 64) & 7;
+    hgi = mapx(B, hcol == 0 ? i0 - 1 : i0 + W);
+    hgj = mapy(B, j0 + r);
+  }
+  T raw_cur[V], raw_next[V], q_prev[V], q_cur[V], q_next[V], tr[V], tq[V];
+  unsigned m_cur[V], m_next[V];
+  prod.template ev<V>(lin(B, ib, gj, mapz(B, k0 - 1)), tr, q_prev, tab.dinv);
+  {
+    long long c = lin(B, ib, gj, k0);
+    prod.template ev<V>(c, raw_cur, q_cur, tab.dinv);
+    ldm<V>(mask, c, m_cur);
+    stv<T, V>(&ring[0][ty + 1][0], tx * V, q_cur);
+    if(hrow >= 0) {
+      prod.template ev<V>(lin(B, hgi, hgj, k0), tr, tq, tab.dinv);
+      stv<T, V>(&ring[0][hrow][0], (tid & 31) * V, tq);
+    } else if(hcol >= 0) {
+      T a[1], bq[1];
+      prod.template ev<1>(lin(B, hgi, hgj, k0), a, bq, tab.dinv);
+      (hcol == 0 ? hw : he)[0][(tid - 64) & 7] = bq[0];
+    }
+  }
+  for(int k = k0; k < k1; k++) {
+    int slot = (k - k0) % 3, nslot = (k - k0 + 1) % 3;
+    long long cn = lin(B, ib, gj, mapz(B, k + 1));
+    prod.template ev<V>(cn, raw_next, q_next, tab.dinv);
+    ldm<V>(mask, cn, m_next);
+    if(k + 1 < k1) {
+      stv<T, V>(&ring[nslot][ty + 1][0], tx * V, q_next);
+      if(hrow >= 0) {
+        prod.template ev<V>(lin(B, hgi, hgj, k + 1), tr, tq, tab.dinv);
+        stv<T, V>(&ring[nslot][hrow][0], (tid & 31) * V, tq);
+      } else if(hcol >= 0) {
+        T a[1], bq[1];
+        prod.template ev<1>(lin(B, hgi, hgj, k + 1), a, bq, tab.dinv);
+        (hcol == 0 ? hw : he)[nslot][(tid - 64) & 7] = bq[0];
+      }
+    }
+    __syncthreads();
+    T left = __shfl_up_sync(0xffffffffu, q_cur[V - 1], 1);
+    T right = __shfl_down_sync(0xffffffffu, q_cur[0], 1);
+    if(tx == 0) left = hw[slot][ty];
+    if(tx == TX - 1) right = he[slot][ty];
+    if(valid) {
+      T S[V], N[V], Aq[V];
+      ldv<T, V>(&ring[slot][ty][0], tx * V, S);
+      ldv<T, V>(&ring[slot][ty + 2][0], tx * V, N);
+#pragma unroll
+      for(int v = 0; v < V; v++) {
+        T qW = v > 0 ? q_cur[v - 1] : left;
+        T qE = v < V - 1 ? q_cur[v + 1] : right;
+        Aq[v] = op_apply<T>(m_cur[v], O, tab.diag[m_cur[v]], q_prev[v], S[v],
+          qW, q_cur[v], qE, N[v], q_next[v]);
+      }
+      epi.template at<V>(lin(B, ib, j, k), raw_cur, Aq, red);
+    }
+#pragma unroll
+    for(int v = 0; v < V; v++) {
+      q_prev[v] = q_cur[v];
+      raw_cur[v] = raw_next[v]; q_cur[v] = q_next[v];
+      m_cur[v] = m_next[v];
+    }
+  }
+}
+
+template <typename T, int V, class P, class E, int NRED>
+__device__ __forceinline__ void tile_stencil(const boxc &B, const opc &O,
+  const uint8_t *__restrict__ mask, const optab<T> &tab, P &prod, E &epi,
+  double (&red)[NRED])
+{
+  if constexpr(V == 1) tile_stencil1<T>(B, O, mask, tab, prod, epi, red);
+  else tile_stencilV<T, V>(B, O, mask, tab, prod, epi, red);
 }
 
 /* ------------------------------------------------ masks */
@@ -266,16 +426,16 @@ void bbb_build_masks(void)
 {
   if(g_dev.masks_valid) return;
   bbb_geom G = bbb_make_geom();
-  k_mask_p<<<1184, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
+  k_mask_p<<<NPW, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
     g_dev.flag_w, g_dev.phase, G, g_dev.mask_p);
   BBB_LAUNCHED();
-  k_mask_face<<<1184, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
+  k_mask_face<<<NPW, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
     g_dev.flag_w, G, 0, G.nx + 1, G.ny, G.nz, g_dev.mask_u);
   BBB_LAUNCHED();
-  k_mask_face<<<1184, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
+  k_mask_face<<<NPW, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
     g_dev.flag_w, G, 1, G.nx, G.ny + 1, G.nz, g_dev.mask_v);
   BBB_LAUNCHED();
-  k_mask_face<<<1184, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
+  k_mask_face<<<NPW, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
     g_dev.flag_w, G, 2, G.nx, G.ny, G.nz + 1, g_dev.mask_w);
   BBB_LAUNCHED();
   g_dev.masks_valid = 1;
@@ -283,36 +443,51 @@ void bbb_build_masks(void)
 
 /* ------------------------------------------------ BiCGSTAB kernels */
 
-/* residual set-up: r = b - A x; rh = r; p = r; (r, r) */
+/* residual set-up: r = b - A x; rh = r; p = r; (r, r), sum x */
 template <typename T>
 struct prod_x {
   const T *x;
-  __device__ __forceinline__ void eval(long long c, T &raw, T &q) const
-  { raw = x[c]; q = raw; }
+  template <int V>
+  __device__ __forceinline__ void ev(long long c, T (&raw)[V], T (&q)[V],
+    const T *dinv) const
+  {
+    ldv<T, V>(x, c, raw);
+#pragma unroll
+    for(int v = 0; v < V; v++) q[v] = raw[v];
+    (void)dinv;
+  }
 };
 template <typename T>
 struct epi_res {
   const T *b; T *r, *rh, *p;
-  __device__ __forceinline__ void at(long long c, T xr, T Ax, double (&red)[2]) const
+  template <int V>
+  __device__ __forceinline__ void at(long long c, const T (&xr)[V],
+    const T (&Ax)[V], double (&red)[2]) const
   {
-    T rv = b[c] - Ax;
-    r[c] = rv; rh[c] = rv; p[c] = rv;
-    red[0] += (double)rv * (double)rv;
-    red[1] += (double)xr;
-    (void)xr;
+    T bb[V], rv[V];
+    ldv<T, V>(b, c, bb);
+#pragma unroll
+    for(int v = 0; v < V; v++) {
+      rv[v] = bb[v] - Ax[v];
+      red[0] += (double)rv[v] * (double)rv[v];
+      red[1] += (double)xr[v];
+    }
+    stv<T, V>(r, c, rv); stv<T, V>(rh, c, rv); stv<T, V>(p, c, rv);
   }
 };
 
-template <typename T>
+template <typename T, int V>
 __global__ void __launch_bounds__(NTHR) k_bicg_setup(boxc B, opc O,
   const uint8_t *__restrict__ mask, const T *__restrict__ b, const T *x,
   T *r, T *rh, T *p, bbb_kry *s, double *partials, double rtol, int maxit)
 {
   __shared__ double sh[32 * 2];
+  __shared__ optab<T> tab;
+  optab_fill<T>(tab, O);
   prod_x<T> P{x};
   epi_res<T> E{b, r, rh, p};
   double red[2] = {0., 0.};
-  tile_stencil<T>(B, O, mask, P, E, red);
+  tile_stencil<T, V>(B, O, mask, tab, P, E, red);
   if(bbb_grid_partial<2>(red, partials, &s->ticket, sh)) {
     bbb_grid_finish_sum<2>(red, partials, &s->ticket, sh);
     if(threadIdx.x == 0 && threadIdx.y == 0) {
@@ -336,26 +511,46 @@ __global__ void __launch_bounds__(NTHR) k_bicg_setup(boxc B, opc O,
 /* p = r + beta p + (-beta omega) v, CUSP's axpbypcz form */
 template <typename T>
 struct prod_k1 {
-  const T *r, *p, *v; const uint8_t *mask; opc O; T beta, bo; int first;
-  __device__ __forceinline__ void eval(long long c, T &raw, T &q) const
+  const T *r, *p, *v; const uint8_t *mask; T beta, bo; int first;
+  template <int V>
+  __device__ __forceinline__ void ev(long long c, T (&raw)[V], T (&q)[V],
+    const T *dinv) const
   {
-    T pn = first ? p[c] : r[c] + beta * p[c] + bo * v[c];
-    raw = pn;
-    q = dinv_of<T>(mask[c], O) * pn;
+    T pp[V];
+    unsigned mm[V];
+    ldv<T, V>(p, c, pp);
+    ldm<V>(mask, c, mm);
+    if(first) {
+#pragma unroll
+      for(int a = 0; a < V; a++) raw[a] = pp[a];
+    } else {
+      T rr[V], vv[V];
+      ldv<T, V>(r, c, rr);
+      ldv<T, V>(v, c, vv);
+#pragma unroll
+      for(int a = 0; a < V; a++) raw[a] = rr[a] + beta * pp[a] + bo * vv[a];
+    }
+#pragma unroll
+    for(int a = 0; a < V; a++) q[a] = dinv[mm[a]] * raw[a];
   }
 };
 template <typename T>
 struct epi_k1 {
   const T *rh; T *pn, *vn;
-  __device__ __forceinline__ void at(long long c, T praw, T Aq, double (&red)[1]) const
+  template <int V>
+  __device__ __forceinline__ void at(long long c, const T (&praw)[V],
+    const T (&Aq)[V], double (&red)[1]) const
   {
-    pn[c] = praw;
-    vn[c] = Aq;
-    red[0] += (double)rh[c] * (double)Aq;
+    T hh[V];
+    ldv<T, V>(rh, c, hh);
+    stv<T, V>(pn, c, praw);
+    stv<T, V>(vn, c, Aq);
+#pragma unroll
+    for(int a = 0; a < V; a++) red[0] += (double)hh[a] * (double)Aq[a];
   }
 };
 
-template <typename T>
+template <typename T, int V>
 __global__ void __launch_bounds__(NTHR) k_bicg1(boxc B, opc O,
   const uint8_t *__restrict__ mask, const T *r, const T *p_old,
   const T *v_old, const T *__restrict__ rh, T *p_new, T *v_new, bbb_kry *s,
@@ -363,11 +558,13 @@ __global__ void __launch_bounds__(NTHR) k_bicg1(boxc B, opc O,
 {
   if(((volatile bbb_kry *)s)->done) return;
   __shared__ double sh[32];
-  prod_k1<T> P{r, p_old, v_old, mask, O, (T)s->beta,
-    (T)(-s->beta * s->omega), s->first};
+  __shared__ optab<T> tab;
+  optab_fill<T>(tab, O);
+  prod_k1<T> P{r, p_old, v_old, mask, (T)s->beta, (T)(-s->beta * s->omega),
+    s->first};
   epi_k1<T> E{rh, p_new, v_new};
   double red[1] = {0.};
-  tile_stencil<T>(B, O, mask, P, E, red);
+  tile_stencil<T, V>(B, O, mask, tab, P, E, red);
   if(bbb_grid_partial<1>(red, partials, &s->ticket, sh)) {
     bbb_grid_finish_sum<1>(red, partials, &s->ticket, sh);
     if(threadIdx.x == 0 && threadIdx.y == 0) {
@@ -379,38 +576,54 @@ __global__ void __launch_bounds__(NTHR) k_bicg1(boxc B, opc O,
 
 template <typename T>
 struct prod_k2 {
-  const T *r, *v; const uint8_t *mask; opc O; T alpha;
-  __device__ __forceinline__ void eval(long long c, T &raw, T &q) const
+  const T *r, *v; const uint8_t *mask; T alpha;
+  template <int V>
+  __device__ __forceinline__ void ev(long long c, T (&raw)[V], T (&q)[V],
+    const T *dinv) const
   {
-    T sv = r[c] - alpha * v[c];
-    raw = sv;
-    q = dinv_of<T>(mask[c], O) * sv;
+    T rr[V], vv[V];
+    unsigned mm[V];
+    ldv<T, V>(r, c, rr);
+    ldv<T, V>(v, c, vv);
+    ldm<V>(mask, c, mm);
+#pragma unroll
+    for(int a = 0; a < V; a++) {
+      raw[a] = rr[a] - alpha * vv[a];
+      q[a] = dinv[mm[a]] * raw[a];
+    }
   }
 };
 template <typename T>
 struct epi_k2 {
   T *sv, *tv;
-  __device__ __forceinline__ void at(long long c, T sraw, T Aq, double (&red)[3]) const
+  template <int V>
+  __device__ __forceinline__ void at(long long c, const T (&sraw)[V],
+    const T (&Aq)[V], double (&red)[3]) const
   {
-    sv[c] = sraw;
-    tv[c] = Aq;
-    red[0] += (double)Aq * (double)sraw;
-    red[1] += (double)Aq * (double)Aq;
-    red[2] += (double)sraw * (double)sraw;
+    stv<T, V>(sv, c, sraw);
+    stv<T, V>(tv, c, Aq);
+#pragma unroll
+    for(int a = 0; a < V; a++) {
+      red[0] += (double)Aq[a] * (double)sraw[a];
+      red[1] += (double)Aq[a] * (double)Aq[a];
+      red[2] += (double)sraw[a] * (double)sraw[a];
+    }
   }
 };
 
-template <typename T>
+template <typename T, int V>
 __global__ void __launch_bounds__(NTHR) k_bicg2(boxc B, opc O,
   const uint8_t *__restrict__ mask, const T *r, const T *v, T *s_out,
   T *t_out, bbb_kry *s, double *partials)
 {
   if(((volatile bbb_kry *)s)->done) return;
   __shared__ double sh[32 * 3];
-  prod_k2<T> P{r, v, mask, O, (T)s->alpha};
+  __shared__ optab<T> tab;
+  optab_fill<T>(tab, O);
+  prod_k2<T> P{r, v, mask, (T)s->alpha};
   epi_k2<T> E{s_out, t_out};
   double red[3] = {0., 0., 0.};
-  tile_stencil<T>(B, O, mask, P, E, red);
+  tile_stencil<T, V>(B, O, mask, tab, P, E, red);
   if(bbb_grid_partial<3>(red, partials, &s->ticket, sh)) {
     bbb_grid_finish_sum<3>(red, partials, &s->ticket, sh);
     if(threadIdx.x == 0 && threadIdx.y == 0) {
@@ -424,8 +637,8 @@ __global__ void __launch_bounds__(NTHR) k_bicg2(boxc B, opc O,
   }
 }
 
-/* pointwise third pass */
-template <typename T>
+/* pointwise third pass, V consecutive unknowns per thread and step */
+template <typename T, int V>
 __global__ void __launch_bounds__(256) k_bicg3(long long n, opc O,
   const uint8_t *__restrict__ mask, T *x, const T *__restrict__ p,
   const T *__restrict__ sv, const T *__restrict__ tv, T *r,
@@ -433,27 +646,43 @@ __global__ void __launch_bounds__(256) k_bicg3(long long n, opc O,
 {
   if(((volatile bbb_kry *)s)->done) return;
   __shared__ double sh[32 * 3];
+  __shared__ optab<T> tab;
+  optab_fill<T>(tab, O);
   double alpha = s->alpha;
   int sconv = s->s_conv;
   double omega = sconv ? 0. : s->t_s / s->t_t;
   T a = (T)alpha, om = (T)omega;
   double red[3] = {0., 0., 0.};
-  for(long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
-      c += (long long)gridDim.x * blockDim.x) {
-    T di = dinv_of<T>(mask[c], O);
-    T xv = x[c];
+  long long nv = n / V;
+  for(long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nv;
+      e += (long long)gridDim.x * blockDim.x) {
+    long long c = e * V;
+    T xv[V], pv[V];
+    unsigned mm[V];
+    ldv<T, V>(x, c, xv);
+    ldv<T, V>(p, c, pv);
+    ldm<V>(mask, c, mm);
     if(sconv) {
-      xv = xv + a * (di * p[c]);
+#pragma unroll
+      for(int q = 0; q < V; q++) xv[q] = xv[q] + a * (tab.dinv[mm[q]] * pv[q]);
     } else {
-      T svv = sv[c];
-      xv = xv + a * (di * p[c]) + om * (di * svv);
-      T rv = svv - om * tv[c];
-      r[c] = rv;
-      red[0] += (double)rh[c] * (double)rv;
-      red[1] += (double)rv * (double)rv;
+      T ss[V], tt[V], hh[V], rv[V];
+      ldv<T, V>(sv, c, ss);
+      ldv<T, V>(tv, c, tt);
+      ldv<T, V>(rh, c, hh);
+#pragma unroll
+      for(int q = 0; q < V; q++) {
+        T di = tab.dinv[mm[q]];
+        xv[q] = xv[q] + a * (di * pv[q]) + om * (di * ss[q]);
+        rv[q] = ss[q] - om * tt[q];
+        red[0] += (double)hh[q] * (double)rv[q];
+        red[1] += (double)rv[q] * (double)rv[q];
+      }
+      stv<T, V>(r, c, rv);
     }
-    x[c] = xv;
-    red[2] += (double)xv;
+    stv<T, V>(x, c, xv);
+#pragma unroll
+    for(int q = 0; q < V; q++) red[2] += (double)xv[q];
   }
   if(bbb_grid_partial<3>(red, partials, &s->ticket, sh)) {
     bbb_grid_finish_sum<3>(red, partials, &s->ticket, sh);
@@ -588,16 +817,17 @@ extern "C" void bbb_profile_get(double *ms, long long *iters, double *bytes)
   *ms = g_prof.ms; *iters = g_prof.iters; *bytes = g_prof.tot_bytes;
 }
 
-/* run iterations until the device says done; host polls in growing
- * batches so that a converged solve costs at most a few no-op launches */
+/* run iterations until the device says done; the host polls the scalars
+ * in growing batches so a converged solve costs at most a few no-op
+ * launches */
 template <typename LaunchIter>
-static int drive(LaunchIter launch_iter, int maxit)
+static int drive(bbb_kry *s, LaunchIter launch_iter, int maxit, int batch0)
 {
-  int batch = 1, total = 0;
+  int batch = batch0, total = 0;
   for(;;) {
-    for(int q = 0; q < batch; q++) launch_iter(total + q);
+    for(int q = 0; q < batch; q++) launch_iter();
     total += batch;
-    BBB_CK(cudaMemcpyAsync(g_dev.kry_host, g_dev.kry, sizeof(bbb_kry),
+    BBB_CK(cudaMemcpyAsync(g_dev.kry_host, s, sizeof(bbb_kry),
       cudaMemcpyDeviceToHost, g_dev.stream));
     BBB_CK(cudaStreamSynchronize(g_dev.stream));
     if(bbb_last_status() == BBB_ERR_CUDA) return -1;
@@ -608,48 +838,77 @@ static int drive(LaunchIter launch_iter, int maxit)
   return g_dev.kry_host->iter;
 }
 
+/* one BiCGSTAB solve on the current (b, x) of the given precision, with
+ * the set-up residual computed by the stencil */
+template <typename T, int V>
+static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
+  const uint8_t *mask, T *r, T *rh, T *p0, T *p1, T *v0, T *v1, T *sv, T *tv,
+  T *x, bbb_kry *s, int maxit, int batch0)
+{
+  dim3 grd = box_grid(B), blk(TX, TY);
+  int npw = NPW;
+  T *pp[2] = {p0, p1}, *vv[2] = {v0, v1};
+  int cur = 0;
+  double it_bytes = (double)n * (17. * sizeof(T) + 3.);
+  drive(s, [&]() {
+    prof_begin(it_bytes);
+    k_bicg1<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, r, pp[cur],
+      vv[cur], rh, pp[cur ^ 1], vv[cur ^ 1], s, g_dev.partials);
+    BBB_LAUNCHED();
+    k_bicg2<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, r, vv[cur ^ 1],
+      sv, tv, s, g_dev.partials);
+    BBB_LAUNCHED();
+    k_bicg3<T, V><<<npw, 256, 0, g_dev.stream>>>(n, O, mask, x, pp[cur ^ 1],
+      sv, tv, r, rh, s, g_dev.partials);
+    BBB_LAUNCHED();
+    prof_end();
+    cur ^= 1;
+  }, maxit, batch0);
+  prof_collect(g_dev.kry_host->iter + (g_dev.kry_host->s_conv ? 1 : 0));
+}
+
+static opc poisson_op(const bbb_geom &G)
+{
+  opc O;
+  O.wx = 1. / (G.dx * G.dx); O.wy = 1. / (G.dy * G.dy); O.wz = 1. / (G.dz * G.dz);
+  O.helm = 0;
+  return O;
+}
+
 int bbb_poisson_solve(int record)
 {
   bbb_dev_require();
   if(!g_dev.ready) return -1;
   bbb_build_masks();
   bbb_geom G = bbb_make_geom();
+  int V = pick_vec(G.nx, sizeof(double));
   boxc B = make_box(G.nx, G.ny, G.nz, bc.pW == BBB_PERIODIC,
-    bc.pS == BBB_PERIODIC, bc.pB == BBB_PERIODIC, 0, 0, 0);
-  opc O;
-  O.wx = 1. / (G.dx * G.dx); O.wy = 1. / (G.dy * G.dy); O.wz = 1. / (G.dz * G.dz);
-  O.helm = 0;
+    bc.pS == BBB_PERIODIC, bc.pB == BBB_PERIODIC, 0, 0, 0, V);
+  opc O = poisson_op(G);
   long long n = (long long)G.nx * G.ny * G.nz;
   bbb_kry *s = g_dev.kry;
-  k_pp_rhs<<<1184, 256, 0, g_dev.stream>>>(g_dev.us, g_dev.vs, g_dev.ws,
+  k_pp_rhs<<<NPW, 256, 0, g_dev.stream>>>(g_dev.us, g_dev.vs, g_dev.ws,
     g_dev.phi, g_dev.phase, G, rho_f / dt, g_dev.kb, g_dev.kx, s, g_dev.partials);
   BBB_LAUNCHED();
   dim3 grd = box_grid(B), blk(TX, TY);
-  k_bicg_setup<double><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
-    g_dev.kb, g_dev.kx, g_dev.kr, g_dev.krh, g_dev.kp[0], s, g_dev.partials,
-    pp_residual, pp_max_iter);
-  BBB_LAUNCHED();
-  int cur = 0;
-  double it_bytes = (double)n * (17. * sizeof(double) + 3.);
-  int it = drive([&](int q) {
-    (void)q;
-    prof_begin(it_bytes);
-    k_bicg1<double><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
-      g_dev.kr, g_dev.kp[cur], g_dev.kv[cur], g_dev.krh, g_dev.kp[cur ^ 1],
-      g_dev.kv[cur ^ 1], s, g_dev.partials);
+  if(V == 2) {
+    k_bicg_setup<double, 2><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
+      g_dev.kb, g_dev.kx, g_dev.kr, g_dev.krh, g_dev.kp[0], s, g_dev.partials,
+      pp_residual, pp_max_iter);
     BBB_LAUNCHED();
-    k_bicg2<double><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
-      g_dev.kr, g_dev.kv[cur ^ 1], g_dev.ks, g_dev.kt, s, g_dev.partials);
+    bicgstab_iterations<double, 2>(B, O, n, g_dev.mask_p, g_dev.kr, g_dev.krh,
+      g_dev.kp[0], g_dev.kp[1], g_dev.kv[0], g_dev.kv[1], g_dev.ks, g_dev.kt,
+      g_dev.kx, s, pp_max_iter, 1);
+  } else {
+    k_bicg_setup<double, 1><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
+      g_dev.kb, g_dev.kx, g_dev.kr, g_dev.krh, g_dev.kp[0], s, g_dev.partials,
+      pp_residual, pp_max_iter);
     BBB_LAUNCHED();
-    k_bicg3<double><<<1184, 256, 0, g_dev.stream>>>(n, O, g_dev.mask_p,
-      g_dev.kx, g_dev.kp[cur ^ 1], g_dev.ks, g_dev.kt, g_dev.kr, g_dev.krh,
-      s, g_dev.partials);
-    BBB_LAUNCHED();
-    prof_end();
-    cur ^= 1;
-  }, pp_max_iter);
-  prof_collect(g_dev.kry_host->iter + (g_dev.kry_host->s_conv ? 1 : 0));
-  k_pp_writeback<<<1184, 256, 0, g_dev.stream>>>(g_dev.kx, g_dev.phi, G, s);
+    bicgstab_iterations<double, 1>(B, O, n, g_dev.mask_p, g_dev.kr, g_dev.krh,
+      g_dev.kp[0], g_dev.kp[1], g_dev.kv[0], g_dev.kv[1], g_dev.ks, g_dev.kt,
+      g_dev.kx, s, pp_max_iter, 1);
+  }
+  k_pp_writeback<<<NPW, 256, 0, g_dev.stream>>>(g_dev.kx, g_dev.phi, G, s);
   BBB_LAUNCHED();
   BBB_CK(cudaMemcpyAsync(g_dev.kry_host, s, sizeof(bbb_kry),
     cudaMemcpyDeviceToHost, g_dev.stream));
@@ -670,7 +929,7 @@ int bbb_poisson_solve(int record)
       exit(EXIT_FAILURE);
     }
   }
-  return it;
+  return h->iter;
 }
 
 /* ------------------------------------------------ mixed precision
@@ -682,30 +941,40 @@ int bbb_poisson_solve(int record)
  * Without particle rows the periodic/Neumann operator is singular; the
  * inner right-hand side is then projected onto zero mean. */
 
-template <typename T>
 struct epi_res64 {
   const double *b; float *rf;
-  __device__ __forceinline__ void at(long long c, double xr, double Ax, double (&red)[3]) const
+  template <int V>
+  __device__ __forceinline__ void at(long long c, const double (&xr)[V],
+    const double (&Ax)[V], double (&red)[3]) const
   {
-    double rv = b[c] - Ax;
-    rf[c] = (float)rv;
-    red[0] += rv * rv;
-    red[1] += xr;
-    red[2] += rv;
+    double bb[V];
+    ldv<double, V>(b, c, bb);
+#pragma unroll
+    for(int a = 0; a < V; a++) {
+      double rv = bb[a] - Ax[a];
+      rf[c + a] = (float)rv;
+      red[0] += rv * rv;
+      red[1] += xr[a];
+      red[2] += rv;
+    }
   }
 };
 
-/* outer residual; finaliser decides convergence and the inner tolerance */
+/* outer residual; the finaliser decides convergence and sets up the inner
+ * solve's tolerance */
+template <int V>
 __global__ void __launch_bounds__(NTHR) k_outer_resid(boxc B, opc O,
   const uint8_t *__restrict__ mask, const double *__restrict__ b,
   const double *x, float *rf, bbb_kry *s, bbb_kry *si, double *partials,
   double inner_tol, int inner_maxit, int project_mean, long long n)
 {
   __shared__ double sh[32 * 3];
+  __shared__ optab<double> tab;
+  optab_fill<double>(tab, O);
   prod_x<double> P{x};
-  epi_res64<double> E{b, rf};
+  epi_res64 E{b, rf};
   double red[3] = {0., 0., 0.};
-  tile_stencil<double>(B, O, mask, P, E, red);
+  tile_stencil<double, V>(B, O, mask, tab, P, E, red);
   if(bbb_grid_partial<3>(red, partials, &s->ticket, sh)) {
     bbb_grid_finish_sum<3>(red, partials, &s->ticket, sh);
     if(threadIdx.x == 0 && threadIdx.y == 0) {
@@ -716,7 +985,6 @@ __global__ void __launch_bounds__(NTHR) k_outer_resid(boxc B, opc O,
       s->s_conv = 0;
       if(!isfinite(rn)) { s->status = BBB_ERR_NONFINITE; s->done = 1; }
       if(s->converged || s->iter >= s->maxit) s->done = 1;
-      /* inner solve set-up scalars */
       double mean = project_mean ? red[2] / (double)n : 0.;
       si->sumx = mean;                 /* subtracted by the inner set-up */
       si->tol = inner_tol * rn;
@@ -727,19 +995,28 @@ __global__ void __launch_bounds__(NTHR) k_outer_resid(boxc B, opc O,
 }
 
 /* inner set-up from e = 0: r = rh = p = rf - mean, e = 0, (r, r) */
-template <typename T>
-__global__ void __launch_bounds__(256) k_inner_setup(long long n, T *rf,
-  T *e, T *rh, T *p, bbb_kry *si, double *partials)
+template <int V>
+__global__ void __launch_bounds__(256) k_inner_setup(long long n, float *rf,
+  float *e, float *rh, float *p, bbb_kry *si, double *partials)
 {
   if(((volatile bbb_kry *)si)->done) return;
   __shared__ double sh[32];
-  T mean = (T)si->sumx;
+  float mean = (float)si->sumx;
   double red[1] = {0.};
-  for(long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
-      c += (long long)gridDim.x * blockDim.x) {
-    T rv = rf[c] - mean;
-    rf[c] = rv; rh[c] = rv; p[c] = rv; e[c] = (T)0.;
-    red[0] += (double)rv * (double)rv;
+  long long nv = n / V;
+  for(long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nv;
+      q += (long long)gridDim.x * blockDim.x) {
+    long long c = q * V;
+    float rv[V], z[V];
+    ldv<float, V>(rf, c, rv);
+#pragma unroll
+    for(int a = 0; a < V; a++) {
+      rv[a] = rv[a] - mean;
+      z[a] = 0.f;
+      red[0] += (double)rv[a] * (double)rv[a];
+    }
+    stv<float, V>(rf, c, rv); stv<float, V>(rh, c, rv); stv<float, V>(p, c, rv);
+    stv<float, V>(e, c, z);
   }
   if(bbb_grid_partial<1>(red, partials, &si->ticket, sh)) {
     bbb_grid_finish_sum<1>(red, partials, &si->ticket, sh);
@@ -758,16 +1035,22 @@ __global__ void __launch_bounds__(256) k_inner_setup(long long n, T *rf,
   }
 }
 
-/* x += e; count the inner iterations into the outer scalars */
+/* x += e */
+template <int V>
 __global__ void __launch_bounds__(256) k_accumulate(long long n, double *x,
-  const float *__restrict__ e, bbb_kry *s, const bbb_kry *si)
+  const float *__restrict__ e, bbb_kry *s)
 {
   if(((volatile bbb_kry *)s)->done) return;
-  for(long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
-      c += (long long)gridDim.x * blockDim.x)
-    x[c] = x[c] + (double)e[c];
+  long long nv = n / V;
+  for(long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nv;
+      q += (long long)gridDim.x * blockDim.x) {
+    long long c = q * V;
+    float ev_[V];
+    ldv<float, V>(e, c, ev_);
+#pragma unroll
+    for(int a = 0; a < V; a++) x[c + a] = x[c + a] + (double)ev_[a];
+  }
   if(blockIdx.x == 0 && threadIdx.x == 0) s->iter += 1;   /* outer sweeps */
-  (void)si;
 }
 
 static void ensure_fp32(void)
@@ -790,12 +1073,13 @@ static void ensure_fp32(void)
 }
 
 /* runs after k_pp_rhs has filled b, x and s->bnorm */
-static int poisson_mixed(const boxc &B, const opc &O, long long n, int record)
+template <int VD, int VF>
+static int poisson_mixed(const boxc &BD, const boxc &BF, const opc &O,
+  long long n, int record)
 {
   ensure_fp32();
   bbb_kry *s = g_dev.kry, *si = g_dev.kry_inner;
-  dim3 grd = box_grid(B), blk(TX, TY);
-  /* outer scalars: tol, iteration counters */
+  dim3 grdD = box_grid(BD), blk(TX, TY);
   bbb_kry init;
   memset(&init, 0, sizeof(init));
   BBB_CK(cudaMemcpyAsync(g_dev.kry_host, s, sizeof(bbb_kry),
@@ -811,44 +1095,19 @@ static int poisson_mixed(const boxc &B, const opc &O, long long n, int record)
   double itol = g_opt.inner_tol > 0 ? g_opt.inner_tol : 1e-4;
   int inner_total = 0;
   for(int outer = 0; outer <= init.maxit; outer++) {
-    k_outer_resid<<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p, g_dev.kb,
-      g_dev.kx, g_dev.fb, s, si, g_dev.partials, itol, pp_max_iter, project, n);
+    k_outer_resid<VD><<<grdD, blk, 0, g_dev.stream>>>(BD, O, g_dev.mask_p,
+      g_dev.kb, g_dev.kx, g_dev.fb, s, si, g_dev.partials, itol, pp_max_iter,
+      project, n);
     BBB_LAUNCHED();
-    k_inner_setup<float><<<1184, 256, 0, g_dev.stream>>>(n, g_dev.fb, g_dev.fx,
+    k_inner_setup<VF><<<NPW, 256, 0, g_dev.stream>>>(n, g_dev.fb, g_dev.fx,
       g_dev.frh, g_dev.fp[0], si, g_dev.partials);
     BBB_LAUNCHED();
-    int cur = 0;
-    /* the inner loop polls the inner scalars */
-    int batch = 4, total = 0;
-    double it_bytes = (double)n * (17. * sizeof(float) + 3.);
-    for(;;) {
-      for(int q = 0; q < batch; q++) {
-        prof_begin(it_bytes);
-        k_bicg1<float><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
-          g_dev.fb, g_dev.fp[cur], g_dev.fv[cur], g_dev.frh, g_dev.fp[cur ^ 1],
-          g_dev.fv[cur ^ 1], si, g_dev.partials);
-        BBB_LAUNCHED();
-        k_bicg2<float><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
-          g_dev.fb, g_dev.fv[cur ^ 1], g_dev.fs, g_dev.ft, si, g_dev.partials);
-        BBB_LAUNCHED();
-        k_bicg3<float><<<1184, 256, 0, g_dev.stream>>>(n, O, g_dev.mask_p,
-          g_dev.fx, g_dev.fp[cur ^ 1], g_dev.fs, g_dev.ft, g_dev.fb, g_dev.frh,
-          si, g_dev.partials);
-        BBB_LAUNCHED();
-        prof_end();
-        cur ^= 1;
-      }
-      total += batch;
-      BBB_CK(cudaMemcpyAsync(g_dev.kry_host, si, sizeof(bbb_kry),
-        cudaMemcpyDeviceToHost, g_dev.stream));
-      BBB_CK(cudaStreamSynchronize(g_dev.stream));
-      if(bbb_last_status() == BBB_ERR_CUDA) return -1;
-      if(g_dev.kry_host->done || total > pp_max_iter + 4) break;
-      if(batch < 16) batch *= 2;
-    }
-    prof_collect(g_dev.kry_host->iter + (g_dev.kry_host->s_conv ? 1 : 0));
+    bicgstab_iterations<float, VF>(BF, O, n, g_dev.mask_p, g_dev.fb, g_dev.frh,
+      g_dev.fp[0], g_dev.fp[1], g_dev.fv[0], g_dev.fv[1], g_dev.fs, g_dev.ft,
+      g_dev.fx, si, pp_max_iter, 4);
+    if(bbb_last_status() == BBB_ERR_CUDA) return -1;
     inner_total += g_dev.kry_host->iter;
-    k_accumulate<<<1184, 256, 0, g_dev.stream>>>(n, g_dev.kx, g_dev.fx, s, si);
+    k_accumulate<VF><<<NPW, 256, 0, g_dev.stream>>>(n, g_dev.kx, g_dev.fx, s);
     BBB_LAUNCHED();
     BBB_CK(cudaMemcpyAsync(g_dev.kry_host, s, sizeof(bbb_kry),
       cudaMemcpyDeviceToHost, g_dev.stream));
@@ -872,18 +1131,21 @@ int bbb_poisson_solve_mixed(int record)
   if(!g_dev.ready) return -1;
   bbb_build_masks();
   bbb_geom G = bbb_make_geom();
-  boxc B = make_box(G.nx, G.ny, G.nz, bc.pW == BBB_PERIODIC,
-    bc.pS == BBB_PERIODIC, bc.pB == BBB_PERIODIC, 0, 0, 0);
-  opc O;
-  O.wx = 1. / (G.dx * G.dx); O.wy = 1. / (G.dy * G.dy); O.wz = 1. / (G.dz * G.dz);
-  O.helm = 0;
+  int VD = pick_vec(G.nx, sizeof(double)), VF = pick_vec(G.nx, sizeof(float));
+  int px = bc.pW == BBB_PERIODIC, py = bc.pS == BBB_PERIODIC, pz = bc.pB == BBB_PERIODIC;
+  boxc BD = make_box(G.nx, G.ny, G.nz, px, py, pz, 0, 0, 0, VD);
+  boxc BF = make_box(G.nx, G.ny, G.nz, px, py, pz, 0, 0, 0, VF);
+  opc O = poisson_op(G);
   long long n = (long long)G.nx * G.ny * G.nz;
-  k_pp_rhs<<<1184, 256, 0, g_dev.stream>>>(g_dev.us, g_dev.vs, g_dev.ws,
+  k_pp_rhs<<<NPW, 256, 0, g_dev.stream>>>(g_dev.us, g_dev.vs, g_dev.ws,
     g_dev.phi, g_dev.phase, G, rho_f / dt, g_dev.kb, g_dev.kx, g_dev.kry,
     g_dev.partials);
   BBB_LAUNCHED();
-  int it = poisson_mixed(B, O, n, record);
-  k_pp_writeback<<<1184, 256, 0, g_dev.stream>>>(g_dev.kx, g_dev.phi, G, g_dev.kry);
+  int it;
+  if(VD == 2 && VF == 4) it = poisson_mixed<2, 4>(BD, BF, O, n, record);
+  else if(VD == 2 && VF == 1) it = poisson_mixed<2, 1>(BD, BF, O, n, record);
+  else it = poisson_mixed<1, 1>(BD, BF, O, n, record);
+  k_pp_writeback<<<NPW, 256, 0, g_dev.stream>>>(g_dev.kx, g_dev.phi, G, g_dev.kry);
   BBB_LAUNCHED();
   bbb_kry *h = g_dev.kry_host;
   if(h->status == BBB_ERR_NONFINITE) bbb_set_status(BBB_ERR_NONFINITE, "pressure-Poisson");
@@ -913,7 +1175,7 @@ extern "C" void cuda_PP_rhs(int dev)
   bbb_dev_require();
   if(!g_dev.ready) return;
   bbb_geom G = bbb_make_geom();
-  k_pp_rhs<<<1184, 256, 0, g_dev.stream>>>(g_dev.us, g_dev.vs, g_dev.ws,
+  k_pp_rhs<<<NPW, 256, 0, g_dev.stream>>>(g_dev.us, g_dev.vs, g_dev.ws,
     g_dev.phi, g_dev.phase, G, rho_f / dt, g_dev.kb, g_dev.kx, g_dev.kry,
     g_dev.partials);
   BBB_LAUNCHED();
@@ -923,36 +1185,55 @@ extern "C" void cuda_PP_rhs(int dev)
 
 template <typename T>
 struct prod_c1 {
-  const T *r, *p; const uint8_t *mask; opc O; T beta; int first;
-  __device__ __forceinline__ void eval(long long c, T &raw, T &q) const
+  const T *r, *p; const uint8_t *mask; T beta; int first;
+  template <int V>
+  __device__ __forceinline__ void ev(long long c, T (&raw)[V], T (&q)[V],
+    const T *dinv) const
   {
-    T pn = first ? p[c] : (T)1. * (dinv_of<T>(mask[c], O) * r[c]) + beta * p[c];
-    raw = pn;
-    q = pn;
+    T pp[V];
+    ldv<T, V>(p, c, pp);
+    if(first) {
+#pragma unroll
+      for(int a = 0; a < V; a++) raw[a] = pp[a];
+    } else {
+      T rr[V];
+      unsigned mm[V];
+      ldv<T, V>(r, c, rr);
+      ldm<V>(mask, c, mm);
+#pragma unroll
+      for(int a = 0; a < V; a++) raw[a] = (T)1. * (dinv[mm[a]] * rr[a]) + beta * pp[a];
+    }
+#pragma unroll
+    for(int a = 0; a < V; a++) q[a] = raw[a];
   }
 };
 template <typename T>
 struct epi_c1 {
   T *pn, *y;
-  __device__ __forceinline__ void at(long long c, T praw, T Ap, double (&red)[1]) const
+  template <int V>
+  __device__ __forceinline__ void at(long long c, const T (&praw)[V],
+    const T (&Ap)[V], double (&red)[1]) const
   {
-    pn[c] = praw;
-    y[c] = Ap;
-    red[0] += (double)Ap * (double)praw;
+    stv<T, V>(pn, c, praw);
+    stv<T, V>(y, c, Ap);
+#pragma unroll
+    for(int a = 0; a < V; a++) red[0] += (double)Ap[a] * (double)praw[a];
   }
 };
 
-template <typename T>
+template <typename T, int V>
 __global__ void __launch_bounds__(NTHR) k_cg1(boxc B, opc O,
   const uint8_t *__restrict__ mask, const T *r, const T *p_old, T *p_new,
   T *y, bbb_kry *s, double *partials)
 {
   if(((volatile bbb_kry *)s)->done) return;
   __shared__ double sh[32];
-  prod_c1<T> P{r, p_old, mask, O, (T)s->beta, s->first};
+  __shared__ optab<T> tab;
+  optab_fill<T>(tab, O);
+  prod_c1<T> P{r, p_old, mask, (T)s->beta, s->first};
   epi_c1<T> E{p_new, y};
   double red[1] = {0.};
-  tile_stencil<T>(B, O, mask, P, E, red);
+  tile_stencil<T, V>(B, O, mask, tab, P, E, red);
   if(bbb_grid_partial<1>(red, partials, &s->ticket, sh)) {
     bbb_grid_finish_sum<1>(red, partials, &s->ticket, sh);
     if(threadIdx.x == 0 && threadIdx.y == 0) {
@@ -969,6 +1250,8 @@ __global__ void __launch_bounds__(256) k_cg2(long long n, opc O,
 {
   if(((volatile bbb_kry *)s)->done) return;
   __shared__ double sh[32 * 2];
+  __shared__ optab<T> tab;
+  optab_fill<T>(tab, O);
   T a = (T)s->alpha;
   double red[2] = {0., 0.};
   for(long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
@@ -977,7 +1260,7 @@ __global__ void __launch_bounds__(256) k_cg2(long long n, opc O,
     x[c] = a * pv + x[c];
     T rv = -a * y[c] + r[c];
     r[c] = rv;
-    T z = dinv_of<T>(mask[c], O) * rv;
+    T z = tab.dinv[mask[c]] * rv;
     red[0] += (double)rv * (double)z;
     red[1] += (double)rv * (double)rv;
   }
@@ -1002,6 +1285,8 @@ __global__ void k_cg_setup(const real *star, bbb_geom G, int comp, int nx,
   double *p, bbb_kry *s, double *partials, double rtol, int maxit)
 {
   __shared__ double sh[32 * 2];
+  __shared__ optab<double> tab;
+  optab_fill<double>(tab, O);
   int s1 = comp == 0 ? G.fx_s1 : (comp == 1 ? G.fy_s1 : G.fz_s1);
   int s2 = comp == 0 ? G.fx_s2 : (comp == 1 ? G.fy_s2 : G.fz_s2);
   long long n = (long long)nx * ny * nz;
@@ -1014,7 +1299,7 @@ __global__ void k_cg_setup(const real *star, bbb_geom G, int comp, int nx,
     double bv = star[i + (long long)j * s1 + (long long)k * s2];
     x[t] = 0.;
     r[t] = bv;
-    double z = dinv_of<double>(mask[t], O) * bv;
+    double z = tab.dinv[mask[t]] * bv;
     p[t] = z;
     red[0] += bv * z;
     red[1] += bv * bv;
@@ -1061,9 +1346,10 @@ int bbb_helmholtz_solve(int comp)
   bbb_geom G = bbb_make_geom();
   int nx = G.nx + (comp == 0), ny = G.ny + (comp == 1), nz = G.nz + (comp == 2);
   int per[3][3] = {{bc.uW, bc.uS, bc.uB}, {bc.vW, bc.vS, bc.vB}, {bc.wW, bc.wS, bc.wB}};
+  int V = pick_vec(nx, sizeof(double));
   boxc B = make_box(nx, ny, nz, per[comp][0] == BBB_PERIODIC,
     per[comp][1] == BBB_PERIODIC, per[comp][2] == BBB_PERIODIC,
-    comp == 0, comp == 1, comp == 2);
+    comp == 0, comp == 1, comp == 2, V);
   opc O;
   O.wx = 0.5 * nu * dt * (1. / (G.dx * G.dx));
   O.wy = 0.5 * nu * dt * (1. / (G.dy * G.dy));
@@ -1073,23 +1359,26 @@ int bbb_helmholtz_solve(int comp)
   real *star = comp == 0 ? g_dev.us : (comp == 1 ? g_dev.vs : g_dev.ws);
   long long n = (long long)nx * ny * nz;
   bbb_kry *s = g_dev.kry;
-  k_cg_setup<<<1184, 256, 0, g_dev.stream>>>(star, G, comp, nx, ny, nz, O,
+  k_cg_setup<<<NPW, 256, 0, g_dev.stream>>>(star, G, comp, nx, ny, nz, O,
     mask, g_dev.kx, g_dev.kr, g_dev.kp[0], s, g_dev.partials, pp_residual,
     pp_max_iter);
   BBB_LAUNCHED();
   dim3 grd = box_grid(B), blk(TX, TY);
   int cur = 0;
-  int it = drive([&](int q) {
-    (void)q;
-    k_cg1<double><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, g_dev.kr,
-      g_dev.kp[cur], g_dev.kp[cur ^ 1], g_dev.kv[0], s, g_dev.partials);
+  drive(s, [&]() {
+    if(V == 2)
+      k_cg1<double, 2><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, g_dev.kr,
+        g_dev.kp[cur], g_dev.kp[cur ^ 1], g_dev.kv[0], s, g_dev.partials);
+    else
+      k_cg1<double, 1><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, g_dev.kr,
+        g_dev.kp[cur], g_dev.kp[cur ^ 1], g_dev.kv[0], s, g_dev.partials);
     BBB_LAUNCHED();
-    k_cg2<double><<<1184, 256, 0, g_dev.stream>>>(n, O, mask, g_dev.kx,
+    k_cg2<double><<<NPW, 256, 0, g_dev.stream>>>(n, O, mask, g_dev.kx,
       g_dev.kp[cur ^ 1], g_dev.kr, g_dev.kv[0], s, g_dev.partials);
     BBB_LAUNCHED();
     cur ^= 1;
-  }, pp_max_iter);
-  k_cg_writeback<<<1184, 256, 0, g_dev.stream>>>(g_dev.kx, star, G, comp,
+  }, pp_max_iter, 1);
+  k_cg_writeback<<<NPW, 256, 0, g_dev.stream>>>(g_dev.kx, star, G, comp,
     nx, ny, nz);
   BBB_LAUNCHED();
   bbb_kry *h = g_dev.kry_host;
@@ -1103,7 +1392,7 @@ int bbb_helmholtz_solve(int comp)
       exit(EXIT_FAILURE);
     }
   }
-  return it;
+  return h->iter;
 }
 
 /* src/cuda_bicgstab.cu:44-316 (and the v, w variants): RHS, boundary
@@ -1144,6 +1433,37 @@ static __device__ __align__(256) unsigned char
 /* device address of g_static_scratch per device, looked up once with that
  * device current */
 static unsigned char *g_static_addr[64];
+
+template <int V>
+static int static_iterations(const boxc &B, const opc &O, long long n,
+  const uint8_t *mask, double *b, double *x, double *r, double *rh,
+  double *const *pp, double *const *vv, double *sv, double *tv, bbb_kry *s,
+  double *partials, double tol, int maxit, cudaStream_t st, bbb_kry *h)
+{
+  dim3 grd = box_grid(B), blk(TX, TY);
+  k_bicg_setup<double, V><<<grd, blk, 0, st>>>(B, O, mask, b, x, r, rh, pp[0],
+    s, partials, tol, maxit);
+  if(cudaPeekAtLastError() != cudaSuccess) return BBB_ERR_CUDA;
+  int cur = 0, batch = 1, total = 0;
+  for(;;) {
+    for(int q = 0; q < batch; q++) {
+      k_bicg1<double, V><<<grd, blk, 0, st>>>(B, O, mask, r, pp[cur], vv[cur],
+        rh, pp[cur ^ 1], vv[cur ^ 1], s, partials);
+      k_bicg2<double, V><<<grd, blk, 0, st>>>(B, O, mask, r, vv[cur ^ 1], sv,
+        tv, s, partials);
+      k_bicg3<double, V><<<NPW, 256, 0, st>>>(n, O, mask, x, pp[cur ^ 1], sv,
+        tv, r, rh, s, partials);
+      cur ^= 1;
+    }
+    total += batch;
+    if(cudaMemcpyAsync(h, s, sizeof(bbb_kry), cudaMemcpyDeviceToHost, st)
+      != cudaSuccess) return BBB_ERR_CUDA;
+    if(cudaStreamSynchronize(st) != cudaSuccess) return BBB_ERR_CUDA;
+    if(h->done || total > maxit + 4) break;
+    if(batch < 16) batch *= 2;
+  }
+  return BBB_OK;
+}
 
 extern "C" int bbb_PP_bicgstab_static(int nx, int ny, int nz, double dx,
   double dy, double dz, int perx, int pery, int perz, const double *u_star_d,
@@ -1189,40 +1509,26 @@ extern "C" int bbb_PP_bicgstab_static(int nx, int ny, int nz, double dx,
   G.fy_s1 = nx + 2; G.fy_s2 = (nx + 2) * (ny + 3);
   G.fz_s1 = nx + 2; G.fz_s2 = (nx + 2) * (ny + 2);
   G.dx = dx; G.dy = dy; G.dz = dz;
-  boxc B = make_box(nx, ny, nz, perx, pery, perz, 0, 0, 0);
-  dim3 grd = box_grid(B), blk(TX, TY);
+  int V = pick_vec(nx, sizeof(double));
+  boxc B = make_box(nx, ny, nz, perx, pery, perz, 0, 0, 0, V);
+  dim3 grd = box_grid(B);
   if((long long)grd.x * grd.y * grd.z > BBB_STATIC_PARTIALS / 4) return BBB_ERR_TOO_LARGE;
   opc O;
   O.wx = 1. / (dx * dx); O.wy = 1. / (dy * dy); O.wz = 1. / (dz * dz);
   O.helm = 0;
   /* the reduction ticket and the scalars start from zero on every call */
   if(cudaMemsetAsync(s, 0, sizeof(bbb_kry), st) != cudaSuccess) return BBB_ERR_CUDA;
-  k_mask_p<<<1184, 256, 0, st>>>(flag_u_d, flag_v_d, flag_w_d, phase_d, G, mask);
-  k_pp_rhs<<<1184, 256, 0, st>>>(u_star_d, v_star_d, w_star_d, phi_d, phase_d,
+  k_mask_p<<<NPW, 256, 0, st>>>(flag_u_d, flag_v_d, flag_w_d, phase_d, G, mask);
+  k_pp_rhs<<<NPW, 256, 0, st>>>(u_star_d, v_star_d, w_star_d, phi_d, phase_d,
     G, rho_f_ / dt_, b, x, s, partials);
-  k_bicg_setup<double><<<grd, blk, 0, st>>>(B, O, mask, b, x, r, rh, pp[0],
-    s, partials, tol, maxit);
-  if(cudaPeekAtLastError() != cudaSuccess) return BBB_ERR_CUDA;
   bbb_kry h;
-  int cur = 0, batch = 1, total = 0;
-  for(;;) {
-    for(int q = 0; q < batch; q++) {
-      k_bicg1<double><<<grd, blk, 0, st>>>(B, O, mask, r, pp[cur], vv[cur], rh,
-        pp[cur ^ 1], vv[cur ^ 1], s, partials);
-      k_bicg2<double><<<grd, blk, 0, st>>>(B, O, mask, r, vv[cur ^ 1], sv, tv,
-        s, partials);
-      k_bicg3<double><<<1184, 256, 0, st>>>(n, O, mask, x, pp[cur ^ 1], sv, tv,
-        r, rh, s, partials);
-      cur ^= 1;
-    }
-    total += batch;
-    if(cudaMemcpyAsync(&h, s, sizeof(bbb_kry), cudaMemcpyDeviceToHost, st)
-      != cudaSuccess) return BBB_ERR_CUDA;
-    if(cudaStreamSynchronize(st) != cudaSuccess) return BBB_ERR_CUDA;
-    if(h.done || total > maxit + 4) break;
-    if(batch < 16) batch *= 2;
-  }
-  k_pp_writeback<<<1184, 256, 0, st>>>(x, phi_d, G, s);
+  int rc = V == 2
+    ? static_iterations<2>(B, O, n, mask, b, x, r, rh, pp, vv, sv, tv, s,
+        partials, tol, maxit, st, &h)
+    : static_iterations<1>(B, O, n, mask, b, x, r, rh, pp, vv, sv, tv, s,
+        partials, tol, maxit, st, &h);
+  if(rc != BBB_OK) return rc;
+  k_pp_writeback<<<NPW, 256, 0, st>>>(x, phi_d, G, s);
   if(cudaMemcpyAsync(&h, s, sizeof(bbb_kry), cudaMemcpyDeviceToHost, st)
     != cudaSuccess) return BBB_ERR_CUDA;
   if(cudaStreamSynchronize(st) != cudaSuccess) return BBB_ERR_CUDA;
