@@ -1,0 +1,114 @@
+"""Host-side logic of the library without a GPU: the reference's input
+readers (src/domain.c:30-730, src/particle.c:79-159), the derived domain
+set-up, the seeded sphere pack and the gravity balance."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from bluebottle_b200 import Sim, configs, abi
+
+
+def _dir_sim(tmp_path, parts, **flow):
+    d = str(tmp_path)
+    configs.write_flow_config(os.path.join(d, "flow.config"), **flow)
+    configs.write_part_config(os.path.join(d, "part.config"), parts)
+    return Sim(input_dir=d)
+
+
+def test_flow_and_part_config_round_trip(tmp_path):
+    sim = _dir_sim(tmp_path,
+                   [dict(r=0.5, x=0.25, y=0.5, z=0.75, rho=3.0, order=3, rsr=1.3),
+                    dict(r=0.4, x=1.0, y=0.2, z=0.4)],
+                   n=(12, 10, 8), lo=(-0.6, 0.0, 0.0), hi=(0.6, 1.0, 0.8),
+                   nu=0.25, rho_f=2.0, pp_residual=1e-9, pp_max_iter=321,
+                   lamb_max_iter=7, lamb_residual=1e-3, lamb_relax=0.9,
+                   lamb_cut=1e-5, periodic=(True, False, True),
+                   gradP=(0.1, -0.2, 0.3), g=(0.0, 0.0, -9.8))
+    d = sim.dom
+    assert (d.xn, d.yn, d.zn) == (12, 10, 8)
+    assert math.isclose(d.dx, 0.1) and math.isclose(d.dy, 0.1) and math.isclose(d.dz, 0.1)
+    assert math.isclose(d.xs, -0.6) and math.isclose(d.xe, 0.6)
+    # ghosted grids: one ghost layer, Gfx one face more along x
+    assert d.Gcc.inb == 14 and d.Gfx.inb == 15 and d.Gfy.jnb == 13 and d.Gfz.knb == 11
+    assert d.Gcc.s1b == d.Gcc.inb and d.Gcc.s2b == d.Gcc.inb * d.Gcc.jnb
+    assert sim.scalar("nu") == 0.25 and sim.scalar("rho_f") == 2.0
+    assert math.isclose(sim.scalar("mu"), 0.5)
+    assert sim.scalar("pp_residual") == 1e-9 and sim.scalar("pp_max_iter") == 321
+    assert sim.scalar("lamb_max_iter") == 7
+    assert sim.scalar("lamb_relax") == 0.9 and sim.scalar("lamb_cut") == 1e-5
+    bc = sim.bc
+    assert bc.pW == 0 and bc.pE == 0 and bc.pB == 0          # PERIODIC
+    assert bc.pS == 2 and bc.pN == 2                          # NEUMANN
+    assert bc.uS == 1 and bc.vN == 1 and bc.wS == 1           # DIRICHLET
+    assert sim.gradP.xm == 0.1 and sim.gradP.ym == -0.2 and sim.gradP.zm == 0.3
+    assert sim.g.zm == -9.8
+    assert sim.nparts == 2
+    p = sim.parts()
+    assert (p[0].r, p[0].x, p[0].y, p[0].z, p[0].rho, p[0].order) == (0.5, 0.25, 0.5, 0.75, 3.0, 3)
+    assert math.isclose(p[1].r, 0.4)
+    # coefficient storage: the largest order sets the stride,
+    # (order+1)(order+2)/2 modes (src/particle.c)
+    assert sim.scalar("coeff_stride") == (3 + 1) * (3 + 2) // 2 or \
+        sim.scalar("coeff_stride") == (4 + 1) * (4 + 2) // 2
+    sim.close()
+
+
+def _pair_gaps(x, L):
+    d = x[:, None, :] - x[None, :, :]
+    d -= L * np.round(d / L)
+    r = np.sqrt((d ** 2).sum(-1))
+    r[np.diag_indices(len(x))] = np.inf
+    return r
+
+
+def test_seeded_pack_reproducible_and_gapped():
+    wl = configs.sedimentation((32, 32, 32), (16.0, 16.0, 16.0), 60, seed=9)
+    sims = []
+    pos = []
+    for _ in range(2):
+        s = Sim(wl)
+        pos.append(np.array([(q.x, q.y, q.z) for q in s.parts()]))
+        L = np.array([s.dom.xl, s.dom.yl, s.dom.zl])
+        s.close()
+    assert pos[0].shape == (60, 3)
+    assert np.array_equal(pos[0], pos[1])
+    r = _pair_gaps(pos[0], L)
+    assert r.min() >= 2.0 + 0.1 - 1e-12          # surface gap >= 0.1 a
+    assert np.all(pos[0] >= 0) and np.all(pos[0] < L)
+    other = Sim(configs.sedimentation((32, 32, 32), (16.0, 16.0, 16.0), 60, seed=10))
+    p2 = np.array([(q.x, q.y, q.z) for q in other.parts()])
+    other.close()
+    assert not np.array_equal(pos[0], p2)
+
+
+def test_gravity_balance_sets_mean_excess_weight():
+    wl = configs.sedimentation((32, 32, 32), (16.0, 16.0, 16.0), 20, seed=2)
+    s = Sim(wl)
+    vol = 4.0 / 3.0 * math.pi
+    expect = 20 * (2.0 - 1.0) * vol * (-1.0) / 16.0 ** 3
+    assert math.isclose(s.gradP.zm, expect, rel_tol=1e-12)
+    s.close()
+
+
+def test_too_dense_pack_reports_config_error():
+    wl = configs.sedimentation((16, 16, 16), (4.0, 4.0, 4.0), 50, seed=1)
+    with pytest.raises(Exception):
+        Sim(wl)
+
+
+def test_options_round_trip():
+    import ctypes as C
+    lib = abi.load()
+    o = abi.Options()
+    lib.bbb_default_options(C.byref(o))
+    assert o.implicit == 1 and o.precision == 0
+    o.precision = 1
+    o.inner_tol = 3e-6
+    lib.bbb_set_options(C.byref(o))
+    g = abi.Options()
+    lib.bbb_get_options(C.byref(g))
+    assert g.precision == 1 and g.inner_tol == 3e-6
+    lib.bbb_default_options(C.byref(o))
+    lib.bbb_set_options(C.byref(o))
