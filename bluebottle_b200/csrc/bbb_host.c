@@ -369,7 +369,7 @@ int bbb_read_input(const char *dir)
  * src/domain.c:1591-2347: grid_info index spaces (one ghost layer), the
  * host field arrays, QUIESCENT / SHEAR / CHANNEL starts and the initial
  * dt. */
-static void set_grid(grid_info *G, int nx, int ny, int nz)
+static void set_grid(grid_info *G, int nx, int ny, int nz, int local)
 {
   G->is = BBB_DOM_BUF; G->isb = G->is - BBB_DOM_BUF; G->in = nx;
   G->inb = G->in + 2 * BBB_DOM_BUF; G->ie = G->is + G->in; G->ieb = G->ie + BBB_DOM_BUF;
@@ -379,7 +379,9 @@ static void set_grid(grid_info *G, int nx, int ny, int nz)
   G->knb = G->kn + 2 * BBB_DOM_BUF; G->ke = G->ks + G->kn; G->keb = G->ke + BBB_DOM_BUF;
   G->s1 = G->in; G->s2 = G->s1 * G->jn; G->s3 = G->s2 * G->kn;
   G->s1b = G->inb; G->s2b = G->s1b * G->jnb; G->s3b = G->s2b * G->knb;
-  /* one subdomain: the device copies equal the global ones */
+  /* the subdomain's own (underscored) indices are filled for dom[] only,
+   * as src/domain.c:1777 does; with one subdomain they equal the global */
+  if(!local) return;
   G->_is = G->is; G->_ie = G->ie; G->_in = G->in; G->_isb = G->isb;
   G->_ieb = G->ieb; G->_inb = G->inb;
   G->_js = G->js; G->_je = G->je; G->_jn = G->jn; G->_jsb = G->jsb;
@@ -390,14 +392,14 @@ static void set_grid(grid_info *G, int nx, int ny, int nz)
   G->_s3 = G->s3; G->_s3b = G->s3b;
 }
 
-static void setup_dom(dom_struct *d)
+static void setup_dom(dom_struct *d, int local)
 {
   d->xl = d->xe - d->xs; d->yl = d->ye - d->ys; d->zl = d->ze - d->zs;
   d->dx = d->xl / d->xn; d->dy = d->yl / d->yn; d->dz = d->zl / d->zn;
-  set_grid(&d->Gcc, d->xn, d->yn, d->zn);
-  set_grid(&d->Gfx, d->xn + 1, d->yn, d->zn);
-  set_grid(&d->Gfy, d->xn, d->yn + 1, d->zn);
-  set_grid(&d->Gfz, d->xn, d->yn, d->zn + 1);
+  set_grid(&d->Gcc, d->xn, d->yn, d->zn, local);
+  set_grid(&d->Gfx, d->xn + 1, d->yn, d->zn, local);
+  set_grid(&d->Gfy, d->xn, d->yn + 1, d->zn, local);
+  set_grid(&d->Gfz, d->xn, d->yn, d->zn + 1, local);
 }
 
 static real *zalloc(long n)
@@ -423,8 +425,8 @@ int bbb_domain_init(void)
     bbb_set_status(BBB_ERR_STATE, "bbb_domain_init before bbb_read_input");
     return BBB_ERR_STATE;
   }
-  setup_dom(&Dom);
-  setup_dom(&dom[0]);
+  setup_dom(&Dom, 0);
+  setup_dom(&dom[0], 1);
   free_fields();
   long ncc = Dom.Gcc.s3b, nfx = Dom.Gfx.s3b, nfy = Dom.Gfy.s3b,
        nfz = Dom.Gfz.s3b;
@@ -760,6 +762,7 @@ int bbb_prepare(void)
   cuda_dom_BC();
   cuda_parts_internal();
   cuda_dom_BC();
+  if(g_opt.learned_guess) bbb_learn_enable(g_opt.learned_guess);
   return bbb_last_status();
 }
 

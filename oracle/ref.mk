@@ -1,0 +1,35 @@
+# Builds the reference's own host set-up code (input readers, domain and
+# particle initialisation: src/domain.c, src/particle.c, src/rng.c) from the
+# reference tree, unmodified, into oracle/_ref/libref_host.so.  The process
+# globals normally defined in src/bluebottle.c (which needs MPI) come from a
+# translation unit generated from the reference headers' extern
+# declarations by oracle/ref_shim.py; src/recorder.h's CGNS include is met
+# by an empty stub header.  Test infrastructure only.
+#
+#   make -f oracle/ref.mk REF=/path/to/reference/src
+REF ?= /root/reference/src
+HERE := $(dir $(lastword $(MAKEFILE_LIST)))
+OUT := $(HERE)_ref
+CC = gcc
+CFLAGS = -std=gnu99 -O2 -fPIC -fopenmp -DDOUBLE -w -I$(OUT) -I$(REF)
+
+all: $(OUT)/libref_host.so
+
+$(OUT)/cgnslib.h:
+	mkdir -p $(OUT)
+	: > $@
+
+$(OUT)/ref_globals.c: $(HERE)ref_shim.py | $(OUT)/cgnslib.h
+	python3 $(HERE)ref_shim.py $(REF) $@
+
+$(OUT)/%.o: $(REF)/%.c $(OUT)/cgnslib.h
+	$(CC) $(CFLAGS) -c $< -o $@
+
+$(OUT)/ref_globals.o: $(OUT)/ref_globals.c
+	$(CC) $(CFLAGS) -c $< -o $@
+
+$(OUT)/libref_host.so: $(OUT)/domain.o $(OUT)/particle.o $(OUT)/rng.o $(OUT)/ref_globals.o
+	$(CC) -shared -fopenmp -o $@ $^ -lm -Wl,--no-undefined
+
+clean:
+	rm -f $(OUT)/*.o $(OUT)/*.so $(OUT)/ref_globals.c $(OUT)/cgnslib.h
