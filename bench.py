@@ -127,11 +127,23 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def run_form(prec, steps, warmup, e2e_steps, profile=True):
+def workload(name, prec):
+    from bluebottle_b200 import configs
+    if name == "small":
+        # the same sedimentation set-up at 1/8 the cells and spheres, for
+        # profiler captures (each FP32 vector 16.8 MB, 10 of them > L2)
+        wl = configs.sedimentation((128, 128, 256), (32.0, 32.0, 64.0), 1000,
+                                   nu=0.05, prec=prec, lamb_max_iter=LAMB_ITERS)
+    else:
+        wl = configs.config_c5(prec=prec, lamb_max_iter=LAMB_ITERS)
+    return wl
+
+
+def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5"):
     """One fresh simulation of the workload in precision form `prec`."""
-    from bluebottle_b200 import Sim, configs
+    from bluebottle_b200 import Sim
     import ctypes as C
-    wl = configs.config_c5(prec=prec, lamb_max_iter=LAMB_ITERS)
+    wl = workload(wl_name, prec)
     sim = Sim(wl, options=dict(lamb_max_iter_override=LAMB_ITERS))
     lib = sim.lib
     sim.prepare()
@@ -141,7 +153,7 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True):
     lib.bbb_profile_reset()
     lib.bbb_profile_enable(1 if profile else 0)
     launches0 = lib.bbb_kernel_launches()
-    iters = 0
+    iters = 0                      # bbb_step resets its stats every step
     lib.bbb_mark(0)
     for _ in range(steps):
         sim.step()
@@ -158,6 +170,9 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True):
     pm, pi, pb = C.c_double(), C.c_longlong(), C.c_double()
     lib.bbb_profile_get(C.byref(pm), C.byref(pi), C.byref(pb))
     out["prof_ms"], out["prof_iters"], out["prof_bytes"] = pm.value, pi.value, pb.value
+    for k in (0, 1):
+        lib.bbb_profile_get_pass(k, C.byref(pm), C.byref(pi), C.byref(pb))
+        out["pass%d" % k] = (pm.value, pi.value, pb.value)
     # end-to-end through the public API: particle records in from pinned
     # host memory, the step, particle records and dt back to the host
     n = sim.nparts
@@ -226,6 +241,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--workload", default="c5", choices=["c5", "small"],
+                    help="c5: the headline 256x256x512 + 8000 spheres; small: "
+                    "128x128x256 + 1000 spheres for profiler captures")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if world > 1:
@@ -263,27 +281,36 @@ def main():
     sampler = ClockSampler(local if world > 1 else 0)
     dist.barrier()
     sampler.start()
-    mixed = run_form(1, steps, warmup, e2e_steps=steps)
+    mixed = run_form(1, steps, warmup, e2e_steps=steps, wl_name=args.workload)
     clocks = sampler.stop()
     ms = dist.max(mixed["ms"])
     e2e_ms = dist.max(mixed["e2e_ms"])
     fp64 = None
     if not args.no_fp64:
-        fp64 = run_form(0, steps, 1, e2e_steps=0, profile=False)
+        fp64 = run_form(0, steps, 1, e2e_steps=0, profile=False,
+                        wl_name=args.workload)
         fp64["ms"] = dist.max(fp64["ms"])
     dist.barrier()
     if rank == 0:
         value = world * steps / (ms / 1000.0)
         e2e_value = world * steps / (e2e_ms / 1000.0)
-        achieved = (mixed["prof_bytes"] / (mixed["prof_ms"] / 1000.0) / 1e9
-                    if mixed["prof_ms"] > 0 else None)
+        # dominant kernel: pass A of the FP32 BiCGSTAB iteration
+        a_ms, a_n, a_bytes = mixed["pass0"]
+        achieved = a_bytes / (a_ms / 1000.0) / 1e9 if a_ms > 0 else None
+        passes = {}
+        for k, nm in ((0, "k_bicgA<float,4>"), (1, "k_bicgB<float,4>")):
+            pms, pn, pby = mixed["pass%d" % k]
+            passes[nm] = {"launches": pn, "ms_per_launch": pms / pn if pn else None,
+                          "GB_s": pby / (pms / 1000.0) / 1e9 if pms > 0 else None}
+        it_gbs = (mixed["prof_bytes"] / (mixed["prof_ms"] / 1000.0) / 1e9
+                  if mixed["prof_ms"] > 0 else None)
         traffic = None
         tfile = os.path.join(ROOT, "profiles", "bicgstab_traffic.json")
         if os.path.exists(tfile):
             try:
                 with open(tfile) as fh:
                     tj = json.load(fh)
-                traffic = tj.get("fp32_iteration_bytes_full_scale")
+                traffic = tj.get("pass_a_fp32_bytes_per_launch_full_scale")
             except Exception:
                 traffic = None
         line = {"metric": METRIC, "value": value, "unit": "timesteps/s",
@@ -291,8 +318,10 @@ def main():
                 "ms_per_step": ms / steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
                 "data": "synthetic (seeded sphere pack, splitmix64 seed 1)",
-                "config": {"workload": "256x256x512 periodic box 64x64x128, 8000 "
-                           "spheres r=1 (6.4%), rho_p/rho_f=2, g=-1 z, nu=0.05, "
+                "config": {"workload": ("256x256x512 periodic box 64x64x128, 8000 "
+                                        if args.workload == "c5" else
+                                        "128x128x256 periodic box 32x32x64, 1000 ")
+                           + "spheres r=1 (6.4%), rho_p/rho_f=2, g=-1 z, nu=0.05, "
                            "CN+Helmholtz CG, Jacobi-BiCGSTAB tol 1e-8, FP32 inner "
                            "in FP64 defect correction",
                            "lamb_iters_per_step": LAMB_ITERS,
@@ -307,8 +336,11 @@ def main():
                              "unit": "GB/s",
                              "frac": achieved / peak if achieved else None,
                              "traffic": traffic,
-                             "kernel": "BiCGSTAB iteration (k_bicg1+k_bicg2+k_bicg3, FP32)",
-                             "peak_kind": peak_kind},
+                             "kernel": "k_bicgA<float,4> (BiCGSTAB pass A, FP32): "
+                             "algorithmic 10 words + 1 mask byte per unknown",
+                             "peak_kind": peak_kind,
+                             "passes": passes,
+                             "iteration_GB_s": it_gbs},
                 "e2e": {"value": e2e_value, "unit": "timesteps/s",
                         "h2d_bytes_per_step": mixed["e2e_h2d"],
                         "d2h_bytes_per_step": mixed["e2e_d2h"]}}

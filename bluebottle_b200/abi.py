@@ -123,8 +123,12 @@ bbb_init_taylor_green bbb_host_free bbb_prepare bbb_release
 bbb_set_record_dir bbb_step bbb_advance_clock bbb_get_stats bbb_last_status
 bbb_status_string bbb_clear_status bbb_set_exit_on_failure bbb_device_count
 bbb_divergence bbb_kernel_launches bbb_reset_kernel_launches
-bbb_profile_enable bbb_profile_reset bbb_profile_get bbb_part_state_push
-bbb_part_state_pull bbb_mark bbb_mark_elapsed bbb_PP_bicgstab_static""".split()
+bbb_profile_enable bbb_profile_reset bbb_profile_get bbb_profile_get_pass
+bbb_part_state_push
+bbb_part_state_pull bbb_mark bbb_mark_elapsed bbb_PP_bicgstab_static
+bbb_learn_enable bbb_learn_train bbb_learn_crops bbb_learn_param_count
+bbb_learn_get_params bbb_learn_set_params bbb_learn_forward
+bbb_learn_use_reference_conv bbb_learn_grad""".split()
 
 _lib = None
 
@@ -173,6 +177,17 @@ def load():
     lib.bbb_mark_elapsed.restype = R
     lib.bbb_profile_get.argtypes = [C.POINTER(R), C.POINTER(C.c_longlong),
                                     C.POINTER(R)]
+    lib.bbb_profile_get_pass.argtypes = [C.c_int, C.POINTER(R),
+                                         C.POINTER(C.c_longlong), C.POINTER(R)]
+    lib.bbb_learn_enable.argtypes = [C.c_int]
+    lib.bbb_learn_train.argtypes = [C.c_int, R]
+    lib.bbb_learn_train.restype = R
+    lib.bbb_learn_get_params.argtypes = [C.POINTER(C.c_float), C.c_int]
+    lib.bbb_learn_set_params.argtypes = [C.POINTER(C.c_float), C.c_int]
+    lib.bbb_learn_forward.argtypes = [C.c_int] * 6 + [vp, vp, C.c_int]
+    lib.bbb_learn_use_reference_conv.argtypes = [C.c_int]
+    lib.bbb_learn_grad.argtypes = [C.c_int] * 5 + [vp, vp, C.POINTER(C.c_float)]
+    lib.bbb_learn_grad.restype = R
     for name in ("cuda_ustar_helmholtz", "cuda_vstar_helmholtz",
                  "cuda_wstar_helmholtz", "cuda_PP_bicgstab", "cuda_PP_rhs",
                  "cuda_part_BC_p", "cuda_ustar_rhs", "cuda_vstar_rhs",

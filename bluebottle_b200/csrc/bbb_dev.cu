@@ -283,6 +283,7 @@ extern "C" void cuda_dom_free(void)
 {
   if(!g_dev.ready) return;
   cudaStreamSynchronize(g_dev.stream);
+  bbb_learn_release();
   real **rs[] = {&g_dev.p0, &g_dev.p, &g_dev.phi, &g_dev.u, &g_dev.v, &g_dev.w,
     &g_dev.u0, &g_dev.v0, &g_dev.w0, &g_dev.us, &g_dev.vs, &g_dev.ws,
     &g_dev.conv_u, &g_dev.conv_v, &g_dev.conv_w, &g_dev.conv0_u,
@@ -310,6 +311,7 @@ extern "C" void cuda_dom_free(void)
 
 extern "C" void cuda_part_free(void)
 {
+  bbb_bins_free();
   dfree(g_dev.parts);
   for(int a = 0; a < 18; a++) dfree(g_dev.coef[a]);
   dfree(g_dev.node_pp); dfree(g_dev.node_ur); dfree(g_dev.node_ut);
@@ -708,6 +710,7 @@ extern "C" void cuda_store_u(void)
     d2d(g_dev.diff0_w, g_dev.diff_w, fz);
   }
   d2d(g_dev.p0, g_dev.p, sizeof(real) * d->Gcc.s3b);
+  bbb_learn_step_boundary();
   d2d(g_dev.u0, g_dev.u, fx);
   d2d(g_dev.v0, g_dev.v, fy);
   d2d(g_dev.w0, g_dev.w, fz);

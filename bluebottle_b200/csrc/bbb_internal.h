@@ -142,5 +142,12 @@ void bbb_part_BC_fields(real *uu, real *vv, real *ww);
 void bbb_star_rhs(int comp_mask, int explicit_ab2);
 void bbb_pp_rhs_to_b(void);
 double bbb_dev_sum_interior_cc(const real *f);
+double bbb_poisson_resid_norm(const double *x);
+/* learned initial guess (bbb_learn.cu) */
+int bbb_learn_pre_solve(void);
+void bbb_learn_post_solve(void);
+void bbb_learn_step_boundary(void);
+void bbb_learn_release(void);
+void bbb_bins_free(void);
 
 #endif

@@ -7,24 +7,36 @@
  * is applied from that byte inside the fused kernels, with the diagonal and
  * the Jacobi scale of the 128 possible bytes tabulated in shared memory.
  *
- * BiCGSTAB (right-preconditioned, as CUSP's krylov::bicgstab) runs as three
- * fused passes per iteration, with all scalars kept on the device:
- *   K1  p = r + beta p - beta omega v;  v = A M p;   (rh, v)   -> alpha
- *   K2  s = r - alpha v;                t = A M s;   (t,s) (t,t) (s,s)
- *   K3  x += alpha M p + omega M s;  r = s - omega t;  (rh,r) (r,r) sum x
- * 17 vector words + 3 mask bytes per unknown and iteration.  CG (CUSP's
- * krylov::cg, used for the Crank-Nicolson Helmholtz solves) runs as two:
+ * BiCGSTAB is CUSP's right-preconditioned krylov::bicgstab (M = diag^-1):
+ *   v = A M p;  alpha = rho / (rh, v);  s = r - alpha v;  t = A M s;
+ *   omega = (t, s) / (t, t);  x += alpha M p + omega M s;  r = s - omega t;
+ *   rho' = (rh, r);  beta = (rho' / rho)(alpha / omega);
+ *   p = r + beta p - beta omega v
+ * run as two fused stencil passes per iteration, all scalars on the device:
+ *   A  r = s - omega t;  x += alpha M p + omega M s;
+ *      p = r + beta p - beta omega v;  v = A M p;
+ *      (r, r) (rh, r) (rh, v) sum x          -> alpha, convergence
+ *   B  s = r - alpha v;  t = A M s;
+ *      (t, s) (t, t) (s, s) (rh, s) (rh, t)  -> omega, beta
+ * beta needs rho' before pass A forms r, so pass B supplies it as
+ * (rh, s) - omega (rh, t), which equals (rh, r) in exact arithmetic; alpha
+ * uses the (rh, r) pass A sums.  15 vector words + 2 mask bytes per unknown
+ * and iteration.  Stopping rule of CUSP's monitor: ||r|| <= rtol ||b||,
+ * iteration count advanced once per full iteration, early exit (without
+ * counting) when ||s|| meets it.
+ *
+ * CG (CUSP's krylov::cg, used for the Crank-Nicolson Helmholtz solves):
  *   C1  p = M r + beta p;  y = A p;  (y, p)
  *   C2  x += alpha p;  r -= alpha y;  (r, M r) (r, r)
- * Stopping rule of CUSP's monitor: ||r|| <= rtol ||b||, iteration count
- * advanced once per full iteration, early exit when ||s|| meets it.
  *
- * Stencil kernels tile x-y with 32x8 threads and march along z through a
- * slab.  Where the row length allows, each thread owns V consecutive cells
- * in x (V = 4 for FP32, 2 for FP64: one 128-bit access per array); x
- * neighbours come from registers and warp shuffles, y neighbours from a
- * three-plane shared-memory ring (one barrier per plane), z neighbours
- * from registers.  Rows of other lengths use a one-cell-per-thread tile.
+ * Stencil kernels tile x-y with 32x8 threads and march along z; the grid
+ * is one wave of resident blocks, each taking an equal run of (tile,
+ * plane) units, so no block idles at the end.  Where the row length
+ * allows, each thread owns V consecutive cells in x (V = 4 for FP32, 2 for
+ * FP64: one 128-bit access per array); x neighbours come from registers and
+ * warp shuffles, y neighbours from a three-plane shared-memory ring (one
+ * barrier per plane), z neighbours from registers.  Rows of other lengths
+ * use a one-cell-per-thread tile.
  */
 #include <math.h>
 #include <stdio.h>
@@ -45,11 +57,15 @@ struct opc {
   int helm;
 };
 
+/* A box of nx*ny*nz unknowns cut into x-y tiles; the work units are
+ * (tile, plane) pairs, tile-major, and block b marches through units
+ * [b chunk, (b+1) chunk): one or two z-segments of one or two tiles. */
 struct boxc {
   int nx, ny, nz;
   int wW, wE, wS, wN, wB, wT;   /* wrapped neighbour index at each edge */
-  int slab;                     /* planes per block                    */
   int vec;                      /* cells per thread along x            */
+  int tiles_x;                  /* tiles along x                       */
+  long long units, chunk;       /* tiles * nz; units per block         */
 };
 
 /* vector width usable for a row of nx cells of element size `esz` */
@@ -60,8 +76,23 @@ static int pick_vec(int nx, int esz)
   return 1;
 }
 
+static int sm_count(void)
+{
+  static int n = 0;
+  if(!n) {
+    int dev = 0;
+    if(cudaGetDevice(&dev) != cudaSuccess ||
+       cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess
+       || n <= 0)
+      n = 148;
+  }
+  return n;
+}
+
+/* `per_sm` resident blocks of the stencil kernels: the units are split
+ * evenly over one wave of resident blocks (at least 4 planes per block) */
 static boxc make_box(int nx, int ny, int nz, int perx, int pery, int perz,
-  int dupx, int dupy, int dupz, int vec)
+  int dupx, int dupy, int dupz, int vec, int per_sm)
 {
   boxc b;
   b.nx = nx; b.ny = ny; b.nz = nz;
@@ -72,22 +103,32 @@ static boxc make_box(int nx, int ny, int nz, int perx, int pery, int perz,
   b.wB = perz ? (dupz ? nz - 2 : nz - 1) : 0;
   b.wT = perz ? (dupz ? 1 : 0) : nz - 1;
   b.vec = vec;
-  /* about two waves of 4 resident blocks per SM; long slabs keep the
-   * re-read of the two z-halo planes small */
-  long long tiles = (long long)((nx + TX * vec - 1) / (TX * vec)) * ((ny + TY - 1) / TY);
-  int slabs = (int)((148LL * 8 + tiles - 1) / tiles);
-  if(slabs < 1) slabs = 1;
-  int kz = (nz + slabs - 1) / slabs;
-  if(kz < 4) kz = 4;
-  if(kz > nz) kz = nz;
-  b.slab = kz;
+  b.tiles_x = (nx + TX * vec - 1) / (TX * vec);
+  long long tiles = (long long)b.tiles_x * ((ny + TY - 1) / TY);
+  b.units = tiles * nz;
+  if(per_sm < 1) per_sm = 1;
+  long long slots = (long long)sm_count() * per_sm;
+  long long chunk = (b.units + slots - 1) / slots;
+  if(chunk < 4) chunk = 4;
+  b.chunk = chunk;
   return b;
 }
 
 static dim3 box_grid(const boxc &b)
 {
-  return dim3((b.nx + TX * b.vec - 1) / (TX * b.vec), (b.ny + TY - 1) / TY,
-    (b.nz + b.slab - 1) / b.slab);
+  return dim3((unsigned)((b.units + b.chunk - 1) / b.chunk));
+}
+
+template <typename K>
+static int resident(K kernel)
+{
+  int nb = 0;
+  if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, NTHR, 0)
+     != cudaSuccess || nb < 1) {
+    cudaGetLastError();
+    nb = 2;
+  }
+  return nb;
 }
 
 __device__ __forceinline__ int mapx(const boxc &b, int g)
@@ -201,22 +242,41 @@ __device__ __forceinline__ void ldm(const uint8_t *p, long long c, unsigned (&o)
   for(int v = 0; v < V; v++) o[v] = e[v];
 }
 
-/* ------------------------------------------------ tiled stencil drivers
- * P: producer; P::ev<V>(c, raw, q, dinv) gives at V consecutive cells the
- * raw value and the value the operator is applied to.  E: epilogue;
- * E::at<V>(c, raw, Aq, red) at the owned cells.  Both drivers fill the
- * shared ring for every plane of the slab. */
-
-/* one cell per thread; any row length (partial tiles wrap by index) */
-template <typename T, class P, class E, int NRED>
-__device__ __forceinline__ void tile_stencil1(const boxc &B, const opc &O,
-  const uint8_t *__restrict__ mask, const optab<T> &tab, P &prod, E &epi,
-  double (&red)[NRED])
+/* the V mask bytes at c packed in one word (byte v = cell c + v) */
+template <int V>
+__device__ __forceinline__ unsigned ldmw(const uint8_t *p, long long c)
 {
+  if constexpr(V == 4) return *reinterpret_cast<const unsigned *>(p + c);
+  else if constexpr(V == 2) return *reinterpret_cast<const unsigned short *>(p + c);
+  else return p[c];
+}
+
+__device__ __forceinline__ unsigned mbyte(unsigned w, int v)
+{ return (w >> (8 * v)) & 0xffu; }
+
+/* two values carried from the producer to the epilogue */
+template <typename T>
+struct raw2 { T a, h; };
+
+/* ------------------------------------------------ tiled stencil drivers
+ * P: producer.  P::ev<V>(c, raw, q, dinv, own, red) gives at V consecutive
+ * cells the value the operator is applied to (q) and what the epilogue
+ * needs (raw, of type P::Raw); `own` is set exactly once for every cell of
+ * the block's units, where the producer may also do the cell's
+ * pointwise work (stores, sums into red).  E: epilogue; E::at<V>(c, raw,
+ * Aq, red) at the owned cells, Aq = (A q) there. */
+
+/* one cell per thread; any row length (partial tiles wrap by index);
+ * planes k0..k1-1 of tile (bx, by) */
+template <typename T, class P, class E, int NRED>
+__device__ __forceinline__ void seg_stencil1(const boxc &B, const opc &O,
+  const uint8_t *__restrict__ mask, const optab<T> &tab, P &prod, E &epi,
+  double (&red)[NRED], int bx, int by, int k0, int k1)
+{
+  typedef typename P::Raw R;
   __shared__ T ring[3][HY][HX];
   int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
-  int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
-  int k0 = blockIdx.z * B.slab, k1 = min(k0 + B.slab, B.nz);
+  int i0 = bx * TX, j0 = by * TY;
   int i = i0 + tx, j = j0 + ty;
   bool valid = (i < B.nx) && (j < B.ny);
   int gi = mapx(B, i), gj = mapy(B, j);
@@ -227,28 +287,32 @@ __device__ __forceinline__ void tile_stencil1(const boxc &B, const opc &O,
   else if(tid < 80) { hsx = HX - 1; hsy = tid - 72 + 1; }
   if(hsx >= 0) { hgi = mapx(B, i0 - 1 + hsx); hgj = mapy(B, j0 - 1 + hsy); }
 
-  T raw_cur[1], raw_next[1], q_prev[1], q_cur[1], q_next[1], hr[1], hq[1];
+  R raw_cur[1], raw_next[1], hr[1];
+  T q_prev[1], q_cur[1], q_next[1], hq[1];
   unsigned m_cur[1], m_next[1];
-  prod.template ev<1>(lin(B, gi, gj, mapz(B, k0 - 1)), hr, q_prev, tab.dinv);
+  prod.template ev<1>(lin(B, gi, gj, mapz(B, k0 - 1)), hr, q_prev, tab.dinv,
+    false, red);
   {
     long long c = lin(B, gi, gj, k0);
-    prod.template ev<1>(c, raw_cur, q_cur, tab.dinv);
+    prod.template ev<1>(c, raw_cur, q_cur, tab.dinv, valid, red);
     ldm<1>(mask, c, m_cur);
     ring[0][ty + 1][tx + 1] = q_cur[0];
     if(hsx >= 0) {
-      prod.template ev<1>(lin(B, hgi, hgj, k0), hr, hq, tab.dinv);
+      prod.template ev<1>(lin(B, hgi, hgj, k0), hr, hq, tab.dinv, false, red);
       ring[0][hsy][hsx] = hq[0];
     }
   }
   for(int k = k0; k < k1; k++) {
     int slot = (k - k0) % 3, nslot = (k - k0 + 1) % 3;
     long long cn = lin(B, gi, gj, mapz(B, k + 1));
-    prod.template ev<1>(cn, raw_next, q_next, tab.dinv);
+    prod.template ev<1>(cn, raw_next, q_next, tab.dinv, valid && (k + 1 < k1),
+      red);
     ldm<1>(mask, cn, m_next);
     if(k + 1 < k1) {
       ring[nslot][ty + 1][tx + 1] = q_next[0];
       if(hsx >= 0) {
-        prod.template ev<1>(lin(B, hgi, hgj, k + 1), hr, hq, tab.dinv);
+        prod.template ev<1>(lin(B, hgi, hgj, k + 1), hr, hq, tab.dinv, false,
+          red);
         ring[nslot][hsy][hsx] = hq[0];
       }
     }
@@ -268,16 +332,16 @@ __device__ __forceinline__ void tile_stencil1(const boxc &B, const opc &O,
 
 /* V cells per thread; requires nx % (32 V) == 0 (full tiles in x) */
 template <typename T, int V, class P, class E, int NRED>
-__device__ __forceinline__ void tile_stencilV(const boxc &B, const opc &O,
+__device__ __forceinline__ void seg_stencilV(const boxc &B, const opc &O,
   const uint8_t *__restrict__ mask, const optab<T> &tab, P &prod, E &epi,
-  double (&red)[NRED])
+  double (&red)[NRED], int bx, int by, int k0, int k1)
 {
+  typedef typename P::Raw R;
   constexpr int W = TX * V;
   __shared__ __align__(16) T ring[3][HY][W];
   __shared__ T hw[3][TY], he[3][TY];
   int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
-  int i0 = blockIdx.x * W, j0 = blockIdx.y * TY;
-  int k0 = blockIdx.z * B.slab, k1 = min(k0 + B.slab, B.nz);
+  int i0 = bx * W, j0 = by * TY;
   int ib = i0 + tx * V, j = j0 + ty;
   bool valid = j < B.ny;
   int gj = mapy(B, j);
@@ -293,36 +357,43 @@ __device__ __forceinline__ void tile_stencilV(const boxc &B, const opc &O,
     hgi = mapx(B, hcol == 0 ? i0 - 1 : i0 + W);
     hgj = mapy(B, j0 + r);
   }
-  T raw_cur[V], raw_next[V], q_prev[V], q_cur[V], q_next[V], tr[V], tq[V];
-  unsigned m_cur[V], m_next[V];
-  prod.template ev<V>(lin(B, ib, gj, mapz(B, k0 - 1)), tr, q_prev, tab.dinv);
+  R raw_cur[V], raw_next[V], tr[V];
+  T q_prev[V], q_cur[V], q_next[V], tq[V];
+  unsigned m_cur, m_next;
+  prod.template ev<V>(lin(B, ib, gj, mapz(B, k0 - 1)), tr, q_prev, tab.dinv,
+    false, red);
   {
     long long c = lin(B, ib, gj, k0);
-    prod.template ev<V>(c, raw_cur, q_cur, tab.dinv);
-    ldm<V>(mask, c, m_cur);
+    prod.template ev<V>(c, raw_cur, q_cur, tab.dinv, valid, red);
+    m_cur = ldmw<V>(mask, c);
     stv<T, V>(&ring[0][ty + 1][0], tx * V, q_cur);
     if(hrow >= 0) {
-      prod.template ev<V>(lin(B, hgi, hgj, k0), tr, tq, tab.dinv);
+      prod.template ev<V>(lin(B, hgi, hgj, k0), tr, tq, tab.dinv, false, red);
       stv<T, V>(&ring[0][hrow][0], (tid & 31) * V, tq);
     } else if(hcol >= 0) {
-      T a[1], bq[1];
-      prod.template ev<1>(lin(B, hgi, hgj, k0), a, bq, tab.dinv);
+      R a[1];
+      T bq[1];
+      prod.template ev<1>(lin(B, hgi, hgj, k0), a, bq, tab.dinv, false, red);
       (hcol == 0 ? hw : he)[0][(tid - 64) & 7] = bq[0];
     }
   }
   for(int k = k0; k < k1; k++) {
     int slot = (k - k0) % 3, nslot = (k - k0 + 1) % 3;
     long long cn = lin(B, ib, gj, mapz(B, k + 1));
-    prod.template ev<V>(cn, raw_next, q_next, tab.dinv);
-    ldm<V>(mask, cn, m_next);
+    prod.template ev<V>(cn, raw_next, q_next, tab.dinv, valid && (k + 1 < k1),
+      red);
+    m_next = ldmw<V>(mask, cn);
     if(k + 1 < k1) {
       stv<T, V>(&ring[nslot][ty + 1][0], tx * V, q_next);
       if(hrow >= 0) {
-        prod.template ev<V>(lin(B, hgi, hgj, k + 1), tr, tq, tab.dinv);
+        prod.template ev<V>(lin(B, hgi, hgj, k + 1), tr, tq, tab.dinv, false,
+          red);
         stv<T, V>(&ring[nslot][hrow][0], (tid & 31) * V, tq);
       } else if(hcol >= 0) {
-        T a[1], bq[1];
-        prod.template ev<1>(lin(B, hgi, hgj, k + 1), a, bq, tab.dinv);
+        R a[1];
+        T bq[1];
+        prod.template ev<1>(lin(B, hgi, hgj, k + 1), a, bq, tab.dinv, false,
+          red);
         (hcol == 0 ? hw : he)[nslot][(tid - 64) & 7] = bq[0];
       }
     }
@@ -339,8 +410,9 @@ __device__ __forceinline__ void tile_stencilV(const boxc &B, const opc &O,
       for(int v = 0; v < V; v++) {
         T qW = v > 0 ? q_cur[v - 1] : left;
         T qE = v < V - 1 ? q_cur[v + 1] : right;
-        Aq[v] = op_apply<T>(m_cur[v], O, tab.diag[m_cur[v]], q_prev[v], S[v],
-          qW, q_cur[v], qE, N[v], q_next[v]);
+        unsigned mv = mbyte(m_cur, v);
+        Aq[v] = op_apply<T>(mv, O, tab.diag[mv], q_prev[v], S[v], qW,
+          q_cur[v], qE, N[v], q_next[v]);
       }
       epi.template at<V>(lin(B, ib, j, k), raw_cur, Aq, red);
     }
@@ -348,18 +420,32 @@ __device__ __forceinline__ void tile_stencilV(const boxc &B, const opc &O,
     for(int v = 0; v < V; v++) {
       q_prev[v] = q_cur[v];
       raw_cur[v] = raw_next[v]; q_cur[v] = q_next[v];
-      m_cur[v] = m_next[v];
     }
+    m_cur = m_next;
   }
 }
 
+/* this block's units, segment by segment (block-uniform loop) */
 template <typename T, int V, class P, class E, int NRED>
 __device__ __forceinline__ void tile_stencil(const boxc &B, const opc &O,
   const uint8_t *__restrict__ mask, const optab<T> &tab, P &prod, E &epi,
   double (&red)[NRED])
 {
-  if constexpr(V == 1) tile_stencil1<T>(B, O, mask, tab, prod, epi, red);
-  else tile_stencilV<T, V>(B, O, mask, tab, prod, epi, red);
+  long long u0 = (long long)blockIdx.x * B.chunk;
+  long long u1 = u0 + B.chunk < B.units ? u0 + B.chunk : B.units;
+  while(u0 < u1) {
+    long long tile = u0 / B.nz;
+    int k0 = (int)(u0 - tile * B.nz);
+    long long left = u1 - u0;
+    int k1 = left < (long long)(B.nz - k0) ? k0 + (int)left : B.nz;
+    int bx = (int)(tile % B.tiles_x), by = (int)(tile / B.tiles_x);
+    if constexpr(V == 1)
+      seg_stencil1<T>(B, O, mask, tab, prod, epi, red, bx, by, k0, k1);
+    else
+      seg_stencilV<T, V>(B, O, mask, tab, prod, epi, red, bx, by, k0, k1);
+    u0 += k1 - k0;
+    __syncthreads();      /* the ring is refilled by the next segment */
+  }
 }
 
 /* ------------------------------------------------ masks */
@@ -443,23 +529,28 @@ void bbb_build_masks(void)
 
 /* ------------------------------------------------ BiCGSTAB kernels */
 
-/* residual set-up: r = b - A x; rh = r; p = r; (r, r), sum x */
+/* residual set-up: r = b - A x into s (pass A starts from r = s) and rh;
+ * (r, r), sum x */
 template <typename T>
 struct prod_x {
   const T *x;
-  template <int V>
+  typedef T Raw;
+  template <int V, int NR>
   __device__ __forceinline__ void ev(long long c, T (&raw)[V], T (&q)[V],
-    const T *dinv) const
+    const T *dinv, bool own, double (&red)[NR]) const
   {
     ldv<T, V>(x, c, raw);
 #pragma unroll
-    for(int v = 0; v < V; v++) q[v] = raw[v];
-    (void)dinv;
+    for(int v = 0; v < V; v++) {
+      q[v] = raw[v];
+      if constexpr(NR > 1) { if(own) red[1] += (double)raw[v]; }
+    }
+    (void)dinv; (void)own;
   }
 };
 template <typename T>
 struct epi_res {
-  const T *b; T *r, *rh, *p;
+  const T *b; T *r, *rh;
   template <int V>
   __device__ __forceinline__ void at(long long c, const T (&xr)[V],
     const T (&Ax)[V], double (&red)[2]) const
@@ -470,22 +561,22 @@ struct epi_res {
     for(int v = 0; v < V; v++) {
       rv[v] = bb[v] - Ax[v];
       red[0] += (double)rv[v] * (double)rv[v];
-      red[1] += (double)xr[v];
     }
-    stv<T, V>(r, c, rv); stv<T, V>(rh, c, rv); stv<T, V>(p, c, rv);
+    stv<T, V>(r, c, rv); stv<T, V>(rh, c, rv);
+    (void)xr;
   }
 };
 
 template <typename T, int V>
 __global__ void __launch_bounds__(NTHR) k_bicg_setup(boxc B, opc O,
   const uint8_t *__restrict__ mask, const T *__restrict__ b, const T *x,
-  T *r, T *rh, T *p, bbb_kry *s, double *partials, double rtol, int maxit)
+  T *r0, T *rh, bbb_kry *s, double *partials, double rtol, int maxit)
 {
   __shared__ double sh[32 * 2];
   __shared__ optab<T> tab;
   optab_fill<T>(tab, O);
   prod_x<T> P{x};
-  epi_res<T> E{b, r, rh, p};
+  epi_res<T> E{b, r0, rh};
   double red[2] = {0., 0.};
   tile_stencil<T, V>(B, O, mask, tab, P, E, red);
   if(bbb_grid_partial<2>(red, partials, &s->ticket, sh)) {
@@ -508,42 +599,71 @@ __global__ void __launch_bounds__(NTHR) k_bicg_setup(boxc B, opc O,
   }
 }
 
-/* p = r + beta p + (-beta omega) v, CUSP's axpbypcz form */
+/* pass A.  red: 0 (rh, v), 1 (r, r), 2 (rh, r), 3 sum x */
 template <typename T>
-struct prod_k1 {
-  const T *r, *p, *v; const uint8_t *mask; T beta, bo; int first;
+struct prod_A {
+  const T *s, *t, *p, *v, *rh; const uint8_t *mask;
+  T *r_out, *p_out, *x;
+  T alpha, omega, beta, bo;
+  int first;
+  typedef T Raw;                 /* rh at the cell */
   template <int V>
-  __device__ __forceinline__ void ev(long long c, T (&raw)[V], T (&q)[V],
-    const T *dinv) const
+  __device__ __forceinline__ void ev(long long c, Raw (&raw)[V], T (&q)[V],
+    const T *dinv, bool own, double (&red)[4]) const
   {
-    T pp[V];
+    T ss[V], rr[V], pn[V];
     unsigned mm[V];
-    ldv<T, V>(p, c, pp);
+    ldv<T, V>(s, c, ss);
     ldm<V>(mask, c, mm);
     if(first) {
 #pragma unroll
-      for(int a = 0; a < V; a++) raw[a] = pp[a];
+      for(int a = 0; a < V; a++) { rr[a] = ss[a]; pn[a] = rr[a]; }
     } else {
-      T rr[V], vv[V];
-      ldv<T, V>(r, c, rr);
+      T tt[V], pp[V], vv[V];
+      ldv<T, V>(t, c, tt);
+      ldv<T, V>(p, c, pp);
       ldv<T, V>(v, c, vv);
 #pragma unroll
-      for(int a = 0; a < V; a++) raw[a] = rr[a] + beta * pp[a] + bo * vv[a];
+      for(int a = 0; a < V; a++) {
+        rr[a] = ss[a] - omega * tt[a];
+        pn[a] = rr[a] + beta * pp[a] + bo * vv[a];
+      }
+      if(own) {
+        T xx[V];
+        ldv<T, V>(x, c, xx);
+#pragma unroll
+        for(int a = 0; a < V; a++) {
+          T di = dinv[mm[a]];
+          xx[a] = xx[a] + alpha * (di * pp[a]) + omega * (di * ss[a]);
+          red[3] += (double)xx[a];
+        }
+        stv<T, V>(x, c, xx);
+      }
     }
 #pragma unroll
-    for(int a = 0; a < V; a++) q[a] = dinv[mm[a]] * raw[a];
+    for(int a = 0; a < V; a++) q[a] = dinv[mm[a]] * pn[a];
+    if(own) {
+      ldv<T, V>(rh, c, raw);
+#pragma unroll
+      for(int a = 0; a < V; a++) {
+        red[1] += (double)rr[a] * (double)rr[a];
+        red[2] += (double)raw[a] * (double)rr[a];
+      }
+      stv<T, V>(r_out, c, rr);
+      stv<T, V>(p_out, c, pn);
+    } else {
+#pragma unroll
+      for(int a = 0; a < V; a++) raw[a] = (T)0.;
+    }
   }
 };
 template <typename T>
-struct epi_k1 {
-  const T *rh; T *pn, *vn;
+struct epi_A {
+  T *vn;
   template <int V>
-  __device__ __forceinline__ void at(long long c, const T (&praw)[V],
-    const T (&Aq)[V], double (&red)[1]) const
+  __device__ __forceinline__ void at(long long c, const T (&hh)[V],
+    const T (&Aq)[V], double (&red)[4]) const
   {
-    T hh[V];
-    ldv<T, V>(rh, c, hh);
-    stv<T, V>(pn, c, praw);
     stv<T, V>(vn, c, Aq);
 #pragma unroll
     for(int a = 0; a < V; a++) red[0] += (double)hh[a] * (double)Aq[a];
@@ -551,35 +671,50 @@ struct epi_k1 {
 };
 
 template <typename T, int V>
-__global__ void __launch_bounds__(NTHR) k_bicg1(boxc B, opc O,
-  const uint8_t *__restrict__ mask, const T *r, const T *p_old,
-  const T *v_old, const T *__restrict__ rh, T *p_new, T *v_new, bbb_kry *s,
-  double *partials)
+__global__ void __launch_bounds__(NTHR, 3) k_bicgA(boxc B, opc O,
+  const uint8_t *__restrict__ mask, const T *sv, const T *tv, const T *p_old,
+  const T *v_old, const T *__restrict__ rh, T *r, T *p_new, T *v_new, T *x,
+  bbb_kry *s, double *partials)
 {
   if(((volatile bbb_kry *)s)->done) return;
-  __shared__ double sh[32];
+  __shared__ double sh[32 * 4];
   __shared__ optab<T> tab;
   optab_fill<T>(tab, O);
-  prod_k1<T> P{r, p_old, v_old, mask, (T)s->beta, (T)(-s->beta * s->omega),
-    s->first};
-  epi_k1<T> E{rh, p_new, v_new};
-  double red[1] = {0.};
+  int first = s->first;
+  double omega = s->omega, beta = s->beta;
+  prod_A<T> P{sv, tv, p_old, v_old, rh, mask, r, p_new, x, (T)s->alpha,
+    (T)omega, (T)beta, (T)(-beta * omega), first};
+  epi_A<T> E{v_new};
+  double red[4] = {0., 0., 0., 0.};
   tile_stencil<T, V>(B, O, mask, tab, P, E, red);
-  if(bbb_grid_partial<1>(red, partials, &s->ticket, sh)) {
-    bbb_grid_finish_sum<1>(red, partials, &s->ticket, sh);
+  if(bbb_grid_partial<4>(red, partials, &s->ticket, sh)) {
+    bbb_grid_finish_sum<4>(red, partials, &s->ticket, sh);
     if(threadIdx.x == 0 && threadIdx.y == 0) {
-      s->alpha = s->rho / red[0];
+      int sconv = s->s_conv;
+      if(!first) {
+        s->sumx = red[3];
+        if(!sconv) s->iter += 1;
+      }
+      double rn = sconv ? s->rnorm : sqrt(red[1]);
+      s->rnorm = rn;
+      s->rho = red[2];
+      s->alpha = red[2] / red[0];
       s->first = 0;
+      s->converged = sconv || (rn <= s->tol);
+      if(!isfinite(rn)) { s->status = BBB_ERR_NONFINITE; s->done = 1; }
+      if(s->converged || s->iter >= s->maxit) s->done = 1;
     }
   }
 }
 
+/* pass B.  red: 0 (t, s), 1 (t, t), 2 (s, s), 3 (rh, s), 4 (rh, t) */
 template <typename T>
-struct prod_k2 {
-  const T *r, *v; const uint8_t *mask; T alpha;
+struct prod_B {
+  const T *r, *v; const uint8_t *mask; T *s_out; T alpha;
+  typedef T Raw;                 /* s at the cell */
   template <int V>
   __device__ __forceinline__ void ev(long long c, T (&raw)[V], T (&q)[V],
-    const T *dinv) const
+    const T *dinv, bool own, double (&red)[5]) const
   {
     T rr[V], vv[V];
     unsigned mm[V];
@@ -591,117 +726,65 @@ struct prod_k2 {
       raw[a] = rr[a] - alpha * vv[a];
       q[a] = dinv[mm[a]] * raw[a];
     }
+    if(own) {
+#pragma unroll
+      for(int a = 0; a < V; a++) red[2] += (double)raw[a] * (double)raw[a];
+      stv<T, V>(s_out, c, raw);
+    }
   }
 };
 template <typename T>
-struct epi_k2 {
-  T *sv, *tv;
+struct epi_B {
+  const T *rh; T *tn;
   template <int V>
-  __device__ __forceinline__ void at(long long c, const T (&sraw)[V],
-    const T (&Aq)[V], double (&red)[3]) const
+  __device__ __forceinline__ void at(long long c, const T (&ss)[V],
+    const T (&Aq)[V], double (&red)[5]) const
   {
-    stv<T, V>(sv, c, sraw);
-    stv<T, V>(tv, c, Aq);
+    T hh[V];
+    ldv<T, V>(rh, c, hh);
+    stv<T, V>(tn, c, Aq);
 #pragma unroll
     for(int a = 0; a < V; a++) {
-      red[0] += (double)Aq[a] * (double)sraw[a];
+      red[0] += (double)Aq[a] * (double)ss[a];
       red[1] += (double)Aq[a] * (double)Aq[a];
-      red[2] += (double)sraw[a] * (double)sraw[a];
+      red[3] += (double)hh[a] * (double)ss[a];
+      red[4] += (double)hh[a] * (double)Aq[a];
     }
   }
 };
 
 template <typename T, int V>
-__global__ void __launch_bounds__(NTHR) k_bicg2(boxc B, opc O,
-  const uint8_t *__restrict__ mask, const T *r, const T *v, T *s_out,
-  T *t_out, bbb_kry *s, double *partials)
+__global__ void __launch_bounds__(NTHR, 3) k_bicgB(boxc B, opc O,
+  const uint8_t *__restrict__ mask, const T *r, const T *v,
+  const T *__restrict__ rh, T *s_out, T *t_out, bbb_kry *s, double *partials)
 {
   if(((volatile bbb_kry *)s)->done) return;
-  __shared__ double sh[32 * 3];
+  __shared__ double sh[32 * 5];
   __shared__ optab<T> tab;
   optab_fill<T>(tab, O);
-  prod_k2<T> P{r, v, mask, (T)s->alpha};
-  epi_k2<T> E{s_out, t_out};
-  double red[3] = {0., 0., 0.};
+  double alpha = s->alpha;
+  prod_B<T> P{r, v, mask, s_out, (T)alpha};
+  epi_B<T> E{rh, t_out};
+  double red[5] = {0., 0., 0., 0., 0.};
   tile_stencil<T, V>(B, O, mask, tab, P, E, red);
-  if(bbb_grid_partial<3>(red, partials, &s->ticket, sh)) {
-    bbb_grid_finish_sum<3>(red, partials, &s->ticket, sh);
+  if(bbb_grid_partial<5>(red, partials, &s->ticket, sh)) {
+    bbb_grid_finish_sum<5>(red, partials, &s->ticket, sh);
     if(threadIdx.x == 0 && threadIdx.y == 0) {
       s->t_s = red[0];
       s->t_t = red[1];
       s->s_s = red[2];
       double sn = sqrt(red[2]);
-      s->s_conv = (sn <= s->tol);
-      if(s->s_conv) s->rnorm = sn;
-    }
-  }
-}
-
-/* pointwise third pass, V consecutive unknowns per thread and step */
-template <typename T, int V>
-__global__ void __launch_bounds__(256) k_bicg3(long long n, opc O,
-  const uint8_t *__restrict__ mask, T *x, const T *__restrict__ p,
-  const T *__restrict__ sv, const T *__restrict__ tv, T *r,
-  const T *__restrict__ rh, bbb_kry *s, double *partials)
-{
-  if(((volatile bbb_kry *)s)->done) return;
-  __shared__ double sh[32 * 3];
-  __shared__ optab<T> tab;
-  optab_fill<T>(tab, O);
-  double alpha = s->alpha;
-  int sconv = s->s_conv;
-  double omega = sconv ? 0. : s->t_s / s->t_t;
-  T a = (T)alpha, om = (T)omega;
-  double red[3] = {0., 0., 0.};
-  long long nv = n / V;
-  for(long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nv;
-      e += (long long)gridDim.x * blockDim.x) {
-    long long c = e * V;
-    T xv[V], pv[V];
-    unsigned mm[V];
-    ldv<T, V>(x, c, xv);
-    ldv<T, V>(p, c, pv);
-    ldm<V>(mask, c, mm);
-    if(sconv) {
-#pragma unroll
-      for(int q = 0; q < V; q++) xv[q] = xv[q] + a * (tab.dinv[mm[q]] * pv[q]);
-    } else {
-      T ss[V], tt[V], hh[V], rv[V];
-      ldv<T, V>(sv, c, ss);
-      ldv<T, V>(tv, c, tt);
-      ldv<T, V>(rh, c, hh);
-#pragma unroll
-      for(int q = 0; q < V; q++) {
-        T di = tab.dinv[mm[q]];
-        xv[q] = xv[q] + a * (di * pv[q]) + om * (di * ss[q]);
-        rv[q] = ss[q] - om * tt[q];
-        red[0] += (double)hh[q] * (double)rv[q];
-        red[1] += (double)rv[q] * (double)rv[q];
-      }
-      stv<T, V>(r, c, rv);
-    }
-    stv<T, V>(x, c, xv);
-#pragma unroll
-    for(int q = 0; q < V; q++) red[2] += (double)xv[q];
-  }
-  if(bbb_grid_partial<3>(red, partials, &s->ticket, sh)) {
-    bbb_grid_finish_sum<3>(red, partials, &s->ticket, sh);
-    if(threadIdx.x == 0) {
-      s->sumx = red[2];
+      int sconv = (sn <= s->tol);
+      s->s_conv = sconv;
       if(sconv) {
-        s->converged = 1;
-        s->done = 1;
+        s->rnorm = sn;
+        s->omega = 0.;
+        s->beta = 0.;
       } else {
-        double rho_new = red[0];
-        s->beta = (rho_new / s->rho) * (alpha / omega);
-        s->rho = rho_new;
+        double omega = red[0] / red[1];
+        double rho_new = red[3] - omega * red[4];
         s->omega = omega;
-        s->iter += 1;
-        double rn = sqrt(red[1]);
-        s->rnorm = rn;
-        s->converged = (rn <= s->tol);
-        if(!isfinite(rn)) { s->status = BBB_ERR_NONFINITE; s->done = 1; }
-        if(s->converged || s->iter >= s->maxit) s->done = 1;
+        s->beta = (rho_new / s->rho) * (alpha / omega);
       }
     }
   }
@@ -759,62 +842,83 @@ __global__ void k_pp_writeback(const double *x, real *ph, bbb_geom G,
   }
 }
 
-/* ------------------------------------------------ live iteration timing
- * CUDA events on the solver stream bracket each BiCGSTAB iteration (K1 to
- * K3) while enabled; after a solve only the iterations the device really
- * executed are summed, with their algorithmic bytes. */
-#define BBB_PROF_EV 8192
+/* ------------------------------------------------ live kernel timing
+ * While enabled, CUDA events on the solver stream bracket each pass of
+ * every BiCGSTAB iteration (slot 0: pass A, slot 1: pass B); after a solve
+ * only the passes the device really executed are summed, each with its
+ * algorithmic bytes (compulsory reads and writes of the owned cells). */
+#define BBB_PROF_IT 8192
+#define BBB_PROF_SLOTS 2
 static struct {
   int on, n;
-  cudaEvent_t ev[2 * BBB_PROF_EV];
-  double bytes[BBB_PROF_EV];
-  double ms, tot_bytes;
+  cudaEvent_t ev[(BBB_PROF_SLOTS + 1) * BBB_PROF_IT];
+  double bytes[BBB_PROF_SLOTS * BBB_PROF_IT];
+  double ms[BBB_PROF_SLOTS], kbytes[BBB_PROF_SLOTS];
+  long long launches[BBB_PROF_SLOTS];
   long long iters;
 } g_prof;
 
-static void prof_begin(double bytes)
+/* event e of the current iteration (0 before pass A, 1 after A, 2 after B) */
+static void prof_event(int e)
 {
-  if(!g_prof.on || g_prof.n >= BBB_PROF_EV) return;
-  int i = g_prof.n;
-  if(!g_prof.ev[2 * i]) {
-    cudaEventCreate(&g_prof.ev[2 * i]);
-    cudaEventCreate(&g_prof.ev[2 * i + 1]);
-  }
-  g_prof.bytes[i] = bytes;
-  cudaEventRecord(g_prof.ev[2 * i], g_dev.stream);
+  if(!g_prof.on || g_prof.n >= BBB_PROF_IT) return;
+  int i = g_prof.n * (BBB_PROF_SLOTS + 1) + e;
+  if(!g_prof.ev[i]) cudaEventCreate(&g_prof.ev[i]);
+  cudaEventRecord(g_prof.ev[i], g_dev.stream);
 }
 
-static void prof_end(void)
+static void prof_bytes(int slot, double b)
 {
-  if(!g_prof.on || g_prof.n >= BBB_PROF_EV) return;
-  cudaEventRecord(g_prof.ev[2 * g_prof.n + 1], g_dev.stream);
+  if(!g_prof.on || g_prof.n >= BBB_PROF_IT) return;
+  g_prof.bytes[g_prof.n * BBB_PROF_SLOTS + slot] = b;
+}
+
+static void prof_next(void)
+{
+  if(!g_prof.on || g_prof.n >= BBB_PROF_IT) return;
   g_prof.n++;
 }
 
-/* the stream has been synchronised; `executed` iterations really ran */
-static void prof_collect(int executed)
+/* the stream has been synchronised: `npass` passes really ran, counted in
+ * launch order (A, B, A, B, ...) */
+static void prof_collect(long long npass)
 {
   if(!g_prof.on) return;
-  int m = executed < g_prof.n ? executed : g_prof.n;
-  for(int i = 0; i < m; i++) {
-    float t = 0.f;
-    if(cudaEventElapsedTime(&t, g_prof.ev[2 * i], g_prof.ev[2 * i + 1]) == cudaSuccess) {
-      g_prof.ms += t;
-      g_prof.tot_bytes += g_prof.bytes[i];
-      g_prof.iters++;
+  long long cnt = 0;
+  for(int i = 0; i < g_prof.n && cnt < npass; i++) {
+    for(int sl = 0; sl < BBB_PROF_SLOTS && cnt < npass; sl++, cnt++) {
+      float t = 0.f;
+      int e = i * (BBB_PROF_SLOTS + 1) + sl;
+      if(cudaEventElapsedTime(&t, g_prof.ev[e], g_prof.ev[e + 1]) == cudaSuccess) {
+        g_prof.ms[sl] += t;
+        g_prof.kbytes[sl] += g_prof.bytes[i * BBB_PROF_SLOTS + sl];
+        g_prof.launches[sl]++;
+      }
     }
   }
+  g_prof.iters += npass / 2;
   g_prof.n = 0;
 }
 
 extern "C" void bbb_profile_enable(int on) { g_prof.on = on; g_prof.n = 0; }
 extern "C" void bbb_profile_reset(void)
 {
-  g_prof.ms = 0.; g_prof.tot_bytes = 0.; g_prof.iters = 0; g_prof.n = 0;
+  for(int a = 0; a < BBB_PROF_SLOTS; a++) {
+    g_prof.ms[a] = 0.; g_prof.kbytes[a] = 0.; g_prof.launches[a] = 0;
+  }
+  g_prof.iters = 0; g_prof.n = 0;
 }
 extern "C" void bbb_profile_get(double *ms, long long *iters, double *bytes)
 {
-  *ms = g_prof.ms; *iters = g_prof.iters; *bytes = g_prof.tot_bytes;
+  *ms = 0.; *bytes = 0.;
+  for(int a = 0; a < BBB_PROF_SLOTS; a++) { *ms += g_prof.ms[a]; *bytes += g_prof.kbytes[a]; }
+  *iters = g_prof.iters;
+}
+extern "C" void bbb_profile_get_pass(int pass, double *ms, long long *launches,
+  double *bytes)
+{
+  if(pass < 0 || pass >= BBB_PROF_SLOTS) { *ms = 0.; *launches = 0; *bytes = 0.; return; }
+  *ms = g_prof.ms[pass]; *launches = g_prof.launches[pass]; *bytes = g_prof.kbytes[pass];
 }
 
 /* run iterations until the device says done; the host polls the scalars
@@ -838,33 +942,53 @@ static int drive(bbb_kry *s, LaunchIter launch_iter, int maxit, int batch0)
   return g_dev.kry_host->iter;
 }
 
-/* one BiCGSTAB solve on the current (b, x) of the given precision, with
- * the set-up residual computed by the stencil */
+/* resident blocks per SM of the two passes of precision T and width V */
+template <typename T, int V>
+static int bicg_per_sm(void)
+{
+  static int nb = 0;
+  if(!nb) {
+    int a = resident(k_bicgA<T, V>), b = resident(k_bicgB<T, V>);
+    nb = a < b ? a : b;
+  }
+  return nb;
+}
+
+/* BiCGSTAB iterations after the set-up kernel (s = r0, rh, scalars) */
 template <typename T, int V>
 static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
   const uint8_t *mask, T *r, T *rh, T *p0, T *p1, T *v0, T *v1, T *sv, T *tv,
   T *x, bbb_kry *s, int maxit, int batch0)
 {
   dim3 grd = box_grid(B), blk(TX, TY);
-  int npw = NPW;
   T *pp[2] = {p0, p1}, *vv[2] = {v0, v1};
-  int cur = 0;
-  double it_bytes = (double)n * (17. * sizeof(T) + 3.);
+  int cur = 0, launched = 0;
+  double w = sizeof(T);
   drive(s, [&]() {
-    prof_begin(it_bytes);
-    k_bicg1<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, r, pp[cur],
-      vv[cur], rh, pp[cur ^ 1], vv[cur ^ 1], s, g_dev.partials);
+    /* pass A: first reads s, rh; later s, t, p, v, x, rh; + mask */
+    double a_bytes = launched == 0 ? (double)n * (5. * w + 1.)
+                                   : (double)n * (10. * w + 1.);
+    prof_event(0);
+    prof_bytes(0, a_bytes);
+    k_bicgA<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, sv, tv, pp[cur],
+      vv[cur], rh, r, pp[cur ^ 1], vv[cur ^ 1], x, s, g_dev.partials);
     BBB_LAUNCHED();
-    k_bicg2<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, r, vv[cur ^ 1],
-      sv, tv, s, g_dev.partials);
+    prof_event(1);
+    prof_bytes(1, (double)n * (5. * w + 1.));
+    k_bicgB<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, r, vv[cur ^ 1],
+      rh, sv, tv, s, g_dev.partials);
     BBB_LAUNCHED();
-    k_bicg3<T, V><<<npw, 256, 0, g_dev.stream>>>(n, O, mask, x, pp[cur ^ 1],
-      sv, tv, r, rh, s, g_dev.partials);
-    BBB_LAUNCHED();
-    prof_end();
+    prof_event(2);
+    prof_next();
     cur ^= 1;
+    launched++;
   }, maxit, batch0);
-  prof_collect(g_dev.kry_host->iter + (g_dev.kry_host->s_conv ? 1 : 0));
+  /* passes executed: the opening pass A, B and A of each counted
+   * iteration, and B and A of an uncounted one that ended on ||s|| (a
+   * solve that converged at set-up ran none) */
+  bbb_kry *h = g_dev.kry_host;
+  long long npass = h->first ? 0 : 2LL * h->iter + 1 + (h->s_conv ? 2 : 0);
+  prof_collect(npass);
 }
 
 static opc poisson_op(const bbb_geom &G)
@@ -875,6 +999,19 @@ static opc poisson_op(const bbb_geom &G)
   return O;
 }
 
+template <int V>
+static void poisson_fp64(const boxc &B, const opc &O, long long n, bbb_kry *s)
+{
+  dim3 grd = box_grid(B), blk(TX, TY);
+  k_bicg_setup<double, V><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
+    g_dev.kb, g_dev.kx, g_dev.ks, g_dev.krh, s, g_dev.partials, pp_residual,
+    pp_max_iter);
+  BBB_LAUNCHED();
+  bicgstab_iterations<double, V>(B, O, n, g_dev.mask_p, g_dev.kr, g_dev.krh,
+    g_dev.kp[0], g_dev.kp[1], g_dev.kv[0], g_dev.kv[1], g_dev.ks, g_dev.kt,
+    g_dev.kx, s, pp_max_iter, 1);
+}
+
 int bbb_poisson_solve(int record)
 {
   bbb_dev_require();
@@ -882,34 +1019,21 @@ int bbb_poisson_solve(int record)
   bbb_build_masks();
   bbb_geom G = bbb_make_geom();
   int V = pick_vec(G.nx, sizeof(double));
+  int per_sm = V == 2 ? bicg_per_sm<double, 2>() : bicg_per_sm<double, 1>();
   boxc B = make_box(G.nx, G.ny, G.nz, bc.pW == BBB_PERIODIC,
-    bc.pS == BBB_PERIODIC, bc.pB == BBB_PERIODIC, 0, 0, 0, V);
+    bc.pS == BBB_PERIODIC, bc.pB == BBB_PERIODIC, 0, 0, 0, V, per_sm);
   opc O = poisson_op(G);
   long long n = (long long)G.nx * G.ny * G.nz;
   bbb_kry *s = g_dev.kry;
   k_pp_rhs<<<NPW, 256, 0, g_dev.stream>>>(g_dev.us, g_dev.vs, g_dev.ws,
     g_dev.phi, g_dev.phase, G, rho_f / dt, g_dev.kb, g_dev.kx, s, g_dev.partials);
   BBB_LAUNCHED();
-  dim3 grd = box_grid(B), blk(TX, TY);
-  if(V == 2) {
-    k_bicg_setup<double, 2><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
-      g_dev.kb, g_dev.kx, g_dev.kr, g_dev.krh, g_dev.kp[0], s, g_dev.partials,
-      pp_residual, pp_max_iter);
-    BBB_LAUNCHED();
-    bicgstab_iterations<double, 2>(B, O, n, g_dev.mask_p, g_dev.kr, g_dev.krh,
-      g_dev.kp[0], g_dev.kp[1], g_dev.kv[0], g_dev.kv[1], g_dev.ks, g_dev.kt,
-      g_dev.kx, s, pp_max_iter, 1);
-  } else {
-    k_bicg_setup<double, 1><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
-      g_dev.kb, g_dev.kx, g_dev.kr, g_dev.krh, g_dev.kp[0], s, g_dev.partials,
-      pp_residual, pp_max_iter);
-    BBB_LAUNCHED();
-    bicgstab_iterations<double, 1>(B, O, n, g_dev.mask_p, g_dev.kr, g_dev.krh,
-      g_dev.kp[0], g_dev.kp[1], g_dev.kv[0], g_dev.kv[1], g_dev.ks, g_dev.kt,
-      g_dev.kx, s, pp_max_iter, 1);
-  }
+  bbb_learn_pre_solve();
+  if(V == 2) poisson_fp64<2>(B, O, n, s);
+  else poisson_fp64<1>(B, O, n, s);
   k_pp_writeback<<<NPW, 256, 0, g_dev.stream>>>(g_dev.kx, g_dev.phi, G, s);
   BBB_LAUNCHED();
+  bbb_learn_post_solve();
   BBB_CK(cudaMemcpyAsync(g_dev.kry_host, s, sizeof(bbb_kry),
     cudaMemcpyDeviceToHost, g_dev.stream));
   BBB_CK(cudaStreamSynchronize(g_dev.stream));
@@ -935,11 +1059,13 @@ int bbb_poisson_solve(int record)
 /* ------------------------------------------------ mixed precision
  * Defect correction: the FP64 outer loop forms r = b - A x in FP64 (with
  * ||r||, the stopping test of the FP64 form, and sum x for the mean),
- * hands r to an FP32 Jacobi-BiCGSTAB that solves A e = r from e = 0 to
- * `inner_tol` relative, and accumulates x += e in FP64.  Stops when the
- * FP64 residual meets pp_residual * ||b||, the same test as the FP64 form.
- * Without particle rows the periodic/Neumann operator is singular; the
- * inner right-hand side is then projected onto zero mean. */
+ * hands r to an FP32 Jacobi-BiCGSTAB that solves A e = r from e = 0, and
+ * accumulates x += e in FP64.  The inner target is `inner_tol` relative,
+ * or looser when half the remaining reduction already meets the outer
+ * test.  Stops when the FP64 residual meets pp_residual * ||b||, the same
+ * test as the FP64 form.  Without particle rows the periodic/Neumann
+ * operator is singular; the inner right-hand side is then projected onto
+ * zero mean. */
 
 struct epi_res64 {
   const double *b; float *rf;
@@ -954,9 +1080,9 @@ struct epi_res64 {
       double rv = bb[a] - Ax[a];
       rf[c + a] = (float)rv;
       red[0] += rv * rv;
-      red[1] += xr[a];
       red[2] += rv;
     }
+    (void)xr;
   }
 };
 
@@ -987,17 +1113,20 @@ __global__ void __launch_bounds__(NTHR) k_outer_resid(boxc B, opc O,
       if(s->converged || s->iter >= s->maxit) s->done = 1;
       double mean = project_mean ? red[2] / (double)n : 0.;
       si->sumx = mean;                 /* subtracted by the inner set-up */
-      si->tol = inner_tol * rn;
+      double need = rn > 0. ? 0.5 * s->tol / rn : 1.;
+      si->tol = fmax(inner_tol, need) * rn;
       si->maxit = inner_maxit;
       si->done = s->done;
     }
   }
 }
 
-/* inner set-up from e = 0: r = rh = p = rf - mean, e = 0, (r, r) */
+/* inner set-up from e = 0: s = rh = rf - mean (pass A starts from r = s),
+ * e = 0, (r, r) */
 template <int V>
-__global__ void __launch_bounds__(256) k_inner_setup(long long n, float *rf,
-  float *e, float *rh, float *p, bbb_kry *si, double *partials)
+__global__ void __launch_bounds__(256) k_inner_setup(long long n,
+  const float *__restrict__ rf, float *s0, float *e, float *rh, bbb_kry *si,
+  double *partials)
 {
   if(((volatile bbb_kry *)si)->done) return;
   __shared__ double sh[32];
@@ -1015,7 +1144,7 @@ __global__ void __launch_bounds__(256) k_inner_setup(long long n, float *rf,
       z[a] = 0.f;
       red[0] += (double)rv[a] * (double)rv[a];
     }
-    stv<float, V>(rf, c, rv); stv<float, V>(rh, c, rv); stv<float, V>(p, c, rv);
+    stv<float, V>(s0, c, rv); stv<float, V>(rh, c, rv);
     stv<float, V>(e, c, z);
   }
   if(bbb_grid_partial<1>(red, partials, &si->ticket, sh)) {
@@ -1099,10 +1228,10 @@ static int poisson_mixed(const boxc &BD, const boxc &BF, const opc &O,
       g_dev.kb, g_dev.kx, g_dev.fb, s, si, g_dev.partials, itol, pp_max_iter,
       project, n);
     BBB_LAUNCHED();
-    k_inner_setup<VF><<<NPW, 256, 0, g_dev.stream>>>(n, g_dev.fb, g_dev.fx,
-      g_dev.frh, g_dev.fp[0], si, g_dev.partials);
+    k_inner_setup<VF><<<NPW, 256, 0, g_dev.stream>>>(n, g_dev.fb, g_dev.fs,
+      g_dev.fx, g_dev.frh, si, g_dev.partials);
     BBB_LAUNCHED();
-    bicgstab_iterations<float, VF>(BF, O, n, g_dev.mask_p, g_dev.fb, g_dev.frh,
+    bicgstab_iterations<float, VF>(BF, O, n, g_dev.mask_p, g_dev.fr, g_dev.frh,
       g_dev.fp[0], g_dev.fp[1], g_dev.fv[0], g_dev.fv[1], g_dev.fs, g_dev.ft,
       g_dev.fx, si, pp_max_iter, 4);
     if(bbb_last_status() == BBB_ERR_CUDA) return -1;
@@ -1133,20 +1262,25 @@ int bbb_poisson_solve_mixed(int record)
   bbb_geom G = bbb_make_geom();
   int VD = pick_vec(G.nx, sizeof(double)), VF = pick_vec(G.nx, sizeof(float));
   int px = bc.pW == BBB_PERIODIC, py = bc.pS == BBB_PERIODIC, pz = bc.pB == BBB_PERIODIC;
-  boxc BD = make_box(G.nx, G.ny, G.nz, px, py, pz, 0, 0, 0, VD);
-  boxc BF = make_box(G.nx, G.ny, G.nz, px, py, pz, 0, 0, 0, VF);
+  int smD = resident(k_outer_resid<1>);
+  if(VD == 2) smD = resident(k_outer_resid<2>);
+  int smF = VF == 4 ? bicg_per_sm<float, 4>() : bicg_per_sm<float, 1>();
+  boxc BD = make_box(G.nx, G.ny, G.nz, px, py, pz, 0, 0, 0, VD, smD);
+  boxc BF = make_box(G.nx, G.ny, G.nz, px, py, pz, 0, 0, 0, VF, smF);
   opc O = poisson_op(G);
   long long n = (long long)G.nx * G.ny * G.nz;
   k_pp_rhs<<<NPW, 256, 0, g_dev.stream>>>(g_dev.us, g_dev.vs, g_dev.ws,
     g_dev.phi, g_dev.phase, G, rho_f / dt, g_dev.kb, g_dev.kx, g_dev.kry,
     g_dev.partials);
   BBB_LAUNCHED();
+  bbb_learn_pre_solve();
   int it;
   if(VD == 2 && VF == 4) it = poisson_mixed<2, 4>(BD, BF, O, n, record);
   else if(VD == 2 && VF == 1) it = poisson_mixed<2, 1>(BD, BF, O, n, record);
   else it = poisson_mixed<1, 1>(BD, BF, O, n, record);
   k_pp_writeback<<<NPW, 256, 0, g_dev.stream>>>(g_dev.kx, g_dev.phi, G, g_dev.kry);
   BBB_LAUNCHED();
+  bbb_learn_post_solve();
   bbb_kry *h = g_dev.kry_host;
   if(h->status == BBB_ERR_NONFINITE) bbb_set_status(BBB_ERR_NONFINITE, "pressure-Poisson");
   if(!h->converged) {
@@ -1157,6 +1291,66 @@ int bbb_poisson_solve_mixed(int record)
     }
   }
   return it;
+}
+
+/* ||b - A x|| of the pressure system for an FP64 candidate x (dense), on
+ * the current b (kb) and operator mask: the gate of the learned guess */
+struct epi_rn {
+  const double *b;
+  template <int V>
+  __device__ __forceinline__ void at(long long c, const double (&xr)[V],
+    const double (&Ax)[V], double (&red)[1]) const
+  {
+    double bb[V];
+    ldv<double, V>(b, c, bb);
+#pragma unroll
+    for(int a = 0; a < V; a++) { double r = bb[a] - Ax[a]; red[0] += r * r; }
+    (void)xr;
+  }
+};
+
+template <int V>
+__global__ void __launch_bounds__(NTHR) k_resid_norm(boxc B, opc O,
+  const uint8_t *__restrict__ mask, const double *__restrict__ b,
+  const double *x, double *partials, unsigned int *ticket, double *out)
+{
+  __shared__ double sh[32];
+  __shared__ optab<double> tab;
+  optab_fill<double>(tab, O);
+  prod_x<double> P{x};
+  epi_rn E{b};
+  double red[1] = {0.};
+  tile_stencil<double, V>(B, O, mask, tab, P, E, red);
+  if(bbb_grid_partial<1>(red, partials, ticket, sh)) {
+    bbb_grid_finish_sum<1>(red, partials, ticket, sh);
+    if(threadIdx.x == 0 && threadIdx.y == 0) *out = sqrt(red[0]);
+  }
+}
+
+double bbb_poisson_resid_norm(const double *x)
+{
+  bbb_build_masks();
+  bbb_geom G = bbb_make_geom();
+  int V = pick_vec(G.nx, sizeof(double));
+  static int sm1 = 0, sm2 = 0;
+  if(!sm1) { sm1 = resident(k_resid_norm<1>); sm2 = resident(k_resid_norm<2>); }
+  boxc B = make_box(G.nx, G.ny, G.nz, bc.pW == BBB_PERIODIC,
+    bc.pS == BBB_PERIODIC, bc.pB == BBB_PERIODIC, 0, 0, 0, V, V == 2 ? sm2 : sm1);
+  opc O = poisson_op(G);
+  dim3 grd = box_grid(B), blk(TX, TY);
+  if(V == 2)
+    k_resid_norm<2><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p, g_dev.kb,
+      x, g_dev.partials, g_dev.red_ticket + 10, g_dev.red_dev + 48);
+  else
+    k_resid_norm<1><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p, g_dev.kb,
+      x, g_dev.partials, g_dev.red_ticket + 10, g_dev.red_dev + 48);
+  BBB_LAUNCHED();
+  double r = -1.;
+  BBB_CK(cudaMemcpyAsync(g_dev.red_host, g_dev.red_dev + 48, sizeof(double),
+    cudaMemcpyDeviceToHost, g_dev.stream));
+  BBB_CK(cudaStreamSynchronize(g_dev.stream));
+  r = g_dev.red_host[0];
+  return r;
 }
 
 /* src/cuda_bicgstab.cu:715-1073 */
@@ -1186,9 +1380,10 @@ extern "C" void cuda_PP_rhs(int dev)
 template <typename T>
 struct prod_c1 {
   const T *r, *p; const uint8_t *mask; T beta; int first;
+  typedef T Raw;
   template <int V>
   __device__ __forceinline__ void ev(long long c, T (&raw)[V], T (&q)[V],
-    const T *dinv) const
+    const T *dinv, bool own, double (&red)[1]) const
   {
     T pp[V];
     ldv<T, V>(p, c, pp);
@@ -1205,6 +1400,7 @@ struct prod_c1 {
     }
 #pragma unroll
     for(int a = 0; a < V; a++) q[a] = raw[a];
+    (void)own; (void)red;
   }
 };
 template <typename T>
@@ -1347,9 +1543,11 @@ int bbb_helmholtz_solve(int comp)
   int nx = G.nx + (comp == 0), ny = G.ny + (comp == 1), nz = G.nz + (comp == 2);
   int per[3][3] = {{bc.uW, bc.uS, bc.uB}, {bc.vW, bc.vS, bc.vB}, {bc.wW, bc.wS, bc.wB}};
   int V = pick_vec(nx, sizeof(double));
+  static int sm1 = 0, sm2 = 0;
+  if(!sm1) { sm1 = resident(k_cg1<double, 1>); sm2 = resident(k_cg1<double, 2>); }
   boxc B = make_box(nx, ny, nz, per[comp][0] == BBB_PERIODIC,
     per[comp][1] == BBB_PERIODIC, per[comp][2] == BBB_PERIODIC,
-    comp == 0, comp == 1, comp == 2, V);
+    comp == 0, comp == 1, comp == 2, V, V == 2 ? sm2 : sm1);
   opc O;
   O.wx = 0.5 * nu * dt * (1. / (G.dx * G.dx));
   O.wy = 0.5 * nu * dt * (1. / (G.dy * G.dy));
@@ -1421,7 +1619,7 @@ extern "C" void cuda_wstar_helmholtz(int rank) { (void)rank; helmholtz_entry(2);
  * the process exits.  No cudaMalloc, cudaFree or allocating library call
  * is made. */
 #define BBB_STATIC_MAX_CELLS (64LL * 64LL * 64LL)
-#define BBB_STATIC_PARTIALS (16384LL * 4LL)
+#define BBB_STATIC_PARTIALS (16384LL * 5LL)
 #define BBB_STATIC_SCRATCH_BYTES \
   (256LL + 256LL * ((BBB_STATIC_PARTIALS * 8LL + 255LL) / 256LL) \
    + 256LL * ((BBB_STATIC_MAX_CELLS + 255LL) / 256LL) \
@@ -1435,24 +1633,22 @@ static __device__ __align__(256) unsigned char
 static unsigned char *g_static_addr[64];
 
 template <int V>
-static int static_iterations(const boxc &B, const opc &O, long long n,
-  const uint8_t *mask, double *b, double *x, double *r, double *rh,
-  double *const *pp, double *const *vv, double *sv, double *tv, bbb_kry *s,
-  double *partials, double tol, int maxit, cudaStream_t st, bbb_kry *h)
+static int static_iterations(const boxc &B, const opc &O, const uint8_t *mask,
+  double *b, double *x, double *r, double *rh, double *const *pp,
+  double *const *vv, double *sv, double *tv, bbb_kry *s, double *partials,
+  double tol, int maxit, cudaStream_t st, bbb_kry *h)
 {
   dim3 grd = box_grid(B), blk(TX, TY);
-  k_bicg_setup<double, V><<<grd, blk, 0, st>>>(B, O, mask, b, x, r, rh, pp[0],
-    s, partials, tol, maxit);
+  k_bicg_setup<double, V><<<grd, blk, 0, st>>>(B, O, mask, b, x, sv, rh, s,
+    partials, tol, maxit);
   if(cudaPeekAtLastError() != cudaSuccess) return BBB_ERR_CUDA;
   int cur = 0, batch = 1, total = 0;
   for(;;) {
     for(int q = 0; q < batch; q++) {
-      k_bicg1<double, V><<<grd, blk, 0, st>>>(B, O, mask, r, pp[cur], vv[cur],
-        rh, pp[cur ^ 1], vv[cur ^ 1], s, partials);
-      k_bicg2<double, V><<<grd, blk, 0, st>>>(B, O, mask, r, vv[cur ^ 1], sv,
-        tv, s, partials);
-      k_bicg3<double, V><<<NPW, 256, 0, st>>>(n, O, mask, x, pp[cur ^ 1], sv,
-        tv, r, rh, s, partials);
+      k_bicgA<double, V><<<grd, blk, 0, st>>>(B, O, mask, sv, tv, pp[cur],
+        vv[cur], rh, r, pp[cur ^ 1], vv[cur ^ 1], x, s, partials);
+      k_bicgB<double, V><<<grd, blk, 0, st>>>(B, O, mask, r, vv[cur ^ 1], rh,
+        sv, tv, s, partials);
       cur ^= 1;
     }
     total += batch;
@@ -1510,9 +1706,10 @@ extern "C" int bbb_PP_bicgstab_static(int nx, int ny, int nz, double dx,
   G.fz_s1 = nx + 2; G.fz_s2 = (nx + 2) * (ny + 2);
   G.dx = dx; G.dy = dy; G.dz = dz;
   int V = pick_vec(nx, sizeof(double));
-  boxc B = make_box(nx, ny, nz, perx, pery, perz, 0, 0, 0, V);
+  int per_sm = V == 2 ? bicg_per_sm<double, 2>() : bicg_per_sm<double, 1>();
+  boxc B = make_box(nx, ny, nz, perx, pery, perz, 0, 0, 0, V, per_sm);
   dim3 grd = box_grid(B);
-  if((long long)grd.x * grd.y * grd.z > BBB_STATIC_PARTIALS / 4) return BBB_ERR_TOO_LARGE;
+  if((long long)grd.x * grd.y * grd.z * 5 > BBB_STATIC_PARTIALS) return BBB_ERR_TOO_LARGE;
   opc O;
   O.wx = 1. / (dx * dx); O.wy = 1. / (dy * dy); O.wz = 1. / (dz * dz);
   O.helm = 0;
@@ -1523,9 +1720,9 @@ extern "C" int bbb_PP_bicgstab_static(int nx, int ny, int nz, double dx,
     G, rho_f_ / dt_, b, x, s, partials);
   bbb_kry h;
   int rc = V == 2
-    ? static_iterations<2>(B, O, n, mask, b, x, r, rh, pp, vv, sv, tv, s,
+    ? static_iterations<2>(B, O, mask, b, x, r, rh, pp, vv, sv, tv, s,
         partials, tol, maxit, st, &h)
-    : static_iterations<1>(B, O, n, mask, b, x, r, rh, pp, vv, sv, tv, s,
+    : static_iterations<1>(B, O, mask, b, x, r, rh, pp, vv, sv, tv, s,
         partials, tol, maxit, st, &h);
   if(rc != BBB_OK) return rc;
   k_pp_writeback<<<NPW, 256, 0, st>>>(x, phi_d, G, s);

@@ -1264,10 +1264,8 @@ extern "C" void cuda_store_coeffs(void)
 }
 
 /* ------------------------------------------------ Newton-Euler
- * collision_init (src/bluebottle_kernel.cu:2400), spring_parts (:3592),
- * move_parts_a/b and rotate (:2247-2398).  Lubrication and contact forces
- * (collision_parts, collision_walls) are not part of this build; the
- * interaction force and torque are zero. */
+ * move_parts_a/b and rotate (src/bluebottle_kernel.cu:2247-2398); the
+ * interaction forces they integrate are computed below. */
 __device__ void d_rotate(double qr, double qi, double qj, double qk,
   double *pi, double *pj, double *pk)
 {
@@ -1278,21 +1276,6 @@ __device__ void d_rotate(double qr, double qi, double qj, double qk,
   *pi = qr * Pi + qi * Pr + qj * Pk - qk * Pj;
   *pj = qr * Pj - qi * Pk + qj * Pr + qk * Pi;
   *pk = qr * Pk + qi * Pj - qj * Pi + qk * Pr;
-}
-
-__device__ void d_springs(part_struct *q)
-{
-  q->iFx = 0.; q->iFy = 0.; q->iFz = 0.;
-  q->iLx = 0.; q->iLy = 0.; q->iLz = 0.;
-  if(q->spring_k > 0.) {
-    double nx = q->x - q->spring_x, ny = q->y - q->spring_y, nz = q->z - q->spring_z;
-    double n = sqrt(nx * nx + ny * ny + nz * nz);
-    double lx = q->spring_l * (nx / n), ly = q->spring_l * (ny / n),
-           lz = q->spring_l * (nz / n);
-    q->kFx = -q->spring_k * (q->x - q->spring_x - lx);
-    q->kFy = -q->spring_k * (q->y - q->spring_y - ly);
-    q->kFz = -q->spring_k * (q->z - q->spring_z - lz);
-  }
 }
 
 __device__ void d_move(part_struct *q, int final, double dt, double rho_f,
@@ -1354,35 +1337,519 @@ __device__ void d_move(part_struct *q, int final, double dt, double rho_f,
   }
 }
 
-__global__ void k_move_parts(part_struct *parts, int np, int final, double dt,
-  double rho_f, g_struct g, gradP_struct gp, bbb_geom G)
+/* ------------------------------------------------ interaction forces
+ * Lubrication and Hertz contact between spheres and with Neumann walls,
+ * springs (src/bluebottle_kernel.cu: collision_init :2400, bin_fill :2422,
+ * bin_start :2454, collision_parts :2500, collision_walls :2875,
+ * spring_parts :3592; sequence src/cuda_bluebottle.cu:4317-4554).  One
+ * thread per particle does the reference's four per-particle kernels in
+ * their order (each writes only its own particle and reads the others'
+ * kinematics, which these kernels do not change).  Neighbours come from a
+ * bin grid (binDom_init src/particle.c:598) built on the device by count,
+ * scan, scatter and a per-bin sort by index, so a particle's partners are
+ * visited in the reference's order: bins z, y, x from -1 to 1, particles
+ * by index within a bin (its sort by bin is stable).  Kept as the
+ * reference computes them: interactionLengthRatio enters as an int; the
+ * contact-list searches read and write one slot past iSt / St (the bytes
+ * that follow in part_struct); every wall's contact branch uses the south
+ * wall's Dirichlet velocities; the east-wall contact torque takes the
+ * function-scope Ftx (0 unless assigned earlier in the call); the x walls'
+ * contact slip takes omega_x in place of omega_y. */
+#define D_MAXN BBB_MAX_NEIGHBORS
+
+struct bin_geom {
+  int xn, yn, zn, s1, s2, s3;
+  double xs, ys, zs, dx, dy, dz;
+};
+
+struct coll_args {
+  double mu, rho_f, nu, dt;
+  int ilr;                        /* (int) interactionLengthRatio */
+  double xs, xe, xl, ys, ye, yl, zs, ze, zl;
+  BC bc;
+};
+
+static struct {
+  int s3, np;
+  bin_geom bg;
+  int *cnt, *start, *fill, *list;
+} g_bins;
+
+__device__ __forceinline__ int d_ist_get(const part_struct *q, int k)
+{
+  int v;
+  memcpy(&v, (const char *)q->iSt + sizeof(int) * k, sizeof(int));
+  return v;
+}
+__device__ __forceinline__ void d_ist_set(part_struct *q, int k, int v)
+{ memcpy((char *)q->iSt + sizeof(int) * k, &v, sizeof(int)); }
+__device__ __forceinline__ double d_st_get(const part_struct *q, int k)
+{
+  double v;
+  memcpy(&v, (const char *)q->St + sizeof(double) * k, sizeof(double));
+  return v;
+}
+__device__ __forceinline__ void d_st_set(part_struct *q, int k, double v)
+{ memcpy((char *)q->St + sizeof(double) * k, &v, sizeof(double)); }
+
+__device__ void d_contact_forget(part_struct *q, int key)
+{
+  int k = 0;
+  while(d_ist_get(q, k) != key && k < D_MAXN) k++;
+  if(d_ist_get(q, k) == key) { d_ist_set(q, k, -1); d_st_set(q, k, 0.); }
+}
+
+__device__ int d_contact_slot(part_struct *q, int key, double St)
+{
+  int k = 0;
+  while(d_ist_get(q, k) != key && k < D_MAXN) k++;
+  if(k == D_MAXN) {
+    k = 0;
+    while(d_ist_get(q, k) != -1 && k < D_MAXN) k++;
+    d_ist_set(q, k, key);
+    d_st_set(q, k, St);
+  }
+  return k;
+}
+
+__device__ __forceinline__ double d_min_image(double a, double b, double L,
+  int periodic)
+{
+  double r = a - b, r1 = a - (b + L), r2 = a - (b - L);
+  if(r1 * r1 < r * r) r = r1;
+  if(r2 * r2 < r * r) r = r2;
+  return periodic * r + (!periodic) * (a - b);
+}
+
+/* force and torque on particle pi from particle pj */
+__device__ void d_pair_force(part_struct *pi, const part_struct *pj, int j,
+  const coll_args &A)
+{
+  double eps = 0.01, mu = A.mu, rhof = A.rho_f, nu = A.nu, dt = A.dt;
+  double ai = pi->r, aj = pj->r, B = aj / ai, hN = A.ilr * pi->r;
+  double rx = d_min_image(pi->x, pj->x, A.xl, A.bc.uW == BBB_PERIODIC);
+  double ry = d_min_image(pi->y, pj->y, A.yl, A.bc.vS == BBB_PERIODIC);
+  double rz = d_min_image(pi->z, pj->z, A.zl, A.bc.wB == BBB_PERIODIC);
+  double ux = 0.5 * ((pi->u - pj->u) + (pi->u0 - pj->u0));
+  double uy = 0.5 * ((pi->v - pj->v) + (pi->v0 - pj->v0));
+  double uz = 0.5 * ((pi->w - pj->w) + (pi->w0 - pj->w0));
+  double r = sqrt(rx * rx + ry * ry + rz * rz);
+  double omx = 0.5 * ((pi->ox + pj->ox) + (pi->ox0 + pj->ox0));
+  double omy = 0.5 * ((pi->oy + pj->oy) + (pi->oy0 + pj->oy0));
+  double omz = 0.5 * ((pi->oz + pj->oz) + (pi->oz0 + pj->oz0));
+  double h = r - ai - aj;
+  double nx = rx / r, ny = ry / r, nz = rz / r;
+  double udotn = ux * nx + uy * ny + uz * nz;
+  double unx = udotn * nx, uny = udotn * ny, unz = udotn * nz;
+  double utx = ux - unx, uty = uy - uny, utz = uz - unz;
+  double opB = 1 + B;
+  double ocnx = omy * nz - omz * ny, ocny = -omx * nz + omz * nx, ocnz = omx * ny - omy * nx;
+  double ucnx = uty * nz - utz * ny, ucny = -utx * nz + utz * nx, ucnz = utx * ny - uty * nx;
+  double Fnx, Fny, Fnz, Ftx, Fty, Ftz, Lox, Loy, Loz;
+  if(h < hN && h > 0) {
+    d_contact_forget(pi, j);
+    if(h < eps * pi->r) h = eps * pi->r;
+    double ah = ai / h - ai / hN, lnah = log(hN / h);
+    Fnx = -1. * B * B / (opB * opB) * ah - B * (1. + 7. * B + B * B) / (5. * opB * opB * opB) * lnah;
+    Fny = Fnx; Fnz = Fnx;
+    Fnx *= 6. * PI * mu * ai * unx;
+    Fny *= 6. * PI * mu * ai * uny;
+    Fnz *= 6. * PI * mu * ai * unz;
+    Ftx = -6. * PI * mu * ai * utx * 4. * B * (2. + B + 2. * B * B) / (15. * opB * opB * opB) * lnah;
+    Fty = -6. * PI * mu * ai * uty * 4. * B * (2. + B + 2. * B * B) / (15. * opB * opB * opB) * lnah;
+    Ftz = -6. * PI * mu * ai * utz * 4. * B * (2. + B + 2. * B * B) / (15. * opB * opB * opB) * lnah;
+    Ftx += 8. * PI * mu * ai * ai * ocnx * B * (4. + B) / (10. * opB * opB) * lnah;
+    Fty += 8. * PI * mu * ai * ai * ocny * B * (4. + B) / (10. * opB * opB) * lnah;
+    Ftz += 8. * PI * mu * ai * ai * ocnz * B * (4. + B) / (10. * opB * opB) * lnah;
+    Lox = -8. * PI * mu * ai * ai * ucnx * B * (4. + B) / (10. * opB * opB) * lnah;
+    Loy = -8. * PI * mu * ai * ai * ucny * B * (4. + B) / (10. * opB * opB) * lnah;
+    Loz = -8. * PI * mu * ai * ai * ucnz * B * (4. + B) / (10. * opB * opB) * lnah;
+    Lox += -8. * PI * mu * ai * ai * ai * omx * 2. * B / (5. * opB) * lnah;
+    Loy += -8. * PI * mu * ai * ai * ai * omy * 2. * B / (5. * opB) * lnah;
+    Loz += -8. * PI * mu * ai * ai * ai * omz * 2. * B / (5. * opB) * lnah;
+  } else {
+    Fnx = 0; Fny = 0; Fnz = 0; Ftx = 0; Fty = 0; Ftz = 0; Lox = 0; Loy = 0; Loz = 0;
+  }
+  if(h < 0) {
+    int q = d_contact_slot(pi, j, 1. / 9. * pi->rho / rhof * 2. * pi->r * fabs(udotn) / nu);
+    double Vx = -utx + 0.5 * (ai + aj + h) * ocnx;
+    double Vy = -uty + 0.5 * (ai + aj + h) * ocny;
+    double Vz = -utz + 0.5 * (ai + aj + h) * ocnz;
+    double Hi = 0.5 * pi->E / (1. + pi->sigma);
+    double kt = 8. / ((1. - pi->sigma * pi->sigma) / Hi + (1. - pi->sigma * pi->sigma) / Hi)
+      / sqrt(1. / ai) * sqrt(-h);
+    double Vdotn = Vx * nx + Vy * ny + Vz * nz;
+    double sx = (Vx - Vdotn * nx) * dt, sy = (Vy - Vdotn * ny) * dt, sz = (Vz - Vdotn * nz) * dt;
+    double k = 4. / 3. / ((1. - pi->sigma * pi->sigma) / pi->E
+      + (1. - pj->sigma * pj->sigma) / pj->E) / sqrt(1. / ai + 1. / aj);
+    double xcx0 = 1.e-4;
+    double e = pi->e_dry + (1. + pi->e_dry) / d_st_get(pi, q) * log(xcx0);
+    if(e < 0) e = 0;
+    double alpha = -2.263 * pow(e, 0.3948) + 2.22;
+    double eta = alpha * sqrt(4. / 3. * PI * ai * ai * ai * pi->rho * k * sqrt(-h));
+    Fnx = (sqrt(-h * h * h) * k - eta * udotn) * nx;
+    Fny = (sqrt(-h * h * h) * k - eta * udotn) * ny;
+    Fnz = (sqrt(-h * h * h) * k - eta * udotn) * nz;
+    double cf = 0.5 * (pi->coeff_fric + pj->coeff_fric);
+    Ftx = -kt * sx; Fty = -kt * sy; Ftz = -kt * sz;
+    double Ftdotn = Ftx * nx + Fty * ny + Ftz * nz;
+    Ftx = Ftx - Ftdotn * nx; Fty = Fty - Ftdotn * ny; Ftz = Ftz - Ftdotn * nz;
+    double Ft = sqrt(Ftx * Ftx + Fty * Fty + Ftz * Ftz);
+    double Fn = sqrt(Fnx * Fnx + Fny * Fny + Fnz * Fnz);
+    if(Ft > cf * Fn) {
+      Ftx = cf * Fn * Ftx / Ft; Fty = cf * Fn * Fty / Ft; Ftz = cf * Fn * Ftz / Ft;
+    }
+    Lox = -(ai + 0.5 * h) * ((Fny + Fty) * nz - (Fnz + Ftz) * ny);
+    Loy = (ai + 0.5 * h) * ((Fnx + Ftx) * nz - (Fnz + Ftz) * nx);
+    Loz = -(ai + 0.5 * h) * ((Fnx + Ftx) * ny - (Fny + Fty) * nx);
+  }
+  pi->iFx += Fnx + Ftx;
+  pi->iFy += Fny + Fty;
+  pi->iFz += Fnz + Ftz;
+  pi->iLx += Lox;
+  pi->iLy += Loy;
+  pi->iLz += Loz;
+}
+
+/* one wall: ax the normal axis, hi = 0 for W/S/B, 1 for E/N/T */
+__device__ void d_wall_force(part_struct *p, int ax, int hi, const coll_args &A,
+  double *Ftx_scope)
+{
+  const BC &bc = A.bc;
+  double eps = 0.01, mu = A.mu, rhof = A.rho_f, nu = A.nu, dt = A.dt;
+  double ai = p->r, hN = A.ilr * p->r;
+  double pos[3] = {p->x, p->y, p->z}, vel[3] = {p->u, p->v, p->w};
+  double vel0[3] = {p->u0, p->v0, p->w0};
+  double om[3] = {p->ox, p->oy, p->oz}, om0[3] = {p->ox0, p->oy0, p->oz0};
+  double wallpos, wv[3];
+  int press, key = -10 - (2 * ax + hi);
+  if(ax == 0) {
+    wallpos = hi ? A.xe - bc.dsE : A.xs + bc.dsW;
+    press = hi ? bc.pE : bc.pW;
+    wv[0] = hi ? bc.uED : bc.uWD; wv[1] = hi ? bc.vED : bc.vWD; wv[2] = hi ? bc.wED : bc.wWD;
+  } else if(ax == 1) {
+    wallpos = hi ? A.ye - bc.dsN : A.ys + bc.dsS;
+    press = hi ? bc.pN : bc.pS;
+    wv[0] = hi ? bc.uND : bc.uSD; wv[1] = hi ? bc.vND : bc.vSD; wv[2] = hi ? bc.wND : bc.wSD;
+  } else {
+    wallpos = hi ? A.ze - bc.dsT : A.zs + bc.dsB;
+    press = hi ? bc.pT : bc.pB;
+    wv[0] = hi ? bc.uTD : bc.uBD; wv[1] = hi ? bc.vTD : bc.vBD; wv[2] = hi ? bc.wTD : bc.wBD;
+  }
+  double sd[3] = {bc.uSD, bc.vSD, bc.wSD};
+  double h = fabs(pos[ax] - wallpos) - ai;
+  double isTrue = (press == BBB_NEUMANN);
+  int t1 = ax == 0 ? 1 : 0, t2 = ax == 2 ? 1 : 2;
+  double sg = hi ? -1. : 1.;
+  if(h < hN && h > 0) {
+    d_contact_forget(p, key);
+    if(h < eps * p->r) h = eps * p->r;
+    double ah = ai / h - ai / hN, lnah = log(hN / h);
+    double Un = vel[ax] - wv[ax];
+    double Ut[3] = {vel[0] - wv[0], vel[1] - wv[1], vel[2] - wv[2]};
+    Ut[ax] = 0.;
+    double F[3] = {0., 0., 0.}, Ft[3] = {0., 0., 0.}, L[3] = {0., 0., 0.};
+    F[ax] = -6. * PI * mu * ai * Un * ah;
+    Ft[t1] = -6. * PI * mu * ai * Ut[t1] * 8. / 15. * lnah;
+    Ft[t2] = -6. * PI * mu * ai * Ut[t2] * 8. / 15. * lnah;
+    double so = (ax == 1) ? -sg : sg;
+    Ft[t1] += so * 8. * PI * mu * ai * ai * om[t2] * 1. / 10. * lnah;
+    Ft[t2] += -so * 8. * PI * mu * ai * ai * om[t1] * 1. / 10. * lnah;
+    L[t1] = -so * 8. * PI * mu * ai * ai * Ut[t2] * 1. / 10. * lnah;
+    L[t2] = so * 8. * PI * mu * ai * ai * Ut[t1] * 1. / 10. * lnah;
+    L[t1] += -8. * PI * mu * ai * ai * ai * om[t1] * 2. / 5. * lnah;
+    L[t2] += -8. * PI * mu * ai * ai * ai * om[t2] * 2. / 5. * lnah;
+    *Ftx_scope = Ft[0];
+    p->iFx += isTrue * (F[0] + Ft[0]);
+    p->iFy += isTrue * (F[1] + Ft[1]);
+    p->iFz += isTrue * (F[2] + Ft[2]);
+    p->iLx += isTrue * L[0];
+    p->iLy += isTrue * L[1];
+    p->iLz += isTrue * L[2];
+  }
+  if(h < 0) {
+    double Un = sg * (vel[ax] - wv[ax]);
+    double Ut1 = 0.5 * (vel[t1] + vel0[t1]) - sd[t1];
+    double Ut2 = 0.5 * (vel[t2] + vel0[t2]) - sd[t2];
+    int q = d_contact_slot(p, key, 1. / 9. * p->rho / rhof * 2. * p->r * fabs(Un) / nu);
+    double o[3] = {0.5 * (om[0] + om0[0]), 0.5 * (om[1] + om0[1]), 0.5 * (om[2] + om0[2])};
+    double so = (ax == 1) ? -1. : 1.;
+    double o2 = ax == 0 ? o[0] : o[t1];
+    double V1 = sg * (Ut1 - so * (ai + 0.5 * h) * o[t2]);
+    double V2 = sg * (Ut2 + so * (ai + 0.5 * h) * o2);
+    double Hi = 0.5 * p->E / (1. + p->sigma);
+    double kt = 8. / ((1. - p->sigma * p->sigma) / Hi + (1. - p->sigma * p->sigma) / Hi)
+      / sqrt(1. / ai) * sqrt(-h);
+    double s1 = V1 * dt, s2 = V2 * dt;
+    double k = 4. / 3. / ((1. - p->sigma * p->sigma) / p->E + (1. - p->sigma * p->sigma) / p->E)
+      / sqrt(1. / ai);
+    double xcx0 = 1.e-4;
+    double e = p->e_dry + (1. + p->e_dry) / d_st_get(p, q) * log(xcx0);
+    if(e < 0) e = 0;
+    double alpha = -2.263 * pow(e, 0.3948) + 2.22;
+    double eta = alpha * sqrt(4. / 3. * PI * ai * ai * ai * p->rho * k * sqrt(-h));
+    double cf = p->coeff_fric;
+    double F1 = -kt * s1, F2 = -kt * s2;
+    double Ft = sqrt(F1 * F1 + F2 * F2);
+    double Fn = sqrt(-h * h * h) * k - eta * Un;
+    if(Ft > fabs(cf * Fn)) {
+      F1 = cf * Fn * F1 / Ft;
+      F2 = cf * Fn * F2 / Ft;
+    }
+    double arm = ai + 0.5 * h;
+    if(ax == 0) {
+      p->iFx += sg * isTrue * Fn;
+      p->iFy += isTrue * F1;
+      p->iFz += isTrue * F2;
+      if(!hi) { p->iLy += isTrue * arm * F2; p->iLz -= isTrue * arm * F1; }
+      else { p->iLy -= isTrue * arm * F2; p->iLz += isTrue * arm * (*Ftx_scope); }
+    } else if(ax == 1) {
+      p->iFx += isTrue * F1;
+      p->iFy += sg * isTrue * Fn;
+      p->iFz += isTrue * F2;
+      if(!hi) { p->iLx -= isTrue * arm * F2; p->iLz += isTrue * arm * F1; }
+      else { p->iLx += isTrue * arm * F2; p->iLz -= isTrue * arm * F1; }
+    } else {
+      p->iFx += isTrue * F1;
+      p->iFy += isTrue * F2;
+      p->iFz += sg * isTrue * Fn;
+      if(!hi) { p->iLx += isTrue * arm * F2; p->iLy -= isTrue * arm * F1; }
+      else { p->iLx -= isTrue * arm * F2; p->iLy += isTrue * arm * F1; }
+    }
+  }
+}
+
+__global__ void k_bin_count(part_struct *parts, int np, bin_geom bg, int *cnt)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if(i >= np) return;
   part_struct *q = &parts[i];
-  d_springs(q);
-  d_move(q, 0, dt, rho_f, g, gp, G);
-  d_springs(q);
-  if(final) d_move(q, 1, dt, rho_f, g, gp, G);
+  int ib = (int)floor((q->x - bg.xs) / bg.dx);
+  int jb = (int)floor((q->y - bg.ys) / bg.dy);
+  int kb = (int)floor((q->z - bg.zs) / bg.dz);
+  int c = ib + jb * bg.s1 + kb * bg.s2;
+  q->bin = c;
+  if(c >= 0 && c < bg.s3) atomicAdd(&cnt[c], 1);
+}
+
+/* exclusive scan of the bin counts (one block) */
+__global__ void k_bin_scan(const int *cnt, int *start, int n)
+{
+  __shared__ int part[1024];
+  int t = threadIdx.x, nt = blockDim.x;
+  int per = (n + nt - 1) / nt, a = t * per, b = min(n, a + per);
+  int s = 0;
+  for(int c = a; c < b; c++) s += cnt[c];
+  part[t] = s;
+  __syncthreads();
+  if(t == 0) {
+    int run = 0;
+    for(int q = 0; q < nt; q++) { int v = part[q]; part[q] = run; run += v; }
+  }
+  __syncthreads();
+  s = part[t];
+  for(int c = a; c < b; c++) { start[c] = s; s += cnt[c]; }
+}
+
+__global__ void k_bin_scatter(const part_struct *parts, int np, bin_geom bg,
+  const int *start, int *fill, int *list)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= np) return;
+  int c = parts[i].bin;
+  if(c < 0 || c >= bg.s3) return;
+  int slot = atomicAdd(&fill[c], 1);
+  list[start[c] + slot] = i;
+}
+
+/* particles of each bin by index (the order of a stable sort by bin) */
+__global__ void k_bin_sort(const int *start, const int *cnt, int *list, int n)
+{
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if(c >= n) return;
+  int a = start[c], m = cnt[c];
+  for(int x = 1; x < m; x++) {
+    int v = list[a + x], y = x - 1;
+    while(y >= 0 && list[a + y] > v) { list[a + y + 1] = list[a + y]; y--; }
+    list[a + y + 1] = v;
+  }
+}
+
+__global__ void k_interact(part_struct *parts, int np, bin_geom bg,
+  const int *start, const int *cnt, const int *list, coll_args A)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= np) return;
+  part_struct *pi = &parts[i];
+  pi->iFx = 0.; pi->iFy = 0.; pi->iFz = 0.;
+  pi->iLx = 0.; pi->iLy = 0.; pi->iLz = 0.;
+  if(np > 1) {
+    int bin = pi->bin;
+    int kbin = bin / bg.s2, jbin = (bin - kbin * bg.s2) / bg.s1;
+    int ibin = bin - kbin * bg.s2 - jbin * bg.s1;
+    int fW = 0, fE = bg.xn - 1, fS = 0, fN = bg.yn - 1, fB = 0, fT = bg.zn - 1;
+    int xnb = bg.xn > 2, ynb = bg.yn > 2, znb = bg.zn > 2;
+    const BC &bc = A.bc;
+    for(int n = -1; n <= 1; n++) {
+      int ks;
+      if((n == -1 && kbin == fB && bc.uB != BBB_PERIODIC) ||
+         (n == 1 && kbin == fT && bc.uT != BBB_PERIODIC) ||
+         (n == -1 && kbin == fB && bc.uB == BBB_PERIODIC && znb == 0) ||
+         (n == 1 && kbin == fT && bc.uT == BBB_PERIODIC && znb == 0)) continue;
+      else if(n == -1 && kbin == fB) ks = fT * bg.s2;
+      else if(n == 1 && kbin == fT) ks = fB * bg.s2;
+      else ks = (kbin + n) * bg.s2;
+      for(int m = -1; m <= 1; m++) {
+        int js;
+        if((m == -1 && jbin == fS && bc.uS != BBB_PERIODIC) ||
+           (m == 1 && jbin == fN && bc.uN != BBB_PERIODIC) ||
+           (m == -1 && jbin == fS && bc.uS == BBB_PERIODIC && ynb == 0) ||
+           (m == 1 && jbin == fN && bc.uN == BBB_PERIODIC && ynb == 0)) continue;
+        else if(m == -1 && jbin == fS) js = fN * bg.s1;
+        else if(m == 1 && jbin == fN) js = fS * bg.s1;
+        else js = (jbin + m) * bg.s1;
+        for(int l = -1; l <= 1; l++) {
+          int is;
+          if((l == -1 && ibin == fW && bc.uW != BBB_PERIODIC) ||
+             (l == 1 && ibin == fE && bc.uE != BBB_PERIODIC) ||
+             (l == -1 && ibin == fW && bc.uW == BBB_PERIODIC && xnb == 0) ||
+             (l == 1 && ibin == fE && bc.uE == BBB_PERIODIC && xnb == 0)) continue;
+          else if(l == -1 && ibin == fW) is = fE;
+          else if(l == 1 && ibin == fE) is = fW;
+          else is = ibin + l;
+          int adj = is + js + ks;
+          if(adj < 0 || adj >= bg.s3) continue;
+          int a = start[adj], m2 = cnt[adj];
+          for(int t = a; t < a + m2; t++) {
+            int j = list[t];
+            if(j != i) d_pair_force(pi, &parts[j], j, A);
+          }
+        }
+      }
+    }
+  }
+  if(pi->spring_k > 0.) {
+    double nx = pi->x - pi->spring_x, ny = pi->y - pi->spring_y, nz = pi->z - pi->spring_z;
+    double n = sqrt(nx * nx + ny * ny + nz * nz);
+    double lx = pi->spring_l * (nx / n), ly = pi->spring_l * (ny / n),
+           lz = pi->spring_l * (nz / n);
+    pi->kFx = -pi->spring_k * (pi->x - pi->spring_x - lx);
+    pi->kFy = -pi->spring_k * (pi->y - pi->spring_y - ly);
+    pi->kFz = -pi->spring_k * (pi->z - pi->spring_z - lz);
+  }
+  double Ftx_scope = 0.;
+  for(int w = 0; w < 6; w++) d_wall_force(pi, w / 2, w % 2, A, &Ftx_scope);
+}
+
+__global__ void k_move(part_struct *parts, int np, int final, double dt,
+  double rho_f, g_struct g, gradP_struct gp, bbb_geom G)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= np) return;
+  d_move(&parts[i], final, dt, rho_f, g, gp, G);
+}
+
+/* bin grid of binDom_init (src/particle.c:598) from the particle radii */
+static void bins_setup(void)
+{
+  if(g_bins.cnt && g_bins.np == nparts) return;
+  double rmax = 0;
+  for(int i = 0; i < nparts; i++)
+    rmax = rmax + (parts[i].r > rmax) * (parts[i].r - rmax);
+  double ilr = interactionLengthRatio;
+  bin_geom &b = g_bins.bg;
+  b.xs = Dom.xs; b.ys = Dom.ys; b.zs = Dom.zs;
+  b.xn = (int)floor(Dom.xl / (2. * rmax + ilr * rmax));
+  if(b.xn == 0) { b.xn = 1; b.dx = Dom.xl; } else b.dx = Dom.xl / b.xn;
+  b.yn = (int)floor(Dom.yl / (2. * rmax + ilr * rmax));
+  if(b.yn == 0) { b.yn = 1; b.dy = Dom.yl; } else b.dy = Dom.yl / b.yn;
+  b.zn = (int)floor(Dom.zl / (2. * rmax + ilr * rmax));
+  if(b.zn == 0) { b.zn = 1; b.dz = Dom.zl; } else b.dz = Dom.zl / b.zn;
+  b.s1 = b.xn; b.s2 = b.s1 * b.yn; b.s3 = b.s2 * b.zn;
+  g_bins.s3 = b.s3;
+  g_bins.np = nparts;
+  int *ps[3];
+  for(int a = 0; a < 3; a++)
+    if(cudaMalloc((void **)&ps[a], sizeof(int) * (size_t)b.s3) != cudaSuccess)
+      bbb_set_status(BBB_ERR_CUDA, "cudaMalloc bins");
+  g_bins.cnt = ps[0]; g_bins.start = ps[1]; g_bins.fill = ps[2];
+  if(cudaMalloc((void **)&g_bins.list, sizeof(int) * (size_t)(nparts > 0 ? nparts : 1)) != cudaSuccess)
+    bbb_set_status(BBB_ERR_CUDA, "cudaMalloc bins");
+}
+
+void bbb_bins_free(void)
+{
+  if(g_bins.cnt) {
+    cudaFree(g_bins.cnt); cudaFree(g_bins.start); cudaFree(g_bins.fill);
+    cudaFree(g_bins.list);
+  }
+  memset(&g_bins, 0, sizeof(g_bins));
+}
+
+static coll_args make_coll_args(void)
+{
+  coll_args A;
+  A.mu = mu; A.rho_f = rho_f; A.nu = nu; A.dt = dt;
+  A.ilr = (int)interactionLengthRatio;
+  A.xs = Dom.xs; A.xe = Dom.xe; A.xl = Dom.xl;
+  A.ys = Dom.ys; A.ye = Dom.ye; A.yl = Dom.yl;
+  A.zs = Dom.zs; A.ze = Dom.ze; A.zl = Dom.zl;
+  A.bc = bc;
+  return A;
+}
+
+/* interaction forces, Newton-Euler half step, interaction forces again;
+ * the final call adds the position update */
+static void move_parts_seq(int final)
+{
+  bbb_dev_require();
+  if(!g_dev.ready || nparts <= 0 || g_dev.np != nparts) return;
+  int nb = (nparts + 127) / 128;
+  coll_args A = make_coll_args();
+  bbb_geom G = bbb_make_geom();
+  if(nparts > 1) {
+    bins_setup();
+    const bin_geom &bg = g_bins.bg;
+    BBB_CK(cudaMemsetAsync(g_bins.cnt, 0, sizeof(int) * (size_t)bg.s3, g_dev.stream));
+    BBB_CK(cudaMemsetAsync(g_bins.fill, 0, sizeof(int) * (size_t)bg.s3, g_dev.stream));
+    k_bin_count<<<nb, 128, 0, g_dev.stream>>>(g_dev.parts, nparts, bg, g_bins.cnt);
+    BBB_LAUNCHED();
+    k_bin_scan<<<1, 1024, 0, g_dev.stream>>>(g_bins.cnt, g_bins.start, bg.s3);
+    BBB_LAUNCHED();
+    k_bin_scatter<<<nb, 128, 0, g_dev.stream>>>(g_dev.parts, nparts, bg,
+      g_bins.start, g_bins.fill, g_bins.list);
+    BBB_LAUNCHED();
+    k_bin_sort<<<(bg.s3 + 255) / 256, 256, 0, g_dev.stream>>>(g_bins.start,
+      g_bins.cnt, g_bins.list, bg.s3);
+    BBB_LAUNCHED();
+  }
+  bin_geom bg = g_bins.bg;
+  for(int pass = 0; pass < 2; pass++) {
+    k_interact<<<nb, 128, 0, g_dev.stream>>>(g_dev.parts, nparts, bg,
+      g_bins.start, g_bins.cnt, g_bins.list, A);
+    BBB_LAUNCHED();
+    if(pass == 0) {
+      k_move<<<nb, 128, 0, g_dev.stream>>>(g_dev.parts, nparts, 0, dt, rho_f, g,
+        gradP, G);
+      BBB_LAUNCHED();
+    }
+  }
+  if(final) {
+    k_move<<<nb, 128, 0, g_dev.stream>>>(g_dev.parts, nparts, 1, dt, rho_f, g,
+      gradP, G);
+    BBB_LAUNCHED();
+  }
 }
 
 /* src/cuda_bluebottle.cu:4317-4433 */
 extern "C" void cuda_move_parts_sub(void)
 {
-  bbb_dev_require();
-  if(!g_dev.ready || nparts <= 0 || g_dev.np != nparts) return;
-  k_move_parts<<<(nparts + 127) / 128, 128, 0, g_dev.stream>>>(g_dev.parts,
-    nparts, 0, dt, rho_f, g, gradP, bbb_make_geom());
-  BBB_LAUNCHED();
+  move_parts_seq(0);
 }
 
 /* src/cuda_bluebottle.cu:4435-4554 */
 extern "C" void cuda_move_parts(void)
 {
-  bbb_dev_require();
-  if(!g_dev.ready || nparts <= 0 || g_dev.np != nparts) return;
-  k_move_parts<<<(nparts + 127) / 128, 128, 0, g_dev.stream>>>(g_dev.parts,
-    nparts, 1, dt, rho_f, g, gradP, bbb_make_geom());
-  BBB_LAUNCHED();
+  move_parts_seq(1);
   g_dev.lf_geo_valid = 0;   /* positions moved */
 }

@@ -153,8 +153,10 @@ typedef struct bbb_options {
   real inner_tol;          /* mixed form: relative tolerance of each FP32
                               inner solve                                  */
   int max_outer;           /* mixed form: defect-correction sweep cap      */
-  int learned_guess;       /* 1: conv-net initial guess for the Poisson
-                              solve (requires bbb_learned_load)            */
+  int learned_guess;       /* conv-net initial guess of the first Poisson
+                              solve of each step, a bit mask: 1 record
+                              training crops, 2 use the (gated) guess;
+                              applied by bbb_prepare via bbb_learn_enable */
   int record;              /* 1: append solver_expd.rec like the reference */
   int gravity_balance;     /* 1: set gradP.z so the box's net weight is 0  */
   int lamb_max_iter_override; /* >0: replaces lamb_max_iter               */
@@ -231,13 +233,18 @@ void bbb_divergence(real *max_abs, real *l2);
 long long bbb_kernel_launches(void);
 void bbb_reset_kernel_launches(void);
 
-/* Live timing of the pressure solver's BiCGSTAB iteration (its three fused
- * passes), by CUDA events on the solver stream, over the iterations the
- * device executed while enabled: total milliseconds, iteration count and
- * algorithmic bytes (17 vector words + 3 mask bytes per unknown). */
+/* Live timing of the pressure solver's BiCGSTAB iterations, by CUDA
+ * events on the solver stream around each of the two fused passes, over
+ * the passes the device executed while enabled.  bbb_profile_get: total
+ * milliseconds, iteration count and algorithmic bytes (15 vector words +
+ * 2 mask bytes per unknown and iteration).  bbb_profile_get_pass: the same
+ * for one pass (0: pass A, the p/v update and first stencil; 1: pass B,
+ * the s/t update and second stencil), with its launch count. */
 void bbb_profile_enable(int on);
 void bbb_profile_reset(void);
 void bbb_profile_get(double *ms, long long *iters, double *bytes);
+void bbb_profile_get_pass(int pass, double *ms, long long *launches,
+  double *bytes);
 
 /* Copy only the particle records (part_struct array) between the host
  * `parts` and the device: the per-step exchange of a caller that moves
@@ -250,6 +257,41 @@ void bbb_part_state_pull(void);
  * mark b and returns milliseconds between marks a and b (-1 on error) */
 void bbb_mark(int i);
 double bbb_mark_elapsed(int a, int b);
+
+/* Learned initial guess of the pressure-Poisson solve.  No counterpart in
+ * the reference, which starts each solve from the previous correction phi
+ * (src/cuda_bicgstab.cu:971-979).  A 4-layer 3x3x3 convolutional net (16
+ * channels, GELU, BF16 tensor-core convolutions with FP32 accumulation)
+ * predicts a correction to that extrapolation from (b, phi_prev, p0, solid
+ * mask); the first solve of each step starts from it when its FP64
+ * residual is below the extrapolation's (counted in bbb_stats.guess_used,
+ * with both initial residuals in guess_r0 / extrap_r0).
+ *   bbb_learn_enable(mode): bit 1 record crops of (features, converged
+ *     correction) at the first solve of each step; bit 2 use the guess.
+ *   bbb_learn_train(iters, lr): Adam steps on batches of 8 recorded crops;
+ *     returns the relative MSE of the last batch (-1 without crops).
+ *   bbb_learn_get/set_params: FP32 weights [layer][tap][cout][cin] then
+ *     biases [layer][cout], bbb_learn_param_count() floats.
+ *   bbb_learn_forward: the net on a caller's device box of features
+ *     (channels-last BF16, 16 channels) into FP32 out; ref = 1 runs the
+ *     FP32 CUDA-core convolution instead of the tensor cores.
+ *   bbb_learn_use_reference_conv(on): route every convolution (inference
+ *     and training) through the FP32 CUDA-core kernels. */
+int bbb_learn_enable(int mode);
+double bbb_learn_train(int iters, double lr);
+int bbb_learn_crops(void);
+int bbb_learn_param_count(void);
+int bbb_learn_get_params(float *host, int n);
+int bbb_learn_set_params(const float *host, int n);
+int bbb_learn_forward(int nx, int ny, int nz, int px, int py, int pz,
+  const void *feat_d, float *out_d, int ref);
+/* loss and gradient (no update) on a caller's device batch of nb crops of
+ * cx*cy*cz cells stacked along z (features as above, FP32 targets), MSE
+ * over cells at least `margin` from crop faces; grad_host receives
+ * bbb_learn_param_count() floats.  Returns the MSE, -1 on failure. */
+double bbb_learn_grad(int cx, int cy, int cz, int nb, int margin,
+  const void *feat_d, const float *tgt_d, float *grad_host);
+void bbb_learn_use_reference_conv(int on);
 
 /* Allocation-free pressure-Poisson solve.  No counterpart in the
  * reference: it is the FP64 solve of cuda_PP_bicgstab for callers that

@@ -854,18 +854,147 @@ void orc_store_coeffs(orc_state *st)
   for(int a = 0; a < 6; a++) memcpy(st->coef[12 + a], st->coef[a], n);
 }
 
-/* ------------------------------------------------ Newton-Euler
- * src/bluebottle_kernel.cu:2247-2398; collision_init :2400 and
- * spring_parts :3592.  Lubrication/contact forces (collision_parts :2500,
- * collision_walls :2875) are not part of this restatement; the interaction
- * force stays zero. */
-static void collisions_and_springs(orc_state *st)
+/* ------------------------------------------------ interaction forces
+ * src/cuda_bluebottle.cu:4317-4554 (sequence), src/bluebottle_kernel.cu:
+ * collision_init :2400, bin_fill :2422, bin_start :2454, collision_parts
+ * :2500, collision_walls :2875, spring_parts :3592; the bin grid of
+ * binDom_init src/particle.c:598.
+ *
+ * Kept as the reference computes them:
+ * - the kernels take interactionLengthRatio as an int (truncated), so the
+ *   lubrication range hN = (int)ratio * a;
+ * - the contact-list searches test iSt[q] before q < MAX_NEIGHBORS, so they
+ *   read (and, in the lubrication branch, write) slot 12: the 4 bytes after
+ *   iSt (the low word of e_dry) and, for St[12], the 8 bytes after St
+ *   (iSt[0], iSt[1]); both are emulated byte for byte below;
+ * - every wall's contact branch takes the tangential wall velocity from the
+ *   south wall's Dirichlet values (bc.uSD, bc.vSD, bc.wSD);
+ * - the east-wall contact torque uses the function-scope Ftx, which only an
+ *   earlier lubrication branch of the same call assigns (0 there); it is 0
+ *   here (the reference reads an unassigned local otherwise);
+ * - the x walls' contact slip takes omega_x in place of omega_y.
+ * Where the reference's new-contact search would run past slot 12 (all 12
+ * slots taken) it stops at 12. */
+#define ORC_MAXN BBB_MAX_NEIGHBORS
+
+static int ist_get(const part_struct *q, int k)
+{
+  int v;
+  memcpy(&v, (const char *)q->iSt + sizeof(int) * (size_t)k, sizeof(int));
+  return v;
+}
+static void ist_set(part_struct *q, int k, int v)
+{
+  memcpy((char *)q->iSt + sizeof(int) * (size_t)k, &v, sizeof(int));
+}
+static real st_get(const part_struct *q, int k)
+{
+  real v;
+  memcpy(&v, (const char *)q->St + sizeof(real) * (size_t)k, sizeof(real));
+  return v;
+}
+static void st_set(part_struct *q, int k, real v)
+{
+  memcpy((char *)q->St + sizeof(real) * (size_t)k, &v, sizeof(real));
+}
+
+/* lubrication range entered: drop `key` from the contact list */
+static void contact_forget(part_struct *q, int key)
+{
+  int k = 0;
+  while(ist_get(q, k) != key && k < ORC_MAXN) k++;
+  if(ist_get(q, k) == key) { ist_set(q, k, -1); st_set(q, k, 0.); }
+}
+
+/* contact: slot of `key`, adding it with Stokes number `St` when new */
+static int contact_slot(part_struct *q, int key, real St)
+{
+  int k = 0;
+  while(ist_get(q, k) != key && k < ORC_MAXN) k++;
+  if(k == ORC_MAXN) {
+    k = 0;
+    while(ist_get(q, k) != -1 && k < ORC_MAXN) k++;
+    ist_set(q, k, key);
+    st_set(q, k, St);
+  }
+  return k;
+}
+
+typedef struct orc_bins {
+  int xn, yn, zn, s1, s2, s3;
+  real xs, ys, zs, dx, dy, dz;
+  int *start, *end, *ind, *bin;
+} orc_bins;
+
+static void bins_geometry(const orc_state *st, orc_bins *B)
+{
+  const dom_struct *D = &st->dom;
+  real rmax = 0;
+  for(int i = 0; i < st->nparts; i++)
+    rmax = rmax + (st->parts[i].r > rmax) * (st->parts[i].r - rmax);
+  real ilr = st->P.interactionLengthRatio;
+  B->xs = D->xs; B->ys = D->ys; B->zs = D->zs;
+  B->xn = (int)floor(D->xl / (2. * rmax + ilr * rmax));
+  if(B->xn == 0) { B->xn = 1; B->dx = D->xl; } else B->dx = D->xl / B->xn;
+  B->yn = (int)floor(D->yl / (2. * rmax + ilr * rmax));
+  if(B->yn == 0) { B->yn = 1; B->dy = D->yl; } else B->dy = D->yl / B->yn;
+  B->zn = (int)floor(D->zl / (2. * rmax + ilr * rmax));
+  if(B->zn == 0) { B->zn = 1; B->dz = D->zl; } else B->dz = D->zl / B->zn;
+  B->s1 = B->xn; B->s2 = B->s1 * B->yn; B->s3 = B->s2 * B->zn;
+}
+
+/* bin of every particle, particles ordered by (bin, index) */
+static void bins_fill(orc_state *st, orc_bins *B)
+{
+  int n = st->nparts;
+  B->start = (int *)malloc(sizeof(int) * (size_t)B->s3);
+  B->end = (int *)malloc(sizeof(int) * (size_t)B->s3);
+  B->ind = (int *)malloc(sizeof(int) * (size_t)n);
+  B->bin = (int *)malloc(sizeof(int) * (size_t)n);
+  for(int c = 0; c < B->s3; c++) { B->start[c] = -1; B->end[c] = -1; }
+  for(int pp = 0; pp < n; pp++) {
+    part_struct *q = &st->parts[pp];
+    int ib = (int)floor((q->x - B->xs) / B->dx);
+    int jb = (int)floor((q->y - B->ys) / B->dy);
+    int kb = (int)floor((q->z - B->zs) / B->dz);
+    int c = ib + jb * B->s1 + kb * B->s2;
+    q->bin = c;
+    B->ind[pp] = pp;
+    B->bin[pp] = c;
+  }
+  /* stable sort by bin (insertion: particle counts are small) */
+  for(int a = 1; a < n; a++) {
+    int kb = B->bin[a], ki = B->ind[a], b = a - 1;
+    while(b >= 0 && B->bin[b] > kb) {
+      B->bin[b + 1] = B->bin[b]; B->ind[b + 1] = B->ind[b]; b--;
+    }
+    B->bin[b + 1] = kb; B->ind[b + 1] = ki;
+  }
+  for(int a = 0; a < n; a++) {
+    if(a == 0 || B->bin[a] != B->bin[a - 1]) {
+      B->start[B->bin[a]] = a;
+      if(a > 0) B->end[B->bin[a - 1]] = a;
+    }
+    if(a == n - 1) B->end[B->bin[a]] = a + 1;
+  }
+}
+
+static void bins_free(orc_bins *B)
+{
+  free(B->start); free(B->end); free(B->ind); free(B->bin);
+}
+
+static void interaction_init(orc_state *st)
 {
   for(int i = 0; i < st->nparts; i++) {
     part_struct *q = &st->parts[i];
     q->iFx = 0.; q->iFy = 0.; q->iFz = 0.;
     q->iLx = 0.; q->iLy = 0.; q->iLz = 0.;
   }
+}
+
+static void springs(orc_state *st)
+{
   for(int i = 0; i < st->nparts; i++) {
     part_struct *q = &st->parts[i];
     if(!(q->spring_k > 0.)) continue;
@@ -876,6 +1005,310 @@ static void collisions_and_springs(orc_state *st)
     q->kFx = -q->spring_k * (q->x - q->spring_x - lx);
     q->kFy = -q->spring_k * (q->y - q->spring_y - ly);
     q->kFz = -q->spring_k * (q->z - q->spring_z - lz);
+  }
+}
+
+/* nearest periodic image of the separation along one axis */
+static real min_image(real a, real b, real L, int periodic)
+{
+  real r = a - b, r1 = a - (b + L), r2 = a - (b - L);
+  if(r1 * r1 < r * r) r = r1;
+  if(r2 * r2 < r * r) r = r2;
+  return periodic * r + (!periodic) * (a - b);
+}
+
+/* force and torque on particle i from particle j (collision_parts body) */
+static void pair_force(orc_state *st, int i, int j)
+{
+  const orc_params *P = &st->P;
+  const dom_struct *D = &st->dom;
+  part_struct *pi = &st->parts[i];
+  const part_struct *pj = &st->parts[j];
+  real eps = 0.01, mu = P->mu, rhof = P->rho_f, nu = P->nu, dt = P->dt;
+  int ilr = (int)P->interactionLengthRatio;
+  real ai = pi->r, aj = pj->r, B = aj / ai, hN = ilr * pi->r;
+  real rx = min_image(pi->x, pj->x, D->xl, P->bc.uW == BBB_PERIODIC);
+  real ry = min_image(pi->y, pj->y, D->yl, P->bc.vS == BBB_PERIODIC);
+  real rz = min_image(pi->z, pj->z, D->zl, P->bc.wB == BBB_PERIODIC);
+  real ux = 0.5 * ((pi->u - pj->u) + (pi->u0 - pj->u0));
+  real uy = 0.5 * ((pi->v - pj->v) + (pi->v0 - pj->v0));
+  real uz = 0.5 * ((pi->w - pj->w) + (pi->w0 - pj->w0));
+  real r = sqrt(rx * rx + ry * ry + rz * rz);
+  real omx = 0.5 * ((pi->ox + pj->ox) + (pi->ox0 + pj->ox0));
+  real omy = 0.5 * ((pi->oy + pj->oy) + (pi->oy0 + pj->oy0));
+  real omz = 0.5 * ((pi->oz + pj->oz) + (pi->oz0 + pj->oz0));
+  real om = sqrt(omx * omx + omy * omy + omz * omz);
+  real h = r - ai - aj;
+  real nx = rx / r, ny = ry / r, nz = rz / r;
+  real udotn = ux * nx + uy * ny + uz * nz;
+  real unx = udotn * nx, uny = udotn * ny, unz = udotn * nz;
+  real utx = ux - unx, uty = uy - uny, utz = uz - unz;
+  real ut = sqrt(utx * utx + uty * uty + utz * utz);
+  real tx, ty, tz, bx, by, bz;
+  if(ut > 0) {
+    tx = utx / ut; ty = uty / ut; tz = utz / ut;
+    bx = ny * tz - nz * ty; by = -nx * tz + nz * tx; bz = nx * ty - ny * tx;
+    real b = sqrt(bx * bx + by * by + bz * bz);
+    bx = bx / b; by = by / b; bz = bz / b;
+  } else if(om > 0) {
+    bx = omx / om; by = omy / om; bz = omz / om;
+    tx = by * nz - bz * ny; ty = -bx * nz + bz * nx; tz = bx * ny - by * nx;
+    real t = sqrt(tx * tx + ty * ty + tz * tz);
+    tx = tx / t; ty = ty / t; tz = tz / t;
+  } else {
+    tx = 1.; ty = 0.; tz = 0.;
+    bx = ny * tz - nz * ty; by = -nx * tz + nz * tx; bz = nx * ty - ny * tx;
+    real b = sqrt(bx * bx + by * by + bz * bz);
+    bx = bx / b; by = by / b; bz = bz / b;
+  }
+  (void)bx; (void)by; (void)bz;
+  real opB = 1 + B;
+  real ocnx = omy * nz - omz * ny, ocny = -omx * nz + omz * nx, ocnz = omx * ny - omy * nx;
+  real ucnx = uty * nz - utz * ny, ucny = -utx * nz + utz * nx, ucnz = utx * ny - uty * nx;
+  real Fnx, Fny, Fnz, Ftx, Fty, Ftz, Lox, Loy, Loz;
+  if(h < hN && h > 0) {
+    contact_forget(pi, j);
+    if(h < eps * pi->r) h = eps * pi->r;
+    real ah = ai / h - ai / hN, lnah = log(hN / h);
+    Fnx = -1. * B * B / (opB * opB) * ah - B * (1. + 7. * B + B * B) / (5. * opB * opB * opB) * lnah;
+    Fny = Fnx; Fnz = Fnx;
+    Fnx *= 6. * PI * mu * ai * unx;
+    Fny *= 6. * PI * mu * ai * uny;
+    Fnz *= 6. * PI * mu * ai * unz;
+    Ftx = -6. * PI * mu * ai * utx * 4. * B * (2. + B + 2. * B * B) / (15. * opB * opB * opB) * lnah;
+    Fty = -6. * PI * mu * ai * uty * 4. * B * (2. + B + 2. * B * B) / (15. * opB * opB * opB) * lnah;
+    Ftz = -6. * PI * mu * ai * utz * 4. * B * (2. + B + 2. * B * B) / (15. * opB * opB * opB) * lnah;
+    Ftx += 8. * PI * mu * ai * ai * ocnx * B * (4. + B) / (10. * opB * opB) * lnah;
+    Fty += 8. * PI * mu * ai * ai * ocny * B * (4. + B) / (10. * opB * opB) * lnah;
+    Ftz += 8. * PI * mu * ai * ai * ocnz * B * (4. + B) / (10. * opB * opB) * lnah;
+    Lox = -8. * PI * mu * ai * ai * ucnx * B * (4. + B) / (10. * opB * opB) * lnah;
+    Loy = -8. * PI * mu * ai * ai * ucny * B * (4. + B) / (10. * opB * opB) * lnah;
+    Loz = -8. * PI * mu * ai * ai * ucnz * B * (4. + B) / (10. * opB * opB) * lnah;
+    Lox += -8. * PI * mu * ai * ai * ai * omx * 2. * B / (5. * opB) * lnah;
+    Loy += -8. * PI * mu * ai * ai * ai * omy * 2. * B / (5. * opB) * lnah;
+    Loz += -8. * PI * mu * ai * ai * ai * omz * 2. * B / (5. * opB) * lnah;
+  } else {
+    Fnx = 0; Fny = 0; Fnz = 0; Ftx = 0; Fty = 0; Ftz = 0; Lox = 0; Loy = 0; Loz = 0;
+  }
+  if(h < 0) {
+    int q = contact_slot(pi, j, 1. / 9. * pi->rho / rhof * 2. * pi->r * fabs(udotn) / nu);
+    real Vx = -utx + 0.5 * (ai + aj + h) * ocnx;
+    real Vy = -uty + 0.5 * (ai + aj + h) * ocny;
+    real Vz = -utz + 0.5 * (ai + aj + h) * ocnz;
+    real Hi = 0.5 * pi->E / (1. + pi->sigma);
+    real kt = 8. / ((1. - pi->sigma * pi->sigma) / Hi + (1. - pi->sigma * pi->sigma) / Hi)
+      / sqrt(1. / ai) * sqrt(-h);
+    real Vdotn = Vx * nx + Vy * ny + Vz * nz;
+    real sx = (Vx - Vdotn * nx) * dt, sy = (Vy - Vdotn * ny) * dt, sz = (Vz - Vdotn * nz) * dt;
+    real k = 4. / 3. / ((1. - pi->sigma * pi->sigma) / pi->E
+      + (1. - pj->sigma * pj->sigma) / pj->E) / sqrt(1. / ai + 1. / aj);
+    real xcx0 = 1.e-4;
+    real e = pi->e_dry + (1. + pi->e_dry) / st_get(pi, q) * log(xcx0);
+    if(e < 0) e = 0;
+    real alpha = -2.263 * pow(e, 0.3948) + 2.22;
+    real eta = alpha * sqrt(4. / 3. * PI * ai * ai * ai * pi->rho * k * sqrt(-h));
+    Fnx = (sqrt(-h * h * h) * k - eta * udotn) * nx;
+    Fny = (sqrt(-h * h * h) * k - eta * udotn) * ny;
+    Fnz = (sqrt(-h * h * h) * k - eta * udotn) * nz;
+    real cf = 0.5 * (pi->coeff_fric + pj->coeff_fric);
+    Ftx = -kt * sx; Fty = -kt * sy; Ftz = -kt * sz;
+    real Ftdotn = Ftx * nx + Fty * ny + Ftz * nz;
+    Ftx = Ftx - Ftdotn * nx; Fty = Fty - Ftdotn * ny; Ftz = Ftz - Ftdotn * nz;
+    real Ft = sqrt(Ftx * Ftx + Fty * Fty + Ftz * Ftz);
+    real Fn = sqrt(Fnx * Fnx + Fny * Fny + Fnz * Fnz);
+    if(Ft > cf * Fn) {
+      Ftx = cf * Fn * Ftx / Ft; Fty = cf * Fn * Fty / Ft; Ftz = cf * Fn * Ftz / Ft;
+    }
+    Lox = -(ai + 0.5 * h) * ((Fny + Fty) * nz - (Fnz + Ftz) * ny);
+    Loy = (ai + 0.5 * h) * ((Fnx + Ftx) * nz - (Fnz + Ftz) * nx);
+    Loz = -(ai + 0.5 * h) * ((Fnx + Ftx) * ny - (Fny + Fty) * nx);
+  }
+  pi->iFx += Fnx + Ftx;
+  pi->iFy += Fny + Fty;
+  pi->iFz += Fnz + Ftz;
+  pi->iLx += Lox;
+  pi->iLy += Loy;
+  pi->iLz += Loz;
+}
+
+/* neighbour bins in the reference's order (z, y, x; -1..1), wrapping only
+ * across periodic faces with more than two bins */
+static void collide_parts(orc_state *st, const orc_bins *B)
+{
+  const BC *bc = &st->P.bc;
+  int fW = 0, fE = B->xn - 1, fS = 0, fN = B->yn - 1, fB = 0, fT = B->zn - 1;
+  int xnb = B->xn > 2, ynb = B->yn > 2, znb = B->zn > 2;
+  for(int index = 0; index < st->nparts; index++) {
+    int i = B->ind[index], bin = B->bin[index];
+    int kbin = bin / B->s2, jbin = (bin - kbin * B->s2) / B->s1;
+    int ibin = bin - kbin * B->s2 - jbin * B->s1;
+    for(int n = -1; n <= 1; n++) {
+      int ks;
+      if((n == -1 && kbin == fB && bc->uB != BBB_PERIODIC) ||
+         (n == 1 && kbin == fT && bc->uT != BBB_PERIODIC) ||
+         (n == -1 && kbin == fB && bc->uB == BBB_PERIODIC && znb == 0) ||
+         (n == 1 && kbin == fT && bc->uT == BBB_PERIODIC && znb == 0)) continue;
+      else if(n == -1 && kbin == fB) ks = fT * B->s2;
+      else if(n == 1 && kbin == fT) ks = fB * B->s2;
+      else ks = (kbin + n) * B->s2;
+      for(int m = -1; m <= 1; m++) {
+        int js;
+        if((m == -1 && jbin == fS && bc->uS != BBB_PERIODIC) ||
+           (m == 1 && jbin == fN && bc->uN != BBB_PERIODIC) ||
+           (m == -1 && jbin == fS && bc->uS == BBB_PERIODIC && ynb == 0) ||
+           (m == 1 && jbin == fN && bc->uN == BBB_PERIODIC && ynb == 0)) continue;
+        else if(m == -1 && jbin == fS) js = fN * B->s1;
+        else if(m == 1 && jbin == fN) js = fS * B->s1;
+        else js = (jbin + m) * B->s1;
+        for(int l = -1; l <= 1; l++) {
+          int is;
+          if((l == -1 && ibin == fW && bc->uW != BBB_PERIODIC) ||
+             (l == 1 && ibin == fE && bc->uE != BBB_PERIODIC) ||
+             (l == -1 && ibin == fW && bc->uW == BBB_PERIODIC && xnb == 0) ||
+             (l == 1 && ibin == fE && bc->uE == BBB_PERIODIC && xnb == 0)) continue;
+          else if(l == -1 && ibin == fW) is = fE;
+          else if(l == 1 && ibin == fE) is = fW;
+          else is = ibin + l;
+          int adj = is + js + ks;
+          if(B->start[adj] == -1) continue;
+          for(int t = B->start[adj]; t < B->end[adj]; t++) {
+            int j = B->ind[t];
+            if(j != i) pair_force(st, i, j);
+          }
+        }
+      }
+    }
+  }
+}
+
+/* one wall (collision_walls).  ax: normal axis 0/1/2; hi: 0 for the W/S/B
+ * wall, 1 for E/N/T; key -10..-15. */
+static void wall_force(orc_state *st, part_struct *p, int ax, int hi, real *Ftx_scope)
+{
+  const orc_params *P = &st->P;
+  const dom_struct *D = &st->dom;
+  const BC *bc = &P->bc;
+  real eps = 0.01, mu = P->mu, rhof = P->rho_f, nu = P->nu, dt = P->dt;
+  int ilr = (int)P->interactionLengthRatio;
+  real ai = p->r, hN = ilr * p->r;
+  real pos[3] = {p->x, p->y, p->z}, vel[3] = {p->u, p->v, p->w};
+  real vel0[3] = {p->u0, p->v0, p->w0};
+  real om[3] = {p->ox, p->oy, p->oz}, om0[3] = {p->ox0, p->oy0, p->oz0};
+  real wallpos, ds;
+  int press;
+  /* Dirichlet wall velocities of this wall, per component */
+  real wv[3];
+  int key = -10 - (2 * ax + hi);
+  if(ax == 0) {
+    ds = hi ? bc->dsE : bc->dsW;
+    wallpos = hi ? D->xe - ds : D->xs + ds;
+    press = hi ? bc->pE : bc->pW;
+    wv[0] = hi ? bc->uED : bc->uWD; wv[1] = hi ? bc->vED : bc->vWD; wv[2] = hi ? bc->wED : bc->wWD;
+  } else if(ax == 1) {
+    ds = hi ? bc->dsN : bc->dsS;
+    wallpos = hi ? D->ye - ds : D->ys + ds;
+    press = hi ? bc->pN : bc->pS;
+    wv[0] = hi ? bc->uND : bc->uSD; wv[1] = hi ? bc->vND : bc->vSD; wv[2] = hi ? bc->wND : bc->wSD;
+  } else {
+    ds = hi ? bc->dsT : bc->dsB;
+    wallpos = hi ? D->ze - ds : D->zs + ds;
+    press = hi ? bc->pT : bc->pB;
+    wv[0] = hi ? bc->uTD : bc->uBD; wv[1] = hi ? bc->vTD : bc->vBD; wv[2] = hi ? bc->wTD : bc->wBD;
+  }
+  real sd[3] = {bc->uSD, bc->vSD, bc->wSD};
+  real h = fabs(pos[ax] - wallpos) - ai;
+  real isTrue = (press == BBB_NEUMANN);
+  /* tangential axes in the reference's order and the sign pattern of the
+   * rotation terms: lo walls (W, S, B) and hi walls mirror each other */
+  int t1 = ax == 0 ? 1 : 0, t2 = ax == 2 ? 1 : 2;
+  real sg = hi ? -1. : 1.;
+  if(h < hN && h > 0) {
+    contact_forget(p, key);
+    if(h < eps * p->r) h = eps * p->r;
+    real ah = ai / h - ai / hN, lnah = log(hN / h);
+    real Un = vel[ax] - wv[ax];
+    real Ut[3] = {vel[0] - wv[0], vel[1] - wv[1], vel[2] - wv[2]};
+    Ut[ax] = 0.;
+    real F[3] = {0., 0., 0.}, Ft[3] = {0., 0., 0.}, L[3] = {0., 0., 0.};
+    F[ax] = -6. * PI * mu * ai * Un * ah;
+    Ft[t1] = -6. * PI * mu * ai * Ut[t1] * 8. / 15. * lnah;
+    Ft[t2] = -6. * PI * mu * ai * Ut[t2] * 8. / 15. * lnah;
+    /* rotation coupling: (t1, t2) = (y, z) for x walls, (x, z) for y walls,
+     * (x, y) for z walls; the y walls carry the opposite orientation */
+    real so = (ax == 1) ? -sg : sg;
+    Ft[t1] += so * 8. * PI * mu * ai * ai * om[t2] * 1. / 10. * lnah;
+    Ft[t2] += -so * 8. * PI * mu * ai * ai * om[t1] * 1. / 10. * lnah;
+    L[t1] = -so * 8. * PI * mu * ai * ai * Ut[t2] * 1. / 10. * lnah;
+    L[t2] = so * 8. * PI * mu * ai * ai * Ut[t1] * 1. / 10. * lnah;
+    L[t1] += -8. * PI * mu * ai * ai * ai * om[t1] * 2. / 5. * lnah;
+    L[t2] += -8. * PI * mu * ai * ai * ai * om[t2] * 2. / 5. * lnah;
+    *Ftx_scope = Ft[0];
+    p->iFx += isTrue * (F[0] + Ft[0]);
+    p->iFy += isTrue * (F[1] + Ft[1]);
+    p->iFz += isTrue * (F[2] + Ft[2]);
+    p->iLx += isTrue * L[0];
+    p->iLy += isTrue * L[1];
+    p->iLz += isTrue * L[2];
+  }
+  if(h < 0) {
+    real Un = sg * (vel[ax] - wv[ax]);
+    real Ut1 = 0.5 * (vel[t1] + vel0[t1]) - sd[t1];
+    real Ut2 = 0.5 * (vel[t2] + vel0[t2]) - sd[t2];
+    int q = contact_slot(p, key, 1. / 9. * p->rho / rhof * 2. * p->r * fabs(Un) / nu);
+    real o[3] = {0.5 * (om[0] + om0[0]), 0.5 * (om[1] + om0[1]), 0.5 * (om[2] + om0[2])};
+    /* slip velocity at the contact point; the x walls take omega_x where
+     * omega_y belongs (src/bluebottle_kernel.cu:2977, :3091) */
+    real so = (ax == 1) ? -1. : 1.;
+    real o2 = ax == 0 ? o[0] : o[t1];
+    real V1 = sg * (Ut1 - so * (ai + 0.5 * h) * o[t2]);
+    real V2 = sg * (Ut2 + so * (ai + 0.5 * h) * o2);
+    real Hi = 0.5 * p->E / (1. + p->sigma);
+    real kt = 8. / ((1. - p->sigma * p->sigma) / Hi + (1. - p->sigma * p->sigma) / Hi)
+      / sqrt(1. / ai) * sqrt(-h);
+    real s1 = V1 * dt, s2 = V2 * dt;
+    real k = 4. / 3. / ((1. - p->sigma * p->sigma) / p->E + (1. - p->sigma * p->sigma) / p->E)
+      / sqrt(1. / ai);
+    real xcx0 = 1.e-4;
+    real e = p->e_dry + (1. + p->e_dry) / st_get(p, q) * log(xcx0);
+    if(e < 0) e = 0;
+    real alpha = -2.263 * pow(e, 0.3948) + 2.22;
+    real eta = alpha * sqrt(4. / 3. * PI * ai * ai * ai * p->rho * k * sqrt(-h));
+    real cf = p->coeff_fric;
+    real F1 = -kt * s1, F2 = -kt * s2;
+    real Ft = sqrt(F1 * F1 + F2 * F2);
+    real Fn = sqrt(-h * h * h) * k - eta * Un;
+    if(Ft > fabs(cf * Fn)) {
+      F1 = cf * Fn * F1 / Ft;
+      F2 = cf * Fn * F2 / Ft;
+    }
+    real arm = ai + 0.5 * h;
+    if(ax == 0) {
+      p->iFx += sg * isTrue * Fn;
+      p->iFy += isTrue * F1;
+      p->iFz += isTrue * F2;
+      if(!hi) { p->iLy += isTrue * arm * F2; p->iLz -= isTrue * arm * F1; }
+      else { p->iLy -= isTrue * arm * F2; p->iLz += isTrue * arm * (*Ftx_scope); }
+    } else if(ax == 1) {
+      p->iFx += isTrue * F1;
+      p->iFy += sg * isTrue * Fn;
+      p->iFz += isTrue * F2;
+      if(!hi) { p->iLx -= isTrue * arm * F2; p->iLz += isTrue * arm * F1; }
+      else { p->iLx += isTrue * arm * F2; p->iLz -= isTrue * arm * F1; }
+    } else {
+      p->iFx += isTrue * F1;
+      p->iFy += isTrue * F2;
+      p->iFz += sg * isTrue * Fn;
+      if(!hi) { p->iLx += isTrue * arm * F2; p->iLy -= isTrue * arm * F1; }
+      else { p->iLx -= isTrue * arm * F2; p->iLy += isTrue * arm * F1; }
+    }
+  }
+}
+
+static void collide_walls(orc_state *st)
+{
+  for(int i = 0; i < st->nparts; i++) {
+    real Ftx_scope = 0.;
+    for(int w = 0; w < 6; w++) wall_force(st, &st->parts[i], w / 2, w % 2, &Ftx_scope);
   }
 }
 
@@ -958,20 +1391,37 @@ static void move_parts(orc_state *st, int final)
 }
 
 /* src/cuda_bluebottle.cu:4317-4433 */
+/* src/cuda_bluebottle.cu:4317-4433: interaction forces, the first
+ * Newton-Euler half step, interaction forces again; the final call adds
+ * the position update (move_parts_b) */
+static void interactions(orc_state *st, int final)
+{
+  int n = st->nparts;
+  if(n <= 0) return;
+  orc_bins B;
+  memset(&B, 0, sizeof(B));
+  if(n > 1) {
+    bins_geometry(st, &B);
+    bins_fill(st, &B);
+  }
+  for(int pass = 0; pass < 2; pass++) {
+    interaction_init(st);
+    if(n > 1) collide_parts(st, &B);
+    springs(st);
+    collide_walls(st);
+    if(pass == 0) move_parts(st, 0);
+  }
+  if(n > 1) bins_free(&B);
+  if(final) move_parts(st, 1);
+}
+
 void orc_move_parts_sub(orc_state *st)
 {
-  if(st->nparts <= 0) return;
-  collisions_and_springs(st);
-  move_parts(st, 0);
-  collisions_and_springs(st);
+  interactions(st, 0);
 }
 
 /* src/cuda_bluebottle.cu:4435-4554 */
 void orc_move_parts(orc_state *st)
 {
-  if(st->nparts <= 0) return;
-  collisions_and_springs(st);
-  move_parts(st, 0);
-  collisions_and_springs(st);
-  move_parts(st, 1);
+  interactions(st, 1);
 }

@@ -1,0 +1,131 @@
+"""Interaction forces (src/bluebottle_kernel.cu collision_parts :2500,
+collision_walls :2875, spring_parts :3592): the oracle against the contact
+laws on the CPU, and the GPU against the oracle.
+
+Scene: x, y periodic, no-slip z walls with Neumann pressure (so wall forces
+apply), (l/a) = 1 so lubrication acts within one radius; two spheres
+overlapping each other, one overlapping the bottom wall, one half a radius
+below the top wall."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from bluebottle_b200 import Sim, configs
+from oracle.orc import Oracle
+
+PART_FIELDS = ("x", "y", "z", "u", "v", "w", "ox", "oy", "oz", "iFx", "iFy",
+               "iFz", "iLx", "iLy", "iLz", "udot", "wdot", "oxdot", "ozdot")
+
+
+def _scene(tmp_path, dt=None, vel=True):
+    d = str(tmp_path)
+    configs.write_flow_config(os.path.join(d, "flow.config"), n=(32, 32, 32),
+                              lo=(0., 0., 0.), hi=(8., 8., 8.),
+                              periodic=(True, True, False), nu=0.1,
+                              lamb_max_iter=1, pp_residual=1e-10)
+    parts = [dict(r=1.0, x=3.0, y=4.0, z=4.0), dict(r=1.0, x=4.95, y=4.1, z=4.0),
+             dict(r=1.0, x=3.0, y=1.5, z=0.98), dict(r=1.0, x=6.5, y=6.6, z=6.5)]
+    configs.write_part_config(os.path.join(d, "part.config"), parts, loa=1.0)
+    opts = {"fixed_dt": dt} if dt else {}
+    sim = Sim(input_dir=d, options=opts)
+    if dt:
+        sim.set_scalar("dt", dt)
+    if vel:
+        P = sim.parts()
+        P[0].u = P[0].u0 = 0.1
+        P[1].u = P[1].u0 = -0.1
+        P[3].w = P[3].w0 = 0.05
+        P[0].oz = P[0].oz0 = 0.2
+        P[2].ox = P[2].ox0 = 0.3
+    return sim
+
+
+def test_contact_laws_on_the_oracle(tmp_path):
+    """With a vanishing time step both interaction passes see the initial
+    kinematics: at rest the sphere-sphere force is the Hertz law
+    sqrt(-h^3) k along the line of centres, k = 4/3 / sum((1-s^2)/E) /
+    sqrt(1/a_i + 1/a_j); the wall contact pushes the sphere off the wall
+    with k_wall = 4/3 / (2 (1-s^2)/E) / sqrt(1/a); lubrication opposes the
+    approach to the top wall with -6 pi mu a U_n (a/h - a/hN)."""
+    sim = _scene(tmp_path, dt=1e-12, vel=False)
+    P = sim.parts()
+    P[3].w = P[3].w0 = 0.05
+    o = Oracle.from_sim(sim, prepare=False)
+    sim.close()
+    o.P.dt = 1e-12
+    o.lib.orc_move_parts_sub(o.st)
+    q = o.field("parts")
+    E, s = 1.e6, 0.5
+    r = math.hypot(1.95, 0.1)
+    h = r - 2.0
+    k = 4. / 3. / (2 * (1 - s * s) / E) / math.sqrt(2.0)
+    F = math.sqrt(-h ** 3) * k
+    nx, ny = -1.95 / r, -0.1 / r
+    assert math.isclose(q[0].iFx, F * nx, rel_tol=1e-6)
+    assert math.isclose(q[0].iFy, F * ny, rel_tol=1e-6)
+    assert math.isclose(q[1].iFx, -F * nx, rel_tol=1e-6)
+    assert list(q[0].iSt)[:2] == [1, -1] and list(q[1].iSt)[:2] == [0, -1]
+    hw = 0.98 - 1.0
+    kw = 4. / 3. / (2 * (1 - s * s) / E) / math.sqrt(1.0)
+    assert math.isclose(q[2].iFz, math.sqrt(-hw ** 3) * kw, rel_tol=1e-6)
+    assert q[2].iSt[0] == -14                      # bottom-wall contact
+    mu = o.P.mu
+    hl = 8.0 - 6.5 - 1.0
+    lub = -6 * math.pi * mu * 1.0 * 0.05 * (1.0 / hl - 1.0 / 1.0)
+    assert math.isclose(q[3].iFz, lub, rel_tol=1e-6)
+    o.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("call", ["sub", "final"])
+def test_gpu_interactions_match_oracle(gpu, tmp_path, call):
+    sim = _scene(tmp_path, dt=0.01)
+    orc = Oracle.from_sim(sim, prepare=False)
+    try:
+        sim.prepare()
+        # prepare() ran the set-up BCs only; the particle records are as set
+        lib = sim.lib
+        lib.cuda_part_push()
+        for _ in range(3):
+            if call == "sub":
+                lib.cuda_move_parts_sub()
+                orc.lib.orc_move_parts_sub(orc.st)
+            else:
+                lib.cuda_move_parts()
+                orc.lib.orc_move_parts(orc.st)
+        lib.cuda_part_pull()
+        g, c = sim.parts(), orc.field("parts")
+        for q in range(4):
+            for f in PART_FIELDS:
+                a, b = getattr(g[q], f), getattr(c[q], f)
+                assert abs(a - b) <= 1e-11 * max(1.0, abs(b)), (q, f, a, b)
+            assert list(g[q].iSt) == list(c[q].iSt), q
+            assert np.allclose(list(g[q].St), list(c[q].St), rtol=1e-12, atol=0), q
+            assert g[q].bin == c[q].bin
+    finally:
+        sim.close()
+        orc.close()
+
+
+@pytest.mark.gpu
+def test_gpu_steps_with_contacts_match_oracle(gpu, tmp_path):
+    """Whole time steps of the contact scene (flow, Lamb coupling, contacts)."""
+    sim = _scene(tmp_path, dt=0.002)
+    orc = Oracle.from_sim(sim)
+    try:
+        sim.prepare()
+        for _ in range(3):
+            sim.step()
+            orc.step()
+        sim.pull()
+        g, c = sim.parts(), orc.field("parts")
+        for q in range(4):
+            for f in ("x", "y", "z", "u", "v", "w", "iFx", "iFz", "Fx", "Fz"):
+                a, b = getattr(g[q], f), getattr(c[q], f)
+                assert abs(a - b) <= 1e-7 * max(1.0, abs(b)), (q, f, a, b)
+            assert list(g[q].iSt) == list(c[q].iSt)
+    finally:
+        sim.close()
+        orc.close()
