@@ -150,7 +150,10 @@ def load():
         getattr(lib, name).restype = R
     for name in ("bbb_read_input", "bbb_domain_init", "bbb_parts_init",
                  "bbb_seed_particles", "bbb_step", "bbb_last_status",
-                 "bbb_device_count", "bbb_prepare"):
+                 "bbb_device_count", "bbb_prepare", "bbb_learn_enable",
+                 "bbb_learn_crops", "bbb_learn_param_count",
+                 "bbb_learn_get_params", "bbb_learn_set_params",
+                 "bbb_learn_forward", "bbb_PP_bicgstab_static"):
         getattr(lib, name).restype = C.c_int
     lib.bbb_kernel_launches.restype = C.c_longlong
     lib.bbb_status_string.restype = C.c_char_p

@@ -57,5 +57,6 @@ def build(force=False, verbose=False, extra=()):
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True)
+    build(force="--force" in sys.argv, verbose=True,
+          extra=[a for a in sys.argv[1:] if a.startswith("-D")])
     print(LIB)

@@ -64,7 +64,12 @@ static void dfree(T *&p) { if(p) cudaFree(p); p = NULL; }
 /* src/cuda_bluebottle.cu:36-297 */
 extern "C" void cuda_dom_malloc(void)
 {
-  if(g_dev.ready) return;
+  /* a second set-up (a new domain in the same process) releases the
+   * previous device state first: its arrays are sized for the old domain */
+  if(g_dev.ready) {
+    cuda_part_free();
+    cuda_dom_free();
+  }
   int ndev = 0;
   if(cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
     bbb_set_status(BBB_ERR_CUDA, "no CUDA device");

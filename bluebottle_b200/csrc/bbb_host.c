@@ -113,6 +113,15 @@ void bbb_set_status(int status, const char *where)
       where ? where : "");
 }
 
+/* as bbb_set_status, naming the source line of the failed call */
+void bbb_set_status_at(int status, const char *what, const char *file, int line)
+{
+  char buf[256];
+  const char *base = strrchr(file, '/');
+  snprintf(buf, sizeof(buf), "%s at %s:%d", what ? what : "", base ? base + 1 : file, line);
+  bbb_set_status(status, buf);
+}
+
 int bbb_fail_exit(void) { return g_exit_on_failure; }
 
 /* record/solver_*.rec, the format of src/recorder.c:1891-1953 */
@@ -559,6 +568,34 @@ static void free_parts_arrays(void)
   phase = phase_shell = flag_u = flag_v = flag_w = NULL;
 }
 
+/* the collision bin grid (binDom_init, src/particle.c:598): bins of at
+ * least 2 a_max + ratio a_max per side, cell-centred indices only */
+static void bin_dom_init(void)
+{
+  real rmax = 0;
+  for(int i = 0; i < nparts; i++)
+    rmax = rmax + (parts[i].r > rmax) * (parts[i].r - rmax);
+  memset(&binDom, 0, sizeof(binDom));
+  real span = 2. * rmax + interactionLengthRatio * rmax;
+  binDom.xs = Dom.xs; binDom.xe = Dom.xe; binDom.xl = Dom.xl;
+  binDom.xn = (int)floor(Dom.xl / span);
+  if(binDom.xn == 0) { binDom.xn = 1; binDom.dx = Dom.xl; }
+  else binDom.dx = Dom.xl / binDom.xn;
+  binDom.ys = Dom.ys; binDom.ye = Dom.ye; binDom.yl = Dom.yl;
+  binDom.yn = (int)floor(Dom.yl / span);
+  if(binDom.yn == 0) { binDom.yn = 1; binDom.dy = Dom.yl; }
+  else binDom.dy = Dom.yl / binDom.yn;
+  binDom.zs = Dom.zs; binDom.ze = Dom.ze; binDom.zl = Dom.zl;
+  binDom.zn = (int)floor(Dom.zl / span);
+  if(binDom.zn == 0) { binDom.zn = 1; binDom.dz = Dom.zl; }
+  else binDom.dz = Dom.zl / binDom.zn;
+  grid_info *G = &binDom.Gcc;
+  G->is = BBB_DOM_BUF; G->in = binDom.xn; G->ie = G->is + G->in;
+  G->js = BBB_DOM_BUF; G->jn = binDom.yn; G->je = G->js + G->jn;
+  G->ks = BBB_DOM_BUF; G->kn = binDom.zn; G->ke = BBB_DOM_BUF + G->kn;
+  G->s1 = G->in; G->s2 = G->s1 * G->jn; G->s3 = G->s2 * G->kn;
+}
+
 int bbb_parts_init(void)
 {
   free_parts_arrays();
@@ -653,6 +690,7 @@ int bbb_parts_init(void)
     gradP.zm = ex * g.zm / (Dom.xl * Dom.yl * Dom.zl);
     gradP.za = 0.;
   }
+  bin_dom_init();
   return BBB_OK;
 }
 

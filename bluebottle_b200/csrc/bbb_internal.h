@@ -118,6 +118,7 @@ bbb_geom bbb_make_geom(void);
 extern "C" {
 #endif
 void bbb_set_status(int status, const char *where);
+void bbb_set_status_at(int status, const char *what, const char *file, int line);
 int bbb_fail_exit(void);
 extern bbb_options g_opt;
 extern bbb_stats g_stats;
@@ -127,10 +128,10 @@ void bbb_record_solver(const char *name, int niter, real resid);
 #endif
 
 #define BBB_CK(call) do { cudaError_t e_ = (call); if(e_ != cudaSuccess) { \
-  bbb_set_status(BBB_ERR_CUDA, cudaGetErrorString(e_)); } } while(0)
+  bbb_set_status_at(BBB_ERR_CUDA, cudaGetErrorString(e_), __FILE__, __LINE__); } } while(0)
 #define BBB_LAUNCHED() do { g_dev.launches++; \
   cudaError_t e_ = cudaPeekAtLastError(); if(e_ != cudaSuccess) \
-    bbb_set_status(BBB_ERR_CUDA, cudaGetErrorString(e_)); } while(0)
+    bbb_set_status_at(BBB_ERR_CUDA, cudaGetErrorString(e_), __FILE__, __LINE__); } while(0)
 
 /* entry points between the .cu files */
 void bbb_dev_require(void);

@@ -50,6 +50,9 @@
 #define HY (TY + 2)
 #define NTHR (TX * TY)
 #define NPW 1184          /* blocks of the pointwise passes (8 per SM) */
+#ifndef BBB_KRY_MINB
+#define BBB_KRY_MINB 4    /* resident blocks per SM the BiCGSTAB passes target */
+#endif
 
 /* operator constants in the form the kernels use */
 struct opc {
@@ -65,7 +68,9 @@ struct boxc {
   int wW, wE, wS, wN, wB, wT;   /* wrapped neighbour index at each edge */
   int vec;                      /* cells per thread along x            */
   int tiles_x;                  /* tiles along x                       */
-  long long units, chunk;       /* tiles * nz; units per block         */
+  long long units;              /* tiles * nz                          */
+  int nblk;                     /* blocks; block b takes q or q+1 units */
+  long long q, r;               /* units / nblk, units % nblk          */
 };
 
 /* vector width usable for a row of nx cells of element size `esz` */
@@ -90,7 +95,8 @@ static int sm_count(void)
 }
 
 /* `per_sm` resident blocks of the stencil kernels: the units are split
- * evenly over one wave of resident blocks (at least 4 planes per block) */
+ * evenly over exactly one wave of resident blocks, so every SM holds the
+ * same number of blocks (at least 4 planes per block) */
 static boxc make_box(int nx, int ny, int nz, int perx, int pery, int perz,
   int dupx, int dupy, int dupz, int vec, int per_sm)
 {
@@ -108,15 +114,17 @@ static boxc make_box(int nx, int ny, int nz, int perx, int pery, int perz,
   b.units = tiles * nz;
   if(per_sm < 1) per_sm = 1;
   long long slots = (long long)sm_count() * per_sm;
-  long long chunk = (b.units + slots - 1) / slots;
-  if(chunk < 4) chunk = 4;
-  b.chunk = chunk;
+  long long nb = b.units / 4 < slots ? b.units / 4 : slots;
+  if(nb < 1) nb = 1;
+  b.nblk = (int)nb;
+  b.q = b.units / nb;
+  b.r = b.units % nb;
   return b;
 }
 
 static dim3 box_grid(const boxc &b)
 {
-  return dim3((unsigned)((b.units + b.chunk - 1) / b.chunk));
+  return dim3((unsigned)b.nblk);
 }
 
 template <typename K>
@@ -379,12 +387,9 @@ __device__ __forceinline__ void seg_stencilV(const boxc &B, const opc &O,
   }
   for(int k = k0; k < k1; k++) {
     int slot = (k - k0) % 3, nslot = (k - k0 + 1) % 3;
-    long long cn = lin(B, ib, gj, mapz(B, k + 1));
-    prod.template ev<V>(cn, raw_next, q_next, tab.dinv, valid && (k + 1 < k1),
-      red);
-    m_next = ldmw<V>(mask, cn);
+    /* halo first: it only loads, so the owned cells' loads below can be
+     * issued before its results are used */
     if(k + 1 < k1) {
-      stv<T, V>(&ring[nslot][ty + 1][0], tx * V, q_next);
       if(hrow >= 0) {
         prod.template ev<V>(lin(B, hgi, hgj, k + 1), tr, tq, tab.dinv, false,
           red);
@@ -397,6 +402,11 @@ __device__ __forceinline__ void seg_stencilV(const boxc &B, const opc &O,
         (hcol == 0 ? hw : he)[nslot][(tid - 64) & 7] = bq[0];
       }
     }
+    long long cn = lin(B, ib, gj, mapz(B, k + 1));
+    prod.template ev<V>(cn, raw_next, q_next, tab.dinv, valid && (k + 1 < k1),
+      red);
+    m_next = ldmw<V>(mask, cn);
+    if(k + 1 < k1) stv<T, V>(&ring[nslot][ty + 1][0], tx * V, q_next);
     __syncthreads();
     T left = __shfl_up_sync(0xffffffffu, q_cur[V - 1], 1);
     T right = __shfl_down_sync(0xffffffffu, q_cur[0], 1);
@@ -431,8 +441,9 @@ __device__ __forceinline__ void tile_stencil(const boxc &B, const opc &O,
   const uint8_t *__restrict__ mask, const optab<T> &tab, P &prod, E &epi,
   double (&red)[NRED])
 {
-  long long u0 = (long long)blockIdx.x * B.chunk;
-  long long u1 = u0 + B.chunk < B.units ? u0 + B.chunk : B.units;
+  long long bx_ = blockIdx.x;
+  long long u0 = bx_ * B.q + (bx_ < B.r ? bx_ : B.r);
+  long long u1 = u0 + B.q + (bx_ < B.r ? 1 : 0);
   while(u0 < u1) {
     long long tile = u0 / B.nz;
     int k0 = (int)(u0 - tile * B.nz);
@@ -671,7 +682,7 @@ struct epi_A {
 };
 
 template <typename T, int V>
-__global__ void __launch_bounds__(NTHR, 3) k_bicgA(boxc B, opc O,
+__global__ void __launch_bounds__(NTHR, BBB_KRY_MINB) k_bicgA(boxc B, opc O,
   const uint8_t *__restrict__ mask, const T *sv, const T *tv, const T *p_old,
   const T *v_old, const T *__restrict__ rh, T *r, T *p_new, T *v_new, T *x,
   bbb_kry *s, double *partials)
@@ -754,7 +765,7 @@ struct epi_B {
 };
 
 template <typename T, int V>
-__global__ void __launch_bounds__(NTHR, 3) k_bicgB(boxc B, opc O,
+__global__ void __launch_bounds__(NTHR, BBB_KRY_MINB) k_bicgB(boxc B, opc O,
   const uint8_t *__restrict__ mask, const T *r, const T *v,
   const T *__restrict__ rh, T *s_out, T *t_out, bbb_kry *s, double *partials)
 {
@@ -1534,10 +1545,190 @@ __global__ void k_cg_writeback(const double *x, real *star, bbb_geom G,
   }
 }
 
+/* ------------------------------------------------ mixed-precision CG
+ * The Crank-Nicolson Helmholtz solves in the FP32-inner form: FP64 outer
+ * residual r = b - A x (b = u* on the component's faces, x from 0), FP32
+ * Jacobi-CG on A e = r to `inner_tol` (or looser when half the remaining
+ * reduction suffices), x += e in FP64; stops on the FP64 test
+ * ||r|| <= pp_residual ||b|| of the FP64 form. */
+
+/* b = u* (dense FP64), x = 0, ||b||; the finaliser sets up the outer
+ * scalars */
+__global__ void k_helm_b(const real *star, bbb_geom G, int comp, int nx,
+  int ny, int nz, double *b, double *x, bbb_kry *s, double *partials,
+  double rtol, int max_outer)
+{
+  __shared__ double sh[32];
+  int s1 = comp == 0 ? G.fx_s1 : (comp == 1 ? G.fy_s1 : G.fz_s1);
+  int s2 = comp == 0 ? G.fx_s2 : (comp == 1 ? G.fy_s2 : G.fz_s2);
+  long long n = (long long)nx * ny * nz;
+  double red[1] = {0.};
+  for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+      t += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(t % nx) + 1;
+    long long rr = t / nx;
+    int j = (int)(rr % ny) + 1, k = (int)(rr / ny) + 1;
+    double bv = star[i + (long long)j * s1 + (long long)k * s2];
+    b[t] = bv;
+    x[t] = 0.;
+    red[0] += bv * bv;
+  }
+  if(bbb_grid_partial<1>(red, partials, &s->ticket, sh)) {
+    bbb_grid_finish_sum<1>(red, partials, &s->ticket, sh);
+    if(threadIdx.x == 0) {
+      double bn = sqrt(red[0]);
+      s->bnorm = bn;
+      s->rnorm = bn;
+      s->tol = rtol * bn;
+      s->iter = 0;
+      s->maxit = max_outer;
+      s->converged = 0;
+      s->done = 0;
+      s->status = isfinite(bn) ? 0 : BBB_ERR_NONFINITE;
+      if(!isfinite(bn)) s->done = 1;
+    }
+  }
+}
+
+/* FP32 inner CG from e = 0: z = M r, p = z, (r, z), ||r|| */
+template <int V>
+__global__ void __launch_bounds__(256) k_cg_inner_setup(long long n, opc O,
+  const uint8_t *__restrict__ mask, const float *__restrict__ r, float *e,
+  float *p, bbb_kry *si, double *partials)
+{
+  if(((volatile bbb_kry *)si)->done) return;
+  __shared__ double sh[32 * 2];
+  __shared__ optab<float> tab;
+  optab_fill<float>(tab, O);
+  double red[2] = {0., 0.};
+  long long nv = n / V;
+  for(long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nv;
+      q += (long long)gridDim.x * blockDim.x) {
+    long long c = q * V;
+    float rv[V], z[V], zero[V];
+    unsigned mm[V];
+    ldv<float, V>(r, c, rv);
+    ldm<V>(mask, c, mm);
+#pragma unroll
+    for(int a = 0; a < V; a++) {
+      z[a] = tab.dinv[mm[a]] * rv[a];
+      zero[a] = 0.f;
+      red[0] += (double)rv[a] * (double)z[a];
+      red[1] += (double)rv[a] * (double)rv[a];
+    }
+    stv<float, V>(p, c, z);
+    stv<float, V>(e, c, zero);
+  }
+  if(bbb_grid_partial<2>(red, partials, &si->ticket, sh)) {
+    bbb_grid_finish_sum<2>(red, partials, &si->ticket, sh);
+    if(threadIdx.x == 0) {
+      double rn = sqrt(red[1]);
+      si->rho = red[0];
+      si->rnorm = rn;
+      si->iter = 0;
+      si->first = 1;
+      si->beta = 0.;
+      si->converged = (rn <= si->tol);
+      si->done = si->converged || si->maxit <= 0 || !isfinite(rn);
+      si->status = isfinite(rn) ? 0 : BBB_ERR_NONFINITE;
+    }
+  }
+}
+
+template <int VD, int VF>
+static int helmholtz_mixed(const boxc &BD, const boxc &BF, const opc &O,
+  const uint8_t *mask, long long n, bbb_geom G, int comp, real *star)
+{
+  ensure_fp32();
+  bbb_kry *s = g_dev.kry, *si = g_dev.kry_inner;
+  int max_outer = g_opt.max_outer > 0 ? g_opt.max_outer : 20;
+  double itol = g_opt.inner_tol > 0 ? g_opt.inner_tol : 1e-4;
+  int nx = BD.nx, ny = BD.ny, nz = BD.nz;
+  k_helm_b<<<NPW, 256, 0, g_dev.stream>>>(star, G, comp, nx, ny, nz, g_dev.kb,
+    g_dev.kx, s, g_dev.partials, pp_residual, max_outer);
+  BBB_LAUNCHED();
+  dim3 grdD = box_grid(BD), grdF = box_grid(BF), blk(TX, TY);
+  int inner_total = 0;
+  for(int outer = 0; outer <= max_outer; outer++) {
+    k_outer_resid<VD><<<grdD, blk, 0, g_dev.stream>>>(BD, O, mask, g_dev.kb,
+      g_dev.kx, g_dev.fr, s, si, g_dev.partials, itol, pp_max_iter, 0, n);
+    BBB_LAUNCHED();
+    k_cg_inner_setup<VF><<<NPW, 256, 0, g_dev.stream>>>(n, O, mask, g_dev.fr,
+      g_dev.fx, g_dev.fp[0], si, g_dev.partials);
+    BBB_LAUNCHED();
+    int cur = 0;
+    drive(si, [&]() {
+      k_cg1<float, VF><<<grdF, blk, 0, g_dev.stream>>>(BF, O, mask, g_dev.fr,
+        g_dev.fp[cur], g_dev.fp[cur ^ 1], g_dev.fv[0], si, g_dev.partials);
+      BBB_LAUNCHED();
+      k_cg2<float><<<NPW, 256, 0, g_dev.stream>>>(n, O, mask, g_dev.fx,
+        g_dev.fp[cur ^ 1], g_dev.fr, g_dev.fv[0], si, g_dev.partials);
+      BBB_LAUNCHED();
+      cur ^= 1;
+    }, pp_max_iter, 2);
+    if(bbb_last_status() == BBB_ERR_CUDA) return -1;
+    inner_total += g_dev.kry_host->iter;
+    k_accumulate<VF><<<NPW, 256, 0, g_dev.stream>>>(n, g_dev.kx, g_dev.fx, s);
+    BBB_LAUNCHED();
+    BBB_CK(cudaMemcpyAsync(g_dev.kry_host, s, sizeof(bbb_kry),
+      cudaMemcpyDeviceToHost, g_dev.stream));
+    BBB_CK(cudaStreamSynchronize(g_dev.stream));
+    if(g_dev.kry_host->done) break;
+  }
+  k_cg_writeback<<<NPW, 256, 0, g_dev.stream>>>(g_dev.kx, star, G, comp,
+    nx, ny, nz);
+  BBB_LAUNCHED();
+  return inner_total;
+}
+
 int bbb_helmholtz_solve(int comp)
 {
   bbb_dev_require();
   if(!g_dev.ready) return -1;
+  if(g_opt.precision == BBB_PREC_MIXED) {
+    bbb_build_masks();
+    bbb_geom G = bbb_make_geom();
+    int nx = G.nx + (comp == 0), ny = G.ny + (comp == 1), nz = G.nz + (comp == 2);
+    int per[3][3] = {{bc.uW, bc.uS, bc.uB}, {bc.vW, bc.vS, bc.vB}, {bc.wW, bc.wS, bc.wB}};
+    int px = per[comp][0] == BBB_PERIODIC, py = per[comp][1] == BBB_PERIODIC,
+        pz = per[comp][2] == BBB_PERIODIC;
+    int VD = pick_vec(nx, sizeof(double)), VF = pick_vec(nx, sizeof(float));
+    static int smd[3], smf[3];
+    if(!smd[0]) {
+      smd[1] = resident(k_outer_resid<1>); smd[2] = resident(k_outer_resid<2>);
+      smf[1] = resident(k_cg1<float, 1>); smf[2] = resident(k_cg1<float, 4>);
+      smd[0] = 1;
+    }
+    boxc BD = make_box(nx, ny, nz, px, py, pz, comp == 0, comp == 1, comp == 2,
+      VD, smd[VD == 2 ? 2 : 1]);
+    boxc BF = make_box(nx, ny, nz, px, py, pz, comp == 0, comp == 1, comp == 2,
+      VF, smf[VF == 4 ? 2 : 1]);
+    opc O;
+    O.wx = 0.5 * nu * dt * (1. / (G.dx * G.dx));
+    O.wy = 0.5 * nu * dt * (1. / (G.dy * G.dy));
+    O.wz = 0.5 * nu * dt * (1. / (G.dz * G.dz));
+    O.helm = 1;
+    const uint8_t *mask = comp == 0 ? g_dev.mask_u : (comp == 1 ? g_dev.mask_v : g_dev.mask_w);
+    real *star = comp == 0 ? g_dev.us : (comp == 1 ? g_dev.vs : g_dev.ws);
+    long long n = (long long)nx * ny * nz;
+    int it;
+    if(VD == 2 && VF == 4) it = helmholtz_mixed<2, 4>(BD, BF, O, mask, n, G, comp, star);
+    else if(VD == 2) it = helmholtz_mixed<2, 1>(BD, BF, O, mask, n, G, comp, star);
+    else it = helmholtz_mixed<1, 1>(BD, BF, O, mask, n, G, comp, star);
+    bbb_kry *h = g_dev.kry_host;
+    real resid = h->bnorm > 0 ? h->rnorm / h->bnorm : h->rnorm;
+    g_stats.helm_iters_total += it > 0 ? it : 0;
+    bbb_record_solver("solver_helmholtz_expd.rec", it, resid);
+    if(h->status == BBB_ERR_NONFINITE) bbb_set_status(BBB_ERR_NONFINITE, "Helmholtz");
+    if(!h->converged) {
+      bbb_set_status(BBB_ERR_NOT_CONVERGED, "Helmholtz (mixed)");
+      if(bbb_fail_exit()) {
+        printf("The Helmholtz equation did not converge.              \n");
+        exit(EXIT_FAILURE);
+      }
+    }
+    return it;
+  }
   bbb_build_masks();
   bbb_geom G = bbb_make_geom();
   int nx = G.nx + (comp == 0), ny = G.ny + (comp == 1), nz = G.nz + (comp == 2);

@@ -1749,23 +1749,21 @@ __global__ void k_move(part_struct *parts, int np, int final, double dt,
   d_move(&parts[i], final, dt, rho_f, g, gp, G);
 }
 
-/* bin grid of binDom_init (src/particle.c:598) from the particle radii */
+/* the bin grid of binDom (binDom_init, src/particle.c:598, filled on the
+ * host by bbb_parts_init or by the reference's own host code) */
 static void bins_setup(void)
 {
   if(g_bins.cnt && g_bins.np == nparts) return;
-  double rmax = 0;
-  for(int i = 0; i < nparts; i++)
-    rmax = rmax + (parts[i].r > rmax) * (parts[i].r - rmax);
-  double ilr = interactionLengthRatio;
   bin_geom &b = g_bins.bg;
-  b.xs = Dom.xs; b.ys = Dom.ys; b.zs = Dom.zs;
-  b.xn = (int)floor(Dom.xl / (2. * rmax + ilr * rmax));
-  if(b.xn == 0) { b.xn = 1; b.dx = Dom.xl; } else b.dx = Dom.xl / b.xn;
-  b.yn = (int)floor(Dom.yl / (2. * rmax + ilr * rmax));
-  if(b.yn == 0) { b.yn = 1; b.dy = Dom.yl; } else b.dy = Dom.yl / b.yn;
-  b.zn = (int)floor(Dom.zl / (2. * rmax + ilr * rmax));
-  if(b.zn == 0) { b.zn = 1; b.dz = Dom.zl; } else b.dz = Dom.zl / b.zn;
-  b.s1 = b.xn; b.s2 = b.s1 * b.yn; b.s3 = b.s2 * b.zn;
+  b.xs = binDom.xs; b.ys = binDom.ys; b.zs = binDom.zs;
+  b.dx = binDom.dx; b.dy = binDom.dy; b.dz = binDom.dz;
+  b.xn = binDom.xn; b.yn = binDom.yn; b.zn = binDom.zn;
+  b.s1 = binDom.Gcc.s1; b.s2 = binDom.Gcc.s2; b.s3 = binDom.Gcc.s3;
+  if(b.s3 <= 0 || b.s1 <= 0 || b.s2 <= 0) {
+    bbb_set_status(BBB_ERR_CONFIG, "collision bins (binDom) not set up");
+    b.s3 = 0;
+    return;
+  }
   g_bins.s3 = b.s3;
   g_bins.np = nparts;
   int *ps[3];
@@ -1809,6 +1807,7 @@ static void move_parts_seq(int final)
   bbb_geom G = bbb_make_geom();
   if(nparts > 1) {
     bins_setup();
+    if(g_bins.bg.s3 <= 0) return;
     const bin_geom &bg = g_bins.bg;
     BBB_CK(cudaMemsetAsync(g_bins.cnt, 0, sizeof(int) * (size_t)bg.s3, g_dev.stream));
     BBB_CK(cudaMemsetAsync(g_bins.fill, 0, sizeof(int) * (size_t)bg.s3, g_dev.stream));

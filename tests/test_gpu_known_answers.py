@@ -47,10 +47,13 @@ def test_stokes_sphere_on_gpu(gpu, tmp_path):
         assert abs(g.Fz - c.Fz) <= 1e-12 * drag
         for k in ("Fx", "Fy", "Lx", "Ly", "Lz"):
             assert abs(getattr(g, k) - getattr(c, k)) < 1e-14, k
-        for nm in ("pnm_re", "phinm_re", "chinm_re", "pnm_im", "phinm_im",
-                   "chinm_im"):
+        # the modes the Stokes field does not excite are round-off (~1e-19):
+        # compare every coefficient on the scale of the largest one
+        names = ("pnm_re", "phinm_re", "chinm_re", "pnm_im", "phinm_im", "chinm_im")
+        scale = max(np.abs(orc.field(nm)).max() for nm in names)
+        for nm in names:
             e = np.abs(sim.array(nm) - orc.field(nm)).max()
-            assert e <= 1e-12 * max(np.abs(orc.field(nm)).max(), 1e-30) + 1e-22, nm
+            assert e <= 1e-12 * scale, nm
         for nm in ("u", "v", "w"):
             got = sim.array(nm)
             assert np.array_equal(sim.array("flag_" + nm), orc.field("flag_" + nm))

@@ -80,8 +80,12 @@ def _torch_net(feat, W, b, dims, periodic, emulate_bf16=True):
 
 def _prepared_sim():
     sim = Sim(configs.taylor_green(32))
-    sim.prepare()
-    assert sim.lib.bbb_learn_enable(0) == 0
+    try:
+        sim.prepare()
+        assert sim.lib.bbb_learn_enable(0) == 0
+    except BaseException:
+        sim.close()
+        raise
     return sim
 
 
@@ -185,7 +189,11 @@ def test_online_record_train_use_keeps_parity(gpu):
     wl = configs.sedimentation((128, 32, 32), (32.0, 8.0, 8.0), 4, nu=0.1,
                                tol=1e-10, lamb_max_iter=2, seed=4)
     sim = Sim(wl, options=dict(lamb_max_iter_override=2, learned_guess=1))
-    orc = Oracle.from_sim(sim)
+    try:
+        orc = Oracle.from_sim(sim)
+    except BaseException:
+        sim.close()
+        raise
     try:
         sim.prepare()
         lib = sim.lib

@@ -140,3 +140,31 @@ def test_particle_step_parity(gpu):
     finally:
         sim.close()
         orc.close()
+
+
+def test_mixed_precision_vector_paths_with_particles(gpu):
+    """FP32-inner form on a 128-cell row length, so the 4-wide FP32 and
+    2-wide FP64 stencil paths run (Poisson and the v, w Helmholtz
+    systems; u has 129 faces per row and takes the scalar path), with
+    spheres: fields within what the 1e-10 stopping rule allows of the FP64
+    oracle."""
+    wl = configs.sedimentation((128, 32, 32), (32.0, 8.0, 8.0), 4, nu=0.1,
+                               tol=1e-10, lamb_max_iter=2, seed=5, prec=1)
+    sim, orc, stats = _run_pair(wl, 2, options=dict(precision=1,
+                                                     lamb_max_iter_override=2))
+    try:
+        d = sim.dom
+        for name in ("u", "v", "w", "p"):
+            e = rel_err(field_interior(d, name, sim.array(name)),
+                        field_interior(d, name, orc.field(name)))
+            assert e < 1e-7, (name, e)
+        for g, _ in stats:
+            assert g.pp_resid_last <= 1e-10
+            assert g.helm_iters_total > 0
+        for pg, po in zip(sim.parts(), orc.field("parts")):
+            for k in ("x", "z", "u", "w", "Fz"):
+                a, b = getattr(pg, k), getattr(po, k)
+                assert abs(a - b) <= 1e-7 * max(1.0, abs(b)), (k, a, b)
+    finally:
+        sim.close()
+        orc.close()

@@ -5,7 +5,7 @@ src/rng.c unmodified into oracle/_ref/libref_host.so.  Both read the same
 flow.config / part.config; the domain structs, boundary conditions, scalar
 globals, particle records and initial fields must then be identical, field
 for field (domain_read_input src/domain.c:30, domain_init :1591,
-parts_read_input src/particle.c:79, parts_init :295).
+parts_read_input src/particle.c:79, parts_init :295, binDom_init :598).
 """
 import ctypes as C
 import os
@@ -96,6 +96,10 @@ def test_host_setup_matches_reference(tmp_path, case):
         md = C.POINTER(abi.DomStruct).in_dll(lib, "dom").contents
         assert _diff(rd, md, "dom[0]") == []
         assert _diff(abi.BCStruct.in_dll(ref, "bc"), sim.bc, "bc") == []
+        ref.binDom_init.restype = C.c_int
+        assert ref.binDom_init() == 0
+        assert _diff(abi.DomStruct.in_dll(ref, "binDom"),
+                     abi.DomStruct.in_dll(lib, "binDom"), "binDom") == []
         for g in ("g", "gradP"):
             assert _diff(abi.GStruct.in_dll(ref, g), abi.GStruct.in_dll(lib, g), g) == []
         for s in REAL_SCALARS:
