@@ -801,6 +801,8 @@ __global__ void __launch_bounds__(NTHR, BBB_KRY_MINB) k_bicgB(boxc B, opc O,
   }
 }
 
+#include "bbb_krylov_async.cuh"
+
 /* ------------------------------------------------ Poisson set-up and
  * write-back (src/bicgstab_kernel.cu:483-562, src/particle_kernel.cu:
  * 840-940, src/cuda_bicgstab.cu:971-1045) */
@@ -965,6 +967,50 @@ static int bicg_per_sm(void)
   return nb;
 }
 
+/* resident blocks per SM of the staged passes (0 when they cannot run) */
+template <typename T, int PASS>
+static int as_per_sm(void)
+{
+  static int nb = -1;
+  if(nb < 0) {
+    typedef as_layout<T, PASS> L;
+    nb = 0;
+    if(cudaFuncSetAttribute(k_bicg_async<T, PASS>,
+         cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM) == cudaSuccess) {
+      int v = 0;
+      if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_bicg_async<T, PASS>,
+           AS_THREADS, L::SMEM) == cudaSuccess) nb = v;
+    }
+    cudaGetLastError();
+  }
+  return nb;
+}
+
+/* the same box cut into 128-cell tiles for a kernel with `per_sm`
+ * resident blocks */
+static boxc retile(const boxc &B0, int per_sm)
+{
+  boxc b = B0;
+  b.vec = AS_W / TX;
+  b.tiles_x = b.nx / AS_W;
+  long long tiles = (long long)b.tiles_x * ((b.ny + TY - 1) / TY);
+  b.units = tiles * b.nz;
+  long long slots = (long long)sm_count() * (per_sm > 0 ? per_sm : 1);
+  long long nb = b.units / 4 < slots ? b.units / 4 : slots;
+  if(nb < 1) nb = 1;
+  b.nblk = (int)nb;
+  b.q = b.units / nb;
+  b.r = b.units % nb;
+  return b;
+}
+
+/* the staged passes run where rows are a multiple of 128 cells */
+#ifndef BBB_NO_ASYNC
+#define BBB_ASYNC_ON 1
+#else
+#define BBB_ASYNC_ON 0
+#endif
+
 /* BiCGSTAB iterations after the set-up kernel (s = r0, rh, scalars) */
 template <typename T, int V>
 static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
@@ -975,19 +1021,45 @@ static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
   T *pp[2] = {p0, p1}, *vv[2] = {v0, v1};
   int cur = 0, launched = 0;
   double w = sizeof(T);
+  bool staged = BBB_ASYNC_ON && B.nx % AS_W == 0 && as_per_sm<T, 0>() > 0
+    && as_per_sm<T, 1>() > 0;
+  boxc BA = B, BB = B;
+  if(staged) { BA = retile(B, as_per_sm<T, 0>()); BB = retile(B, as_per_sm<T, 1>()); }
   drive(s, [&]() {
     /* pass A: first reads s, rh; later s, t, p, v, x, rh; + mask */
     double a_bytes = launched == 0 ? (double)n * (5. * w + 1.)
                                    : (double)n * (10. * w + 1.);
     prof_event(0);
     prof_bytes(0, a_bytes);
-    k_bicgA<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, sv, tv, pp[cur],
-      vv[cur], rh, r, pp[cur ^ 1], vv[cur ^ 1], x, s, g_dev.partials);
+    if(staged) {
+      as_args<T> A;
+      A.mask = mask;
+      A.h[0] = sv; A.h[1] = tv; A.h[2] = pp[cur]; A.h[3] = vv[cur];
+      A.o[0] = x; A.o[1] = rh;
+      A.w0 = r; A.w1 = pp[cur ^ 1]; A.w2 = vv[cur ^ 1]; A.x = x;
+      A.s = s; A.partials = g_dev.partials;
+      k_bicg_async<T, 0><<<BA.nblk, AS_THREADS, as_layout<T, 0>::SMEM,
+        g_dev.stream>>>(BA, O, A);
+    } else {
+      k_bicgA<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, sv, tv, pp[cur],
+        vv[cur], rh, r, pp[cur ^ 1], vv[cur ^ 1], x, s, g_dev.partials);
+    }
     BBB_LAUNCHED();
     prof_event(1);
     prof_bytes(1, (double)n * (5. * w + 1.));
-    k_bicgB<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, r, vv[cur ^ 1],
-      rh, sv, tv, s, g_dev.partials);
+    if(staged) {
+      as_args<T> A;
+      A.mask = mask;
+      A.h[0] = r; A.h[1] = vv[cur ^ 1]; A.h[2] = NULL; A.h[3] = NULL;
+      A.o[0] = rh; A.o[1] = NULL;
+      A.w0 = sv; A.w1 = tv; A.w2 = NULL; A.x = NULL;
+      A.s = s; A.partials = g_dev.partials;
+      k_bicg_async<T, 1><<<BB.nblk, AS_THREADS, as_layout<T, 1>::SMEM,
+        g_dev.stream>>>(BB, O, A);
+    } else {
+      k_bicgB<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, r, vv[cur ^ 1],
+        rh, sv, tv, s, g_dev.partials);
+    }
     BBB_LAUNCHED();
     prof_event(2);
     prof_next();
