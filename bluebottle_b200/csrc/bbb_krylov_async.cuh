@@ -1,60 +1,106 @@
 /* bbb_krylov_async.cuh -- the two BiCGSTAB passes with their inputs staged
- * by asynchronous bulk copies (included by bbb_krylov.cu, which defines
- * boxc, opc, optab, op_apply, mapx/y/z, lin, ldv/stv and the reductions).
+ * by the tensor memory accelerator (included by bbb_krylov.cu, which
+ * defines boxc, opc, optab, op_apply, mapx/y/z, lin and the reductions).
  *
  * Same arithmetic as k_bicgA / k_bicgB, for rows of a multiple of 128
- * cells.  A block owns a 128 x 8 tile and marches along z; for every plane
- * it needs, one warp issues cp.async.bulk copies of whole 128-cell row
- * segments (plus the 16-byte chunks holding the x-halo cells) of each
- * input array into a shared-memory stage, and the stage's mbarrier
- * completes when all bytes have landed.  Three stages rotate, so two
- * planes are in flight while the block computes the third: the memory
- * system sees long bulk transfers independent of the threads' registers,
- * instead of one load round per plane per thread.  The compute reads the
- * stage exactly as the register version reads global memory.
+ * cells.  A block owns a 128 x 8 tile and marches along z.  For every plane
+ * it needs, one thread issues a handful of 3-D tensor copies -- per input
+ * array one box of 10 rows x (128 + two 16-byte x-halo chunks), the mask
+ * likewise, the block's own 8 rows of the arrays only it reads -- into a
+ * shared-memory stage whose mbarrier completes when all bytes have landed.
+ * Three stages rotate, so two planes are in flight while the block computes
+ * the third; the warps synchronise only through the stages' barriers and
+ * release counts, never block-wide inside a run of planes.
  *
- * Stage layout (bytes; T the element type, CH = 16 / sizeof(T) cells per
- * 16-byte chunk, W = 128):
- *   halo arrays (pass A: s, t, p, v; pass B: r, v), 10 rows each (tile rows
- *     j0-1 .. j0+8), a row = [CH cells left of the tile | W cells | CH cells
- *     right], the side chunks filled for the 8 tile rows only;
- *   mask, 10 rows of [16 | 128 | 16] bytes;
- *   own arrays (pass A: x, rh; pass B: rh), 8 rows of W cells.
+ * Every warp owns one tile row and computes the Jacobi-scaled stencil input
+ * q for its row and for the rows just south and north of it straight from
+ * the stage (no shared ring, so three stages fit twice per SM in FP32); the
+ * row's x-halo q comes from the stage's halo chunks.  q of the plane below
+ * and of the plane being stencilled stay in registers.
+ *
+ * Wrap-around neighbours that a tiled box cannot express land in slots of
+ * their own, never under a box (two asynchronous writes to one byte would
+ * race): the rows y = -1 and y = ny (the box's wS / wN rows) as plain bulk
+ * copies of the tile's 128 cells, and the x-halo chunks at x = -1 and
+ * x = nx (holding cells wW / wE) as 16-byte-wide boxes of the tile's 8
+ * rows.  The tiled boxes' out-of-range parts are zero-filled and never read.
+ *
  * Waits on the stage barriers are bounded; a wait that runs out marks the
  * solve failed (status BBB_ERR_CUDA through the scalars) and the kernel
- * carries on without reading stale data past its bounds. */
+ * carries on without reading past its buffers. */
 #ifndef BBB_KRYLOV_ASYNC_CUH
 #define BBB_KRYLOV_ASYNC_CUH
+
+#include <cuda.h>
 
 #define AS_W 128
 #define AS_NS 3
 #define AS_THREADS 256
 
+__host__ __device__ constexpr int as_rup(int v, int a) { return (v + a - 1) / a * a; }
+
+/* Stage layout in bytes (T the element type, CH = 16 / sizeof(T)):
+ *   per halo array (pass A: s, t, p, v; pass B: r, v) a region of
+ *     10 box rows of [CH | 128 | CH] cells (tile rows j0-1 .. j0+8),
+ *     2 extra rows of 128 cells (y = -1, y = ny);
+ *   mask: 10 rows of [16 | 128 | 16] bytes, 2 extra rows of 128;
+ *   own arrays (pass A: x, rh; pass B: rh): 8 rows of 128 cells;
+ *   x-wrap chunks: per halo array and the mask [2 sides][8 rows][16 B].
+ * Regions start on 128-byte boundaries (tensor-copy destinations). */
 template <typename T, int PASS>
 struct as_layout {
-  static constexpr int CH = 16 / (int)sizeof(T);
-  static constexpr int NA = PASS == 0 ? 4 : 2;        /* halo arrays  */
-  static constexpr int NO = PASS == 0 ? 2 : 1;        /* own arrays   */
-  static constexpr int ROWB = (AS_W + 2 * CH) * (int)sizeof(T);
-  static constexpr int MROWB = 160;
-  static constexpr int OWNB = AS_W * (int)sizeof(T);
-  static constexpr int HALO_OFF = 0;
-  static constexpr int MASK_OFF = NA * 10 * ROWB;
-  static constexpr int OWN_OFF = MASK_OFF + 10 * MROWB;
-  static constexpr int STAGE = OWN_OFF + NO * 8 * OWNB;
-  /* bytes one stage receives */
-  static constexpr int TXB = NA * (10 * AS_W * (int)sizeof(T) + 16 * 16)
-    + (10 * 128 + 16 * 16) + NO * 8 * OWNB;
-  static constexpr int NCOPY = NA * 26 + 26 + NO * 8;
-  static constexpr int RING_OFF = AS_NS * STAGE;
-  static constexpr int RING = 3 * 10 * AS_W * (int)sizeof(T);
-  static constexpr int HWE_OFF = RING_OFF + RING;
-  static constexpr int HWE = 2 * 3 * 8 * (int)sizeof(T);
-  static constexpr int TAB_OFF = HWE_OFF + HWE;
-  static constexpr int TAB = 2 * 128 * (int)sizeof(T);
-  static constexpr int BAR_OFF = (TAB_OFF + TAB + 15) / 16 * 16;
-  static constexpr int SH_OFF = BAR_OFF + AS_NS * 8;
-  static constexpr int SMEM = SH_OFF + 32 * 5 * 8 + 16;
+  static constexpr int ESZ = (int)sizeof(T);
+  static constexpr int CH = 16 / ESZ;
+  static constexpr int NA = PASS == 0 ? 4 : 2;
+  static constexpr int NO = PASS == 0 ? 2 : 1;
+  static constexpr int BOXW = AS_W + 2 * CH;        /* halo-array box  */
+  static constexpr int BOXH = 10;
+  static constexpr int MBOXW = AS_W + 32;            /* mask box        */
+  static constexpr int ROWP = BOXW * ESZ;
+  static constexpr int OWNB = AS_W * ESZ;
+  static constexpr int EXT_OFF = 10 * ROWP;
+  static constexpr int AREG = as_rup(EXT_OFF + 2 * OWNB, 128);
+  static constexpr int MROWP = MBOXW;
+  static constexpr int MEXT_OFF = 10 * MROWP;
+  static constexpr int MREG = as_rup(MEXT_OFF + 2 * 128, 128);
+  static constexpr int MASK_OFF = NA * AREG;
+  static constexpr int OWN_OFF = MASK_OFF + MREG;
+  static constexpr int XW_OFF = OWN_OFF + NO * 8 * OWNB;
+  static constexpr int STAGE = as_rup(XW_OFF + (NA + 1) * 256, 128);
+  static constexpr int TAB_OFF = AS_NS * STAGE;
+  static constexpr int BAR_OFF = TAB_OFF + 2 * 128 * ESZ;
+  static constexpr int CNT_OFF = BAR_OFF + AS_NS * 8;   /* release counts */
+  static constexpr int SH_OFF = as_rup(CNT_OFF + AS_NS * 4, 16);
+  /* + 128: the dynamic window is aligned up to 128 bytes at run time */
+  static constexpr int SMEM = SH_OFF + 32 * 5 * 8 + 128;
+  /* resident blocks per SM the register budget targets */
+  static constexpr int MINB = ESZ == 4 ? (PASS == 1 ? 3 : 2) : (PASS == 1 ? 2 : 1);
+  /* plane-aligned block runs (retile): measured faster for the FP32 pass A
+   * only -- the latency-bound passes lose more to the idle slots */
+  static constexpr bool ALIGN = ESZ == 4 && PASS == 0;
+  /* bytes a stage receives: the boxes always, the wrap slots at edges */
+  static constexpr int TX_BASE = NA * BOXH * ROWP + BOXH * MROWP + NO * 8 * OWNB;
+  static constexpr int TX_XSIDE = (NA + 1) * 8 * 16;
+  static constexpr int TX_YSIDE = NA * OWNB + 128;
+};
+
+/* the tensor maps of one pass, passed by value as a grid constant */
+struct as_maps {
+  CUtensorMap h[4];     /* halo arrays, box {128 + 2 CH, 10, 1}    */
+  CUtensorMap hx[4];    /* halo arrays, box {CH, 8, 1}             */
+  CUtensorMap m, mx;    /* mask, boxes {160, 10, 1} and {16, 8, 1} */
+  CUtensorMap o[2];     /* own arrays, box {128, 8, 1}             */
+};
+
+/* the global arrays of one pass */
+template <typename T>
+struct as_args {
+  const uint8_t *mask;
+  const T *h[4];          /* halo arrays                                 */
+  T *w0, *w1, *w2;        /* pass A: r, p_new, v_new; pass B: s, t       */
+  T *x;                   /* pass A: x, updated in place                 */
+  bbb_kry *s;
+  double *partials;
 };
 
 __device__ __forceinline__ uint32_t as_saddr(const void *p)
@@ -71,6 +117,7 @@ __device__ __forceinline__ void as_expect(uint32_t bar, uint32_t bytes)
                :: "r"(bar), "r"(bytes) : "memory");
 }
 
+/* contiguous bulk copy global -> shared (16-byte aligned, 16-byte multiple) */
 __device__ __forceinline__ void as_copy(uint32_t dst, const void *src,
   uint32_t bytes, uint32_t bar)
 {
@@ -79,91 +126,97 @@ __device__ __forceinline__ void as_copy(uint32_t dst, const void *src,
                :: "r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
 }
 
-/* bounded wait for the phase of parity `par`; false when the limit ran out */
+/* 3-D tiled tensor copy of the box at (x, y, z); x * element size is a
+ * multiple of 16 bytes at every call site */
+__device__ __forceinline__ void as_box(uint32_t dst, const CUtensorMap *map,
+  int x, int y, int z, uint32_t bar)
+{
+  asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile"
+               ".mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+               :: "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y),
+                  "r"(z), "r"(bar) : "memory");
+}
+
+/* bounded wait for the phase of parity `par`; false when the limit ran
+ * out.  Each try may suspend the thread for up to 20 us until the phase
+ * completes, so waiting warps do not spin on the issue slots; the bound is
+ * 2^16 tries. */
 __device__ __forceinline__ bool as_wait(uint32_t bar, uint32_t par)
 {
-  for(int it = 0; it < (1 << 21); it++) {
+  for(int it = 0; it < (1 << 16); it++) {
     uint32_t ok;
     asm volatile("{\n\t.reg .pred p;\n\t"
-                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
                  "selp.u32 %0, 1, 0, p;\n\t}\n"
-                 : "=r"(ok) : "r"(bar), "r"(par) : "memory");
+                 : "=r"(ok) : "r"(bar), "r"(par), "r"(20000) : "memory");
     if(ok) return true;
   }
   return false;
 }
 
-__device__ __forceinline__ void as_fence_proxy(void)
+/* one warp's release of a stage: acquire-release add on the stage's count
+ * (orders the warp's reads of the stage before the refill its last
+ * releaser issues); returns the count before the add */
+__device__ __forceinline__ uint32_t as_release(uint32_t cnt)
 {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  uint32_t old;
+  asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], 1;"
+               : "=r"(old) : "r"(cnt) : "memory");
+  return old;
 }
 
-/* the global arrays of one pass */
-template <typename T>
-struct as_args {
-  const uint8_t *mask;
-  const T *h[4];          /* halo arrays                                 */
-  const T *o[2];          /* own arrays (pass A: x, rh; pass B: rh)      */
-  T *w0, *w1, *w2;        /* pass A: r, p_new, v_new; pass B: s, t       */
-  T *x;                   /* pass A: x, updated in place                 */
-  bbb_kry *s;
-  double *partials;
+/* where a tile touches the box's faces */
+struct as_edges {
+  int xl, xr, ys, yn;     /* i0 == 0, i0 + 128 == nx, j0 == 0, j0 + 8 >= ny */
 };
 
-/* Issue the bulk copies of plane gk of tile (i0, j0) into stage `st`
- * (warp 0; lane 0 arms the barrier with the stage's byte count first). */
+__device__ __forceinline__ as_edges as_tile_edges(const boxc &B, int i0, int j0)
+{
+  as_edges e;
+  e.xl = i0 == 0;
+  e.xr = i0 + AS_W == B.nx;
+  e.ys = j0 == 0;
+  e.yn = j0 + 8 >= B.ny;
+  return e;
+}
+
+/* Issue the copies of plane gk of tile (i0, j0) into the stage at shared
+ * address st (one thread; it arms the barrier with the byte count first). */
 template <typename T, int PASS>
 __device__ __forceinline__ void as_issue(const boxc &B, const as_args<T> &A,
-  uint8_t *st, uint32_t bar, int i0, int j0, int gk)
+  const as_maps &M, uint32_t st, uint32_t bar, int i0, int j0, int gk,
+  const as_edges &E)
 {
   typedef as_layout<T, PASS> L;
-  int lane = threadIdx.x & 31;
-  if(lane == 0) as_expect(bar, (uint32_t)L::TXB);
-  __syncwarp();
-  int gxl = mapx(B, i0 - 1), gxr = mapx(B, i0 + AS_W);
-  int cl = gxl / L::CH * L::CH, cr = gxr / L::CH * L::CH;
-  int ml = gxl / 16 * 16, mr = gxr / 16 * 16;
-  uint32_t sbase = as_saddr(st);
-  for(int c = lane; c < L::NCOPY; c += 32) {
-    int grp, q;
-    if(c < L::NA * 26) { grp = c / 26; q = c % 26; }
-    else if(c < L::NA * 26 + 26) { grp = L::NA; q = c - L::NA * 26; }
-    else { grp = L::NA + 1 + (c - L::NA * 26 - 26) / 8; q = (c - L::NA * 26 - 26) % 8; }
-    if(grp < L::NA) {                      /* halo array */
-      const T *src = A.h[grp];
-      uint32_t d = sbase + L::HALO_OFF + grp * 10 * L::ROWB;
-      if(q < 10) {
-        int gj = mapy(B, j0 - 1 + q);
-        as_copy(d + q * L::ROWB + L::CH * (int)sizeof(T), src + lin(B, i0, gj, gk),
-          AS_W * sizeof(T), bar);
-      } else {
-        int r = 1 + (q - 10) / 2, side = (q - 10) % 2;
-        int gj = mapy(B, j0 - 1 + r);
-        if(side == 0)
-          as_copy(d + r * L::ROWB, src + lin(B, cl, gj, gk), 16, bar);
-        else
-          as_copy(d + r * L::ROWB + (L::CH + AS_W) * (int)sizeof(T),
-            src + lin(B, cr, gj, gk), 16, bar);
-      }
-    } else if(grp == L::NA) {              /* mask */
-      uint32_t d = sbase + L::MASK_OFF;
-      if(q < 10) {
-        int gj = mapy(B, j0 - 1 + q);
-        as_copy(d + q * L::MROWB + 16, A.mask + lin(B, i0, gj, gk), 128, bar);
-      } else {
-        int r = 1 + (q - 10) / 2, side = (q - 10) % 2;
-        int gj = mapy(B, j0 - 1 + r);
-        if(side == 0)
-          as_copy(d + r * L::MROWB, A.mask + lin(B, ml, gj, gk), 16, bar);
-        else
-          as_copy(d + r * L::MROWB + 144, A.mask + lin(B, mr, gj, gk), 16, bar);
-      }
-    } else {                               /* own array rows 1..8 */
-      int b = grp - L::NA - 1, r = 1 + q;
-      int gj = mapy(B, j0 - 1 + r);
-      as_copy(sbase + L::OWN_OFF + b * 8 * L::OWNB + q * L::OWNB,
-        A.o[b] + lin(B, i0, gj, gk), L::OWNB, bar);
-    }
+  uint32_t tx = L::TX_BASE + (uint32_t)(E.xl + E.xr) * L::TX_XSIDE
+    + (uint32_t)(E.ys + E.yn) * L::TX_YSIDE;
+  as_expect(bar, tx);
+#pragma unroll
+  for(int a = 0; a < L::NA; a++)
+    as_box(st + a * L::AREG, &M.h[a], i0 - (L::BOXW - AS_W) / 2,
+      j0 - (L::BOXH - 8) / 2, gk, bar);
+  as_box(st + L::MASK_OFF, &M.m, i0 - (L::MBOXW - AS_W) / 2, j0 - (L::BOXH - 8) / 2,
+    gk, bar);
+#pragma unroll
+  for(int b = 0; b < L::NO; b++)
+    as_box(st + L::OWN_OFF + b * 8 * L::OWNB, &M.o[b], i0, j0, gk, bar);
+  for(int side = 0; side < 2; side++) {
+    if(side == 0 ? !E.xl : !E.xr) continue;
+    int g = side == 0 ? B.wW : B.wE;
+    uint32_t d = st + L::XW_OFF + side * 128;
+#pragma unroll
+    for(int a = 0; a < L::NA; a++)
+      as_box(d + a * 256, &M.hx[a], g / L::CH * L::CH, j0, gk, bar);
+    as_box(d + L::NA * 256, &M.mx, g / 16 * 16, j0, gk, bar);
+  }
+  for(int side = 0; side < 2; side++) {
+    if(side == 0 ? !E.ys : !E.yn) continue;
+    long long c = lin(B, i0, side == 0 ? B.wS : B.wN, gk);
+#pragma unroll
+    for(int a = 0; a < L::NA; a++)
+      as_copy(st + a * L::AREG + L::EXT_OFF + side * L::OWNB, A.h[a] + c,
+        L::OWNB, bar);
+    as_copy(st + L::MASK_OFF + L::MEXT_OFF + side * 128, A.mask + c, 128, bar);
   }
 }
 
@@ -191,260 +244,334 @@ __device__ __forceinline__ void as_st4(T *p, const T (&v)[4])
   }
 }
 
+/* r += sum of a[v] * b[v] over 4 cells: exact FP64 products (FP32
+ * operands widen exactly) summed one by one, the order of the register
+ * kernels.  (Fusing the 4 FP32 products in FP32 first saves a few
+ * instructions but cost the FP32 inner solves 3% more iterations.) */
+template <typename T>
+__device__ __forceinline__ void as_dot4(double &r, const T (&a)[4], const T (&b)[4])
+{
+#pragma unroll
+  for(int v = 0; v < 4; v++) r += (double)a[v] * (double)b[v];
+}
+
+template <typename T>
+__device__ __forceinline__ void as_sum4(double &r, const T (&a)[4])
+{
+#pragma unroll
+  for(int v = 0; v < 4; v++) r += (double)a[v];
+}
+
+/* (A q) at one cell, as op_apply (same terms in the same order), with the
+ * face terms of clear mask bits skipped rather than multiplied by zero --
+ * the same value for finite q; w* already carry the operator's sign */
+template <typename T>
+__device__ __forceinline__ T as_apply(unsigned m, T d, T wx, T wy, T wz, T qB,
+  T qS, T qW, T qC, T qE, T qN, T qT)
+{
+  T acc = (T)0.;
+  if(m & BBB_MB) acc += wz * qB;
+  if(m & BBB_MS) acc += wy * qS;
+  if(m & BBB_MW) acc += wx * qW;
+  acc += d * qC;
+  if(m & BBB_ME) acc += wx * qE;
+  if(m & BBB_MN) acc += wy * qN;
+  if(m & BBB_MT) acc += wz * qT;
+  return (m & BBB_MID) ? qC : acc;
+}
+
 /* pass scalars, read once per kernel */
 struct as_scal {
   double alpha, omega, beta, bo;
   int first;
 };
 
-/* The stencil input q at 4 consecutive cells of staged row `row` starting
- * at tile column `col`, and, for cells the block owns (`own`), the pass's
- * pointwise work: stores to global index gc and sums into red.  raw0/raw1
- * carry what the epilogue needs (pass A: rh; pass B: s, rh). */
+/* q at 4 consecutive cells of a staged row: h the first cell of array 0
+ * (array a at h + a * AREG), mw the 4 mask bytes */
 template <typename T, int PASS>
-__device__ __forceinline__ void as_cell4(const uint8_t *st, int row, int col,
-  const T *dinv, const as_scal &S, bool own, long long gc,
-  const as_args<T> &A, T (&q)[4], T (&raw0)[4], T (&raw1)[4], unsigned &mw,
-  double (&red)[5])
+__device__ __forceinline__ void as_q4(const uint8_t *h, unsigned mw,
+  const T *dinv, const as_scal &S, T (&q)[4])
 {
   typedef as_layout<T, PASS> L;
-  const int ho = (L::CH + col) * (int)sizeof(T);
-  mw = *reinterpret_cast<const unsigned *>(st + L::MASK_OFF + row * L::MROWB + 16 + col);
+  if constexpr(PASS == 0) {
+    T ss[4];
+    as_ld4<T>(h, ss);
+    if(S.first) {
+#pragma unroll
+      for(int a = 0; a < 4; a++) q[a] = dinv[mbyte(mw, a)] * ss[a];
+    } else {
+      T tt[4], pp[4], vv[4];
+      T om = (T)S.omega, be = (T)S.beta, bo = (T)S.bo;
+      as_ld4<T>(h + 1 * L::AREG, tt);
+      as_ld4<T>(h + 2 * L::AREG, pp);
+      as_ld4<T>(h + 3 * L::AREG, vv);
+#pragma unroll
+      for(int a = 0; a < 4; a++) {
+        T rr = ss[a] - om * tt[a];
+        T pn = rr + be * pp[a] + bo * vv[a];
+        q[a] = dinv[mbyte(mw, a)] * pn;
+      }
+    }
+  } else {
+    T rr[4], vv[4];
+    T al = (T)S.alpha;
+    as_ld4<T>(h, rr);
+    as_ld4<T>(h + 1 * L::AREG, vv);
+#pragma unroll
+    for(int a = 0; a < 4; a++) q[a] = dinv[mbyte(mw, a)] * (rr[a] - al * vv[a]);
+  }
+}
+
+/* The block's own 4 cells of a staged row: q, and the pass's pointwise
+ * work -- stores at global index gc, sums into red.  o is the cells' first
+ * own-array entry (pass A: x at o, rh at o + 8 rows; pass B: rh at o);
+ * raw0 / raw1 carry what the epilogue needs (pass A: rh; pass B: s, rh). */
+template <typename T, int PASS>
+__device__ __forceinline__ void as_own4(const uint8_t *h, unsigned mw,
+  const uint8_t *o, const T *dinv, const as_scal &S, long long gc,
+  const as_args<T> &A, T (&q)[4], T (&raw0)[4], T (&raw1)[4], double (&red)[5])
+{
+  typedef as_layout<T, PASS> L;
   if constexpr(PASS == 0) {
     T ss[4], rr[4], pn[4];
-    as_ld4<T>(st + L::HALO_OFF + 0 * 10 * L::ROWB + row * L::ROWB + ho, ss);
-    T al = (T)S.alpha, om = (T)S.omega, be = (T)S.beta, bo = (T)S.bo;
+    as_ld4<T>(h, ss);
     if(S.first) {
 #pragma unroll
       for(int a = 0; a < 4; a++) { rr[a] = ss[a]; pn[a] = rr[a]; }
     } else {
-      T tt[4], pp[4], vv[4];
-      as_ld4<T>(st + L::HALO_OFF + 1 * 10 * L::ROWB + row * L::ROWB + ho, tt);
-      as_ld4<T>(st + L::HALO_OFF + 2 * 10 * L::ROWB + row * L::ROWB + ho, pp);
-      as_ld4<T>(st + L::HALO_OFF + 3 * 10 * L::ROWB + row * L::ROWB + ho, vv);
+      T tt[4], pp[4], vv[4], xx[4];
+      T al = (T)S.alpha, om = (T)S.omega, be = (T)S.beta, bo = (T)S.bo;
+      as_ld4<T>(h + 1 * L::AREG, tt);
+      as_ld4<T>(h + 2 * L::AREG, pp);
+      as_ld4<T>(h + 3 * L::AREG, vv);
+      as_ld4<T>(o, xx);
 #pragma unroll
       for(int a = 0; a < 4; a++) {
         rr[a] = ss[a] - om * tt[a];
         pn[a] = rr[a] + be * pp[a] + bo * vv[a];
+        T di = dinv[mbyte(mw, a)];
+        xx[a] = xx[a] + al * (di * pp[a]) + om * (di * ss[a]);
       }
-      if(own) {
-        T xx[4];
-        as_ld4<T>(st + L::OWN_OFF + (row - 1) * L::OWNB + col * (int)sizeof(T), xx);
-#pragma unroll
-        for(int a = 0; a < 4; a++) {
-          T di = dinv[mbyte(mw, a)];
-          xx[a] = xx[a] + al * (di * pp[a]) + om * (di * ss[a]);
-          red[3] += (double)xx[a];
-        }
-        as_st4<T>(A.x + gc, xx);
-      }
+      as_sum4<T>(red[3], xx);
+      as_st4<T>(A.x + gc, xx);
     }
 #pragma unroll
     for(int a = 0; a < 4; a++) q[a] = dinv[mbyte(mw, a)] * pn[a];
-    if(own) {
-      as_ld4<T>(st + L::OWN_OFF + 8 * L::OWNB + (row - 1) * L::OWNB
-        + col * (int)sizeof(T), raw0);
-#pragma unroll
-      for(int a = 0; a < 4; a++) {
-        red[1] += (double)rr[a] * (double)rr[a];
-        red[2] += (double)raw0[a] * (double)rr[a];
-      }
-      as_st4<T>(A.w0 + gc, rr);
-      as_st4<T>(A.w1 + gc, pn);
-    } else {
-#pragma unroll
-      for(int a = 0; a < 4; a++) raw0[a] = (T)0.;
-    }
+    as_ld4<T>(o + 8 * L::OWNB, raw0);
+    as_dot4<T>(red[1], rr, rr);
+    as_dot4<T>(red[2], raw0, rr);
+    as_st4<T>(A.w0 + gc, rr);
+    as_st4<T>(A.w1 + gc, pn);
   } else {
     T rr[4], vv[4];
-    as_ld4<T>(st + L::HALO_OFF + 0 * 10 * L::ROWB + row * L::ROWB + ho, rr);
-    as_ld4<T>(st + L::HALO_OFF + 1 * 10 * L::ROWB + row * L::ROWB + ho, vv);
     T al = (T)S.alpha;
+    as_ld4<T>(h, rr);
+    as_ld4<T>(h + 1 * L::AREG, vv);
 #pragma unroll
     for(int a = 0; a < 4; a++) {
       raw0[a] = rr[a] - al * vv[a];
       q[a] = dinv[mbyte(mw, a)] * raw0[a];
     }
-    if(own) {
-      as_ld4<T>(st + L::OWN_OFF + (row - 1) * L::OWNB + col * (int)sizeof(T), raw1);
-#pragma unroll
-      for(int a = 0; a < 4; a++) red[2] += (double)raw0[a] * (double)raw0[a];
-      as_st4<T>(A.w0 + gc, raw0);
-    } else {
-#pragma unroll
-      for(int a = 0; a < 4; a++) raw1[a] = (T)0.;
-    }
+    as_ld4<T>(o, raw1);
+    as_dot4<T>(red[2], raw0, raw0);
+    as_st4<T>(A.w0 + gc, raw0);
   }
 }
 
-/* q at one x-halo cell: staged row `row`, byte offset `boff` inside the
- * halo-array row and `moff` inside the mask row */
+/* q at one x-halo cell: h its array-0 entry, arrays `stride` bytes apart,
+ * m its mask byte */
 template <typename T, int PASS>
-__device__ __forceinline__ T as_cell1(const uint8_t *st, int row, int boff,
-  int moff, const T *dinv, const as_scal &S)
+__device__ __forceinline__ T as_q1(const uint8_t *h, int stride, unsigned m,
+  const T *dinv, const as_scal &S)
 {
-  typedef as_layout<T, PASS> L;
-  unsigned m = st[L::MASK_OFF + row * L::MROWB + moff];
-  const uint8_t *h = st + L::HALO_OFF + row * L::ROWB + boff;
   if constexpr(PASS == 0) {
     T ss = *reinterpret_cast<const T *>(h);
     T pn;
     if(S.first) pn = ss;
     else {
-      T tt = *reinterpret_cast<const T *>(h + 1 * 10 * L::ROWB);
-      T pp = *reinterpret_cast<const T *>(h + 2 * 10 * L::ROWB);
-      T vv = *reinterpret_cast<const T *>(h + 3 * 10 * L::ROWB);
+      T tt = *reinterpret_cast<const T *>(h + 1 * stride);
+      T pp = *reinterpret_cast<const T *>(h + 2 * stride);
+      T vv = *reinterpret_cast<const T *>(h + 3 * stride);
       T rr = ss - (T)S.omega * tt;
       pn = rr + (T)S.beta * pp + (T)S.bo * vv;
     }
     return dinv[m] * pn;
   } else {
     T rr = *reinterpret_cast<const T *>(h);
-    T vv = *reinterpret_cast<const T *>(h + 1 * 10 * L::ROWB);
-    T ss = rr - (T)S.alpha * vv;
-    return dinv[m] * ss;
+    T vv = *reinterpret_cast<const T *>(h + stride);
+    return dinv[m] * (rr - (T)S.alpha * vv);
   }
 }
 
 /* One BiCGSTAB pass (PASS 0: pass A, 1: pass B) over this block's units,
  * 256 threads = 8 warps, warp w owning tile row w, lane l cells 4l..4l+3.
- * Per plane: wait for the stage, produce q (own cells, halo rows by warps
- * 0-1, halo columns by 16 threads of warp 2), one barrier, re-arm the
- * stage with the plane three ahead, then the stencil and epilogue of the
- * plane below. */
+ * Per plane: wait for the stage; each warp forms q of its row (with the
+ * pointwise work where the plane is the block's) and of its south / north
+ * rows and x-halo cells; releases the stage (the last warp to release it
+ * refills it with the plane three ahead); then the stencil and epilogue of
+ * the plane below, from registers. */
 template <typename T, int PASS>
-__global__ void __launch_bounds__(AS_THREADS) k_bicg_async(boxc B, opc O,
-  as_args<T> A)
+__global__ void __launch_bounds__(AS_THREADS, as_layout<T, PASS>::MINB)
+k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
 {
   typedef as_layout<T, PASS> L;
   bbb_kry *s = A.s;
   if(((volatile bbb_kry *)s)->done) return;
-  extern __shared__ __align__(128) uint8_t as_sm[];
-  T (*ring)[10][AS_W] = reinterpret_cast<T (*)[10][AS_W]>(as_sm + L::RING_OFF);
-  T *hwe = reinterpret_cast<T *>(as_sm + L::HWE_OFF);   /* [side][slot][row] */
-  optab<T> &tab = *reinterpret_cast<optab<T> *>(as_sm + L::TAB_OFF);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(as_sm + L::BAR_OFF);
-  double *sh = reinterpret_cast<double *>(as_sm + L::SH_OFF);
-  int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  extern __shared__ __align__(128) uint8_t as_dyn[];
+  /* aligned by an offset into the shared array (not by pointer masking),
+   * so every access below stays a shared-space access */
+  uint8_t *sm = as_dyn + ((128u - (as_saddr(as_dyn) & 127u)) & 127u);
+  optab<T> &tab = *reinterpret_cast<optab<T> *>(sm + L::TAB_OFF);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sm + L::BAR_OFF);
+  double *sh = reinterpret_cast<double *>(sm + L::SH_OFF);
+  const uint32_t sbase = as_saddr(sm);
+  const int tid = threadIdx.x, tx = tid & 31, w = tid >> 5;
+  uint32_t *rel = reinterpret_cast<uint32_t *>(sm + L::CNT_OFF);
   if(tid == 0) {
-    for(int b = 0; b < AS_NS; b++) as_bar_init(as_saddr(&bars[b]));
+    for(int b = 0; b < AS_NS; b++) { as_bar_init(as_saddr(&bars[b])); rel[b] = 0u; }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   optab_fill<T>(tab, O);                  /* ends with a barrier */
   as_scal S;
   S.alpha = s->alpha; S.omega = s->omega; S.beta = s->beta;
   S.bo = -S.beta * S.omega; S.first = s->first;
+  const T sg = O.helm ? (T)-1. : (T)1.;
+  const T wx = (T)O.wx * sg, wy = (T)O.wy * sg, wz = (T)O.wz * sg;
   double red[5] = {0., 0., 0., 0., 0.};
   int bad = 0;
   long long nload = 0;
-  long long bxl = blockIdx.x;
+  const long long bxl = blockIdx.x;
   long long u0 = bxl * B.q + (bxl < B.r ? bxl : B.r);
-  long long u1 = u0 + B.q + (bxl < B.r ? 1 : 0);
-  int gxl = 0, gxr = 0;
+  const long long u1 = u0 + B.q + (bxl < B.r ? 1 : 0);
+  const int col = tx * 4;
   while(u0 < u1) {
-    long long tile = u0 / B.nz;
-    int k0 = (int)(u0 - tile * B.nz);
-    long long left_ = u1 - u0;
-    int k1 = left_ < (long long)(B.nz - k0) ? k0 + (int)left_ : B.nz;
-    int i0 = (int)(tile % B.tiles_x) * AS_W, j0 = (int)(tile / B.tiles_x) * 8;
-    int j = j0 + ty;
-    bool valid = j < B.ny;
-    gxl = mapx(B, i0 - 1); gxr = mapx(B, i0 + AS_W);
-    int cnt = k1 - k0 + 2;
-    long long L0 = nload;
-    if(ty == 0)
+    const long long tile = u0 / B.nz;
+    const int k0 = (int)(u0 - tile * B.nz);
+    const long long left_ = u1 - u0;
+    const int k1 = left_ < (long long)(B.nz - k0) ? k0 + (int)left_ : B.nz;
+    const int i0 = (int)(tile % B.tiles_x) * AS_W, j0 = (int)(tile / B.tiles_x) * 8;
+    const int j = j0 + w;
+    const bool valid = j < B.ny;
+    const as_edges E = as_tile_edges(B, i0, j0);
+    const int cnt = k1 - k0 + 2;
+    const long long L0 = nload;
+    if(tid == 0)
       for(int a = 0; a < AS_NS && a < cnt; a++) {
         int b = (int)((L0 + a) % AS_NS);
-        as_issue<T, PASS>(B, A, as_sm + b * L::STAGE, as_saddr(&bars[b]), i0, j0,
-          mapz(B, k0 - 1 + a));
+        as_issue<T, PASS>(B, A, M, sbase + b * L::STAGE, as_saddr(&bars[b]), i0, j0,
+          mapz(B, k0 - 1 + a), E);
       }
-    T qm[4], qc[4], qn[4], r0c[4], r1c[4], r0n[4], r1n[4];
+    /* this warp's offsets inside a stage: own row (box row w + 1), south
+     * and north rows (box rows w, w + 2, or the wrap rows at the faces),
+     * x-halo cell (lane 0 west, lane 31 east) */
+    const int h_own = (w + 1) * L::ROWP + (L::CH + col) * L::ESZ;
+    const int m_own = L::MASK_OFF + (w + 1) * L::MROWP + 16 + col;
+    const int h_s = j == 0 ? L::EXT_OFF + col * L::ESZ
+                           : w * L::ROWP + (L::CH + col) * L::ESZ;
+    const int m_s = j == 0 ? L::MASK_OFF + L::MEXT_OFF + col
+                           : L::MASK_OFF + w * L::MROWP + 16 + col;
+    const int h_n = j + 1 == B.ny ? L::EXT_OFF + L::OWNB + col * L::ESZ
+                                  : (w + 2) * L::ROWP + (L::CH + col) * L::ESZ;
+    const int m_n = j + 1 == B.ny ? L::MASK_OFF + L::MEXT_OFF + 128 + col
+                                  : L::MASK_OFF + (w + 2) * L::MROWP + 16 + col;
+    int h_x, m_x, x_stride;
+    if(tx == 0) {
+      if(E.xl) {
+        h_x = L::XW_OFF + w * 16 + (B.wW % L::CH) * L::ESZ;
+        m_x = L::XW_OFF + L::NA * 256 + w * 16 + B.wW % 16;
+        x_stride = 256;
+      } else {
+        h_x = (w + 1) * L::ROWP + (L::CH - 1) * L::ESZ;
+        m_x = L::MASK_OFF + (w + 1) * L::MROWP + 15;
+        x_stride = L::AREG;
+      }
+    } else {
+      if(E.xr) {
+        h_x = L::XW_OFF + 128 + w * 16 + (B.wE % L::CH) * L::ESZ;
+        m_x = L::XW_OFF + L::NA * 256 + 128 + w * 16 + B.wE % 16;
+        x_stride = 256;
+      } else {
+        h_x = (w + 1) * L::ROWP + (L::CH + AS_W) * L::ESZ;
+        m_x = L::MASK_OFF + (w + 1) * L::MROWP + 16 + AS_W;
+        x_stride = L::AREG;
+      }
+    }
+    const int o_own = L::OWN_OFF + w * L::OWNB + col * L::ESZ;
+    T qm[4], qc[4], qn[4], qSc[4], qNc[4], qSn[4], qNn[4];
+    T r0c[4], r1c[4], r0n[4], r1n[4];
+    T xqc = (T)0., xqn = (T)0.;
     unsigned mc = 0, mn = 0;
 #pragma unroll
     for(int v = 0; v < 4; v++) {
-      qm[v] = qc[v] = qn[v] = (T)0.;
+      qm[v] = qc[v] = qn[v] = qSc[v] = qNc[v] = qSn[v] = qNn[v] = (T)0.;
       r0c[v] = r1c[v] = r0n[v] = r1n[v] = (T)0.;
     }
     for(int a = 0; a < cnt; a++) {
-      int pl = k0 - 1 + a;
-      long long Ld = L0 + a;
-      int buf = (int)(Ld % AS_NS);
-      uint32_t par = (uint32_t)((Ld / AS_NS) & 1);
-      uint8_t *st = as_sm + buf * L::STAGE;
+      const int pl = k0 - 1 + a;
+      const long long Ld = L0 + a;
+      const int buf = (int)(Ld % AS_NS);
+      const uint32_t par = (uint32_t)((Ld / AS_NS) & 1);
+      const uint8_t *st = sm + buf * L::STAGE;
       if(!as_wait(as_saddr(&bars[buf]), par)) bad = 1;
-      bool full = pl >= k0 && pl < k1;
-      bool own = valid && full;
-      long long gc = own ? lin(B, i0 + tx * 4, j, pl) : 0;
-      as_cell4<T, PASS>(st, ty + 1, tx * 4, tab.dinv, S, own, gc, A, qn, r0n,
-        r1n, mn, red);
-      if(full) {
-        int slot = (pl - k0) % 3;
-        as_st4<T>(&ring[slot][ty + 1][tx * 4], qn);
-        if(tid < 64) {
-          int hr = tid < 32 ? 0 : 9;
-          T hq[4], d0[4], d1[4];
-          unsigned hm;
-          as_cell4<T, PASS>(st, hr, (tid & 31) * 4, tab.dinv, S, false, 0, A,
-            hq, d0, d1, hm, red);
-          as_st4<T>(&ring[slot][hr][(tid & 31) * 4], hq);
-        } else if(tid < 80) {
-          int side = tid < 72 ? 0 : 1, r = 1 + ((tid - 64) & 7);
-          int boff, moff;
-          if(side == 0) {
-            boff = (gxl - gxl / L::CH * L::CH) * (int)sizeof(T);
-            moff = gxl - gxl / 16 * 16;
-          } else {
-            boff = (L::CH + AS_W + (gxr - gxr / L::CH * L::CH)) * (int)sizeof(T);
-            moff = 144 + (gxr - gxr / 16 * 16);
-          }
-          hwe[(side * 3 + slot) * 8 + (r - 1)] =
-            as_cell1<T, PASS>(st, r, boff, moff, tab.dinv, S);
+      const bool full = pl >= k0 && pl < k1;
+      if(valid) {
+        mn = *reinterpret_cast<const unsigned *>(st + m_own);
+        if(full) {
+          as_own4<T, PASS>(st + h_own, mn, st + o_own, tab.dinv, S,
+            lin(B, i0 + col, j, pl), A, qn, r0n, r1n, red);
+          as_q4<T, PASS>(st + h_s, *reinterpret_cast<const unsigned *>(st + m_s),
+            tab.dinv, S, qSn);
+          as_q4<T, PASS>(st + h_n, *reinterpret_cast<const unsigned *>(st + m_n),
+            tab.dinv, S, qNn);
+          if(tx == 0 || tx == 31)
+            xqn = as_q1<T, PASS>(st + h_x, x_stride, st[m_x], tab.dinv, S);
+        } else {
+          as_q4<T, PASS>(st + h_own, mn, tab.dinv, S, qn);
         }
       }
-      as_fence_proxy();
-      __syncthreads();
-      if(a + AS_NS < cnt && ty == 0)
-        as_issue<T, PASS>(B, A, st, as_saddr(&bars[buf]), i0, j0,
-          mapz(B, pl + AS_NS));
-      if(a >= 2) {
-        int k = pl - 1, sl = (k - k0) % 3;
+      /* release the stage: the last of the 8 warps to finish reading it
+       * refills it with the plane three ahead (no block-wide barrier, so
+       * warps drift apart by up to the stage depth) */
+      __syncwarp();
+      if(tx == 0) {
+        uint32_t old = as_release(as_saddr(&rel[buf]));
+        if(old % 8u == 7u && a + AS_NS < cnt)
+          as_issue<T, PASS>(B, A, M, sbase + buf * L::STAGE, as_saddr(&bars[buf]),
+            i0, j0, mapz(B, pl + AS_NS), E);
+      }
+      if(a >= 2 && valid) {
+        const int k = pl - 1;
         T lft = __shfl_up_sync(0xffffffffu, qc[3], 1);
         T rgt = __shfl_down_sync(0xffffffffu, qc[0], 1);
-        if(tx == 0) lft = hwe[(0 * 3 + sl) * 8 + ty];
-        if(tx == 31) rgt = hwe[(1 * 3 + sl) * 8 + ty];
-        if(valid) {
-          T Sv[4], Nv[4], Aq[4];
-          as_ld4<T>(reinterpret_cast<const uint8_t *>(&ring[sl][ty][tx * 4]), Sv);
-          as_ld4<T>(reinterpret_cast<const uint8_t *>(&ring[sl][ty + 2][tx * 4]), Nv);
+        if(tx == 0) lft = xqc;
+        if(tx == 31) rgt = xqc;
+        T Aq[4];
 #pragma unroll
-          for(int v = 0; v < 4; v++) {
-            unsigned mv = mbyte(mc, v);
-            T qW = v > 0 ? qc[v - 1] : lft;
-            T qE = v < 3 ? qc[v + 1] : rgt;
-            Aq[v] = op_apply<T>(mv, O, tab.diag[mv], qm[v], Sv[v], qW, qc[v], qE,
-              Nv[v], qn[v]);
-          }
-          long long ge = lin(B, i0 + tx * 4, j, k);
-          if constexpr(PASS == 0) {
-            as_st4<T>(A.w2 + ge, Aq);
-#pragma unroll
-            for(int v = 0; v < 4; v++) red[0] += (double)r0c[v] * (double)Aq[v];
-          } else {
-            as_st4<T>(A.w1 + ge, Aq);
-#pragma unroll
-            for(int v = 0; v < 4; v++) {
-              red[0] += (double)Aq[v] * (double)r0c[v];
-              red[1] += (double)Aq[v] * (double)Aq[v];
-              red[3] += (double)r1c[v] * (double)r0c[v];
-              red[4] += (double)r1c[v] * (double)Aq[v];
-            }
-          }
+        for(int v = 0; v < 4; v++) {
+          unsigned mv = mbyte(mc, v);
+          T qW = v > 0 ? qc[v - 1] : lft;
+          T qE = v < 3 ? qc[v + 1] : rgt;
+          Aq[v] = as_apply<T>(mv, tab.diag[mv], wx, wy, wz, qm[v], qSc[v], qW,
+            qc[v], qE, qNc[v], qn[v]);
+        }
+        const long long ge = lin(B, i0 + col, j, k);
+        if constexpr(PASS == 0) {
+          as_st4<T>(A.w2 + ge, Aq);
+          as_dot4<T>(red[0], r0c, Aq);
+        } else {
+          as_st4<T>(A.w1 + ge, Aq);
+          as_dot4<T>(red[0], Aq, r0c);
+          as_dot4<T>(red[1], Aq, Aq);
+          as_dot4<T>(red[3], r1c, r0c);
+          as_dot4<T>(red[4], r1c, Aq);
         }
       }
 #pragma unroll
       for(int v = 0; v < 4; v++) {
-        qm[v] = qc[v]; qc[v] = qn[v]; r0c[v] = r0n[v]; r1c[v] = r1n[v];
+        qm[v] = qc[v]; qc[v] = qn[v]; qSc[v] = qSn[v]; qNc[v] = qNn[v];
+        r0c[v] = r0n[v]; r1c[v] = r1n[v];
       }
+      xqc = xqn;
       mc = mn;
     }
     nload = L0 + cnt;
@@ -454,10 +581,11 @@ __global__ void __launch_bounds__(AS_THREADS) k_bicg_async(boxc B, opc O,
   if(__syncthreads_or(bad)) {
     /* a stage never completed: let whatever is still landing finish
      * before the block's shared memory is released */
-    for(int b = 0; b < AS_NS; b++) {
-      long long last = nload - 1 - ((nload - 1 - b) % AS_NS + AS_NS) % AS_NS;
-      if(last >= 0) as_wait(as_saddr(&bars[b]), (uint32_t)((last / AS_NS) & 1));
-    }
+    if(nload > 0)
+      for(int b = 0; b < AS_NS; b++) {
+        long long last = nload - 1 - ((nload - 1 - b) % AS_NS + AS_NS) % AS_NS;
+        if(last >= 0) as_wait(as_saddr(&bars[b]), (uint32_t)((last / AS_NS) & 1));
+      }
     if(tid == 0) atomicOr(&s->pad, 1);
   }
   /* the pass's reductions and scalar updates, as k_bicgA / k_bicgB */

@@ -459,11 +459,25 @@ static void dia_spmv(const dia13 *A, const real *x, real *y)
   }
 }
 
+/* Dot product with a summation order fixed by n alone (chunks of VCHUNK
+ * summed in index order), so the oracle's iterates do not depend on the
+ * host's thread count. */
+#define VCHUNK 4096
 static real vdot(long n, const real *a, const real *b)
 {
+  long nc = (n + VCHUNK - 1) / VCHUNK;
+  real part_stack[64];
+  real *part = nc <= 64 ? part_stack : (real *)malloc(sizeof(real) * (size_t)nc);
+  #pragma omp parallel for schedule(static)
+  for(long c = 0; c < nc; c++) {
+    long i1 = (c + 1) * VCHUNK < n ? (c + 1) * VCHUNK : n;
+    real s = 0.;
+    for(long i = c * VCHUNK; i < i1; i++) s += a[i] * b[i];
+    part[c] = s;
+  }
   real s = 0.;
-  #pragma omp parallel for reduction(+:s) schedule(static)
-  for(long i = 0; i < n; i++) s += a[i] * b[i];
+  for(long c = 0; c < nc; c++) s += part[c];
+  if(part != part_stack) free(part);
   return s;
 }
 static real vnrm2(long n, const real *a) { return sqrt(vdot(n, a, a)); }
