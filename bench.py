@@ -298,7 +298,7 @@ def main():
         a_ms, a_n, a_bytes = mixed["pass0"]
         achieved = a_bytes / (a_ms / 1000.0) / 1e9 if a_ms > 0 else None
         passes = {}
-        for k, nm in ((0, "k_bicgA<float,4>"), (1, "k_bicgB<float,4>")):
+        for k, nm in ((0, "k_bicg_async<float,0>"), (1, "k_bicg_async<float,1>")):
             pms, pn, pby = mixed["pass%d" % k]
             passes[nm] = {"launches": pn, "ms_per_launch": pms / pn if pn else None,
                           "GB_s": pby / (pms / 1000.0) / 1e9 if pms > 0 else None}
@@ -336,7 +336,8 @@ def main():
                              "unit": "GB/s",
                              "frac": achieved / peak if achieved else None,
                              "traffic": traffic,
-                             "kernel": "k_bicgA<float,4> (BiCGSTAB pass A, FP32): "
+                             "kernel": "k_bicg_async<float,0> (BiCGSTAB pass A, "
+                             "FP32, inputs staged by tensor-map copies): "
                              "algorithmic 10 words + 1 mask byte per unknown",
                              "peak_kind": peak_kind,
                              "passes": passes,
