@@ -88,7 +88,8 @@ class Options(C.Structure):
                 ("precision", C.c_int), ("inner_tol", C.c_double),
                 ("max_outer", C.c_int), ("learned_guess", C.c_int),
                 ("record", C.c_int), ("gravity_balance", C.c_int),
-                ("lamb_max_iter_override", C.c_int), ("verbose", C.c_int)]
+                ("lamb_max_iter_override", C.c_int), ("verbose", C.c_int),
+                ("reliable", C.c_int)]
 
 
 class Stats(C.Structure):

@@ -74,6 +74,7 @@ void bbb_default_options(bbb_options *opt)
   opt->gravity_balance = 0;
   opt->lamb_max_iter_override = 0;
   opt->verbose = 0;
+  opt->reliable = 0;
 }
 
 static void opt_init(void)

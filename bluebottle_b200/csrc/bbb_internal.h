@@ -53,7 +53,14 @@ struct bbb_kry {
   double bnorm, rnorm;             /* ||b||, latest residual norm         */
   double sumx;                     /* sum of the solution (mean removal)  */
   double t_s, t_t, s_s;            /* (t,s), (t,t), (s,s) of the last K2  */
+  double rhv;                      /* (rh, v) of the last BiCGSTAB pass A */
+  double rstart;                   /* ||r|| at a residual replacement; a
+                                      resumed solve whose ||r|| grows 1e3-
+                                      fold past it stops (status -1)      */
   int iter, maxit, done, converged, s_conv, status, first, pad;
+  int keep;                        /* 1: no early exit on ||s|| (the inner
+                                      solve resumes after its last pass A) */
+  int keep_pad;
   unsigned int ticket;             /* last-block election counter         */
 };
 

@@ -602,6 +602,7 @@ __global__ void __launch_bounds__(NTHR) k_bicg_setup(boxc B, opc O,
       s->maxit = maxit;
       s->first = 1;
       s->pad = 0;
+      s->keep = 0;
       s->s_conv = 0;
       s->alpha = s->omega = s->beta = 0.;
       s->converged = (rn <= s->tol);
@@ -710,11 +711,13 @@ __global__ void __launch_bounds__(NTHR, BBB_KRY_MINB) k_bicgA(boxc B, opc O,
       double rn = sconv ? s->rnorm : sqrt(red[1]);
       s->rnorm = rn;
       s->rho = red[2];
+      s->rhv = red[0];
       s->alpha = red[2] / red[0];
       s->first = 0;
       s->converged = sconv || (rn <= s->tol);
       if(!isfinite(rn)) { s->status = BBB_ERR_NONFINITE; s->done = 1; }
       if(s->converged || s->iter >= s->maxit) s->done = 1;
+      if(s->keep && !(rn <= 1e3 * s->rstart)) { s->status = -1; s->done = 1; }
     }
   }
 }
@@ -786,7 +789,7 @@ __global__ void __launch_bounds__(NTHR, BBB_KRY_MINB) k_bicgB(boxc B, opc O,
       s->t_t = red[1];
       s->s_s = red[2];
       double sn = sqrt(red[2]);
-      int sconv = (sn <= s->tol);
+      int sconv = (sn <= s->tol) && (!s->keep || sn == 0.);
       s->s_conv = sconv;
       if(sconv) {
         s->rnorm = sn;
@@ -861,53 +864,49 @@ __global__ void k_pp_writeback(const double *x, real *ph, bbb_geom G,
  * every BiCGSTAB iteration (slot 0: pass A, slot 1: pass B); after a solve
  * only the passes the device really executed are summed, each with its
  * algorithmic bytes (compulsory reads and writes of the owned cells). */
-#define BBB_PROF_IT 8192
-#define BBB_PROF_SLOTS 2
+#define BBB_PROF_MAX 16384
 static struct {
   int on, n;
-  cudaEvent_t ev[(BBB_PROF_SLOTS + 1) * BBB_PROF_IT];
-  double bytes[BBB_PROF_SLOTS * BBB_PROF_IT];
-  double ms[BBB_PROF_SLOTS], kbytes[BBB_PROF_SLOTS];
-  long long launches[BBB_PROF_SLOTS];
+  cudaEvent_t ev[2 * BBB_PROF_MAX];     /* start / end event of each launch */
+  int slot[BBB_PROF_MAX];               /* 0 pass A, 1 pass B              */
+  double bytes[BBB_PROF_MAX];
+  double ms[2], kbytes[2];
+  long long launches[2];
   long long iters;
 } g_prof;
 
-/* event e of the current iteration (0 before pass A, 1 after A, 2 after B) */
-static void prof_event(int e)
+/* before a pass launch: its slot and algorithmic bytes, start event */
+static void prof_begin(int slot, double b)
 {
-  if(!g_prof.on || g_prof.n >= BBB_PROF_IT) return;
-  int i = g_prof.n * (BBB_PROF_SLOTS + 1) + e;
-  if(!g_prof.ev[i]) cudaEventCreate(&g_prof.ev[i]);
-  cudaEventRecord(g_prof.ev[i], g_dev.stream);
+  if(!g_prof.on || g_prof.n >= BBB_PROF_MAX) return;
+  int i = g_prof.n;
+  if(!g_prof.ev[2 * i]) cudaEventCreate(&g_prof.ev[2 * i]);
+  if(!g_prof.ev[2 * i + 1]) cudaEventCreate(&g_prof.ev[2 * i + 1]);
+  g_prof.slot[i] = slot;
+  g_prof.bytes[i] = b;
+  cudaEventRecord(g_prof.ev[2 * i], g_dev.stream);
 }
 
-static void prof_bytes(int slot, double b)
+/* after the launch: end event */
+static void prof_end(void)
 {
-  if(!g_prof.on || g_prof.n >= BBB_PROF_IT) return;
-  g_prof.bytes[g_prof.n * BBB_PROF_SLOTS + slot] = b;
-}
-
-static void prof_next(void)
-{
-  if(!g_prof.on || g_prof.n >= BBB_PROF_IT) return;
+  if(!g_prof.on || g_prof.n >= BBB_PROF_MAX) return;
+  cudaEventRecord(g_prof.ev[2 * g_prof.n + 1], g_dev.stream);
   g_prof.n++;
 }
 
-/* the stream has been synchronised: `npass` passes really ran, counted in
- * launch order (A, B, A, B, ...) */
+/* the stream has been synchronised: the first `npass` recorded launches
+ * really ran (later ones returned at once) */
 static void prof_collect(long long npass)
 {
   if(!g_prof.on) return;
-  long long cnt = 0;
-  for(int i = 0; i < g_prof.n && cnt < npass; i++) {
-    for(int sl = 0; sl < BBB_PROF_SLOTS && cnt < npass; sl++, cnt++) {
-      float t = 0.f;
-      int e = i * (BBB_PROF_SLOTS + 1) + sl;
-      if(cudaEventElapsedTime(&t, g_prof.ev[e], g_prof.ev[e + 1]) == cudaSuccess) {
-        g_prof.ms[sl] += t;
-        g_prof.kbytes[sl] += g_prof.bytes[i * BBB_PROF_SLOTS + sl];
-        g_prof.launches[sl]++;
-      }
+  for(int i = 0; i < g_prof.n && i < npass; i++) {
+    float t = 0.f;
+    if(cudaEventElapsedTime(&t, g_prof.ev[2 * i], g_prof.ev[2 * i + 1]) == cudaSuccess) {
+      int sl = g_prof.slot[i];
+      g_prof.ms[sl] += t;
+      g_prof.kbytes[sl] += g_prof.bytes[i];
+      g_prof.launches[sl]++;
     }
   }
   g_prof.iters += npass / 2;
@@ -917,7 +916,7 @@ static void prof_collect(long long npass)
 extern "C" void bbb_profile_enable(int on) { g_prof.on = on; g_prof.n = 0; }
 extern "C" void bbb_profile_reset(void)
 {
-  for(int a = 0; a < BBB_PROF_SLOTS; a++) {
+  for(int a = 0; a < 2; a++) {
     g_prof.ms[a] = 0.; g_prof.kbytes[a] = 0.; g_prof.launches[a] = 0;
   }
   g_prof.iters = 0; g_prof.n = 0;
@@ -925,13 +924,13 @@ extern "C" void bbb_profile_reset(void)
 extern "C" void bbb_profile_get(double *ms, long long *iters, double *bytes)
 {
   *ms = 0.; *bytes = 0.;
-  for(int a = 0; a < BBB_PROF_SLOTS; a++) { *ms += g_prof.ms[a]; *bytes += g_prof.kbytes[a]; }
+  for(int a = 0; a < 2; a++) { *ms += g_prof.ms[a]; *bytes += g_prof.kbytes[a]; }
   *iters = g_prof.iters;
 }
 extern "C" void bbb_profile_get_pass(int pass, double *ms, long long *launches,
   double *bytes)
 {
-  if(pass < 0 || pass >= BBB_PROF_SLOTS) { *ms = 0.; *launches = 0; *bytes = 0.; return; }
+  if(pass < 0 || pass >= 2) { *ms = 0.; *launches = 0; *bytes = 0.; return; }
   *ms = g_prof.ms[pass]; *launches = g_prof.launches[pass]; *bytes = g_prof.kbytes[pass];
 }
 
@@ -1083,36 +1082,44 @@ static bool as_pass_maps(as_maps *M, const boxc &B, const uint8_t *mask,
 #define BBB_ASYNC_ON 0
 #endif
 
-/* BiCGSTAB iterations after the set-up kernel (s = r0, rh, scalars) */
+/* BiCGSTAB iterations after a set-up kernel.  Fresh (`resume` false): the
+ * set-up left s = r0 = rh and first = 1; launches go A, B, A, B, ...
+ * Resumed after a residual replacement: r holds the replaced residual,
+ * alpha its (rh, r) / (rh, v), p and v the directions in buffers *curp;
+ * launches go B, A, B, A, ...  Either way a run ends after a pass A.
+ * *curp (when given) returns the buffer index of the latest p, v. */
 template <typename T, int V>
 static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
   const uint8_t *mask, T *r, T *rh, T *p0, T *p1, T *v0, T *v1, T *sv, T *tv,
-  T *x, bbb_kry *s, int maxit, int batch0)
+  T *x, bbb_kry *s, int maxit, int batch0, int *curp = NULL, bool resume = false)
 {
   dim3 grd = box_grid(B), blk(TX, TY);
   T *pp[2] = {p0, p1}, *vv[2] = {v0, v1};
-  int cur = 0, launched = 0;
+  const int cur0 = curp ? *curp : 0;
+  int cur = cur0, launched = 0;
   double w = sizeof(T);
   bool staged = BBB_ASYNC_ON && B.nx % AS_W == 0 && as_per_sm<T, 0>() > 0
     && as_per_sm<T, 1>() > 0;
   boxc BA = B, BB = B;
-  as_maps MA[2], MB[2];            /* pass A / B maps for cur = 0, 1 */
+  as_maps MA[2], MB[2];   /* pass A maps reading p, v of buffer c; pass B
+                             maps reading v of buffer c */
   if(staged) {
     BA = retile(B, as_per_sm<T, 0>(), as_layout<T, 0>::ALIGN);
     BB = retile(B, as_per_sm<T, 1>(), as_layout<T, 1>::ALIGN);
     for(int c = 0; c < 2 && staged; c++) {
       const T *ha[4] = {sv, tv, pp[c], vv[c]}, *oa[2] = {x, rh};
-      const T *hb[4] = {r, vv[c ^ 1], NULL, NULL}, *ob[2] = {rh, NULL};
+      const T *hb[4] = {r, vv[c], NULL, NULL}, *ob[2] = {rh, NULL};
       staged = as_pass_maps<T, 0>(&MA[c], BA, mask, ha, oa)
             && as_pass_maps<T, 1>(&MB[c], BB, mask, hb, ob);
     }
   }
-  drive(s, [&]() {
-    /* pass A: first reads s, rh; later s, t, p, v, x, rh; + mask */
-    double a_bytes = launched == 0 ? (double)n * (5. * w + 1.)
-                                   : (double)n * (10. * w + 1.);
-    prof_event(0);
-    prof_bytes(0, a_bytes);
+  /* pass A: reads p, v of buffer cur, writes buffer cur ^ 1, then cur flips */
+  auto pass_a = [&]() {
+    /* the opening pass of a fresh solve reads s, rh; later ones s, t, p, v,
+     * x, rh; + mask */
+    double a_bytes = (launched == 0 && !resume) ? (double)n * (5. * w + 1.)
+                                                : (double)n * (10. * w + 1.);
+    prof_begin(0, a_bytes);
     if(staged) {
       as_args<T> A;
       A.mask = mask;
@@ -1126,32 +1133,46 @@ static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
         vv[cur], rh, r, pp[cur ^ 1], vv[cur ^ 1], x, s, g_dev.partials);
     }
     BBB_LAUNCHED();
-    prof_event(1);
-    prof_bytes(1, (double)n * (5. * w + 1.));
+    prof_end();
+    cur ^= 1;
+    launched++;
+  };
+  /* pass B: reads r and the latest v (buffer cur) */
+  auto pass_b = [&]() {
+    prof_begin(1, (double)n * (5. * w + 1.));
     if(staged) {
       as_args<T> A;
       A.mask = mask;
-      A.h[0] = r; A.h[1] = vv[cur ^ 1]; A.h[2] = NULL; A.h[3] = NULL;
+      A.h[0] = r; A.h[1] = vv[cur]; A.h[2] = NULL; A.h[3] = NULL;
       A.w0 = sv; A.w1 = tv; A.w2 = NULL; A.x = NULL;
       A.s = s; A.partials = g_dev.partials;
       k_bicg_async<T, 1><<<BB.nblk, AS_THREADS, as_layout<T, 1>::SMEM,
         g_dev.stream>>>(BB, O, A, MB[cur]);
     } else {
-      k_bicgB<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, r, vv[cur ^ 1],
+      k_bicgB<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, r, vv[cur],
         rh, sv, tv, s, g_dev.partials);
     }
     BBB_LAUNCHED();
-    prof_event(2);
-    prof_next();
-    cur ^= 1;
-    launched++;
-  }, maxit, batch0);
-  /* passes executed: the opening pass A, B and A of each counted
-   * iteration, and B and A of an uncounted one that ended on ||s|| (a
-   * solve that converged at set-up ran none) */
+    prof_end();
+  };
+  if(resume) drive(s, [&]() { pass_b(); pass_a(); }, maxit, batch0);
+  else drive(s, [&]() { pass_a(); pass_b(); }, maxit, batch0);
+  /* passes executed -- fresh: the opening pass A, B and A of each counted
+   * iteration, B and A of an uncounted one that ended on ||s|| (a solve
+   * that converged at set-up ran none); resumed: B and A of each counted
+   * iteration and of an uncounted last one */
   bbb_kry *h = g_dev.kry_host;
-  long long npass = h->first ? 0 : 2LL * h->iter + 1 + (h->s_conv ? 2 : 0);
+  long long npass;
+  if(resume) npass = 2LL * h->iter + (h->s_conv ? 2 : 0);
+  else npass = h->first ? 0 : 2LL * h->iter + 1 + (h->s_conv ? 2 : 0);
   prof_collect(npass);
+  /* launches after convergence return at once but still flip `cur`: the
+   * latest p, v are where the passes A that really ran left them */
+  if(curp) {
+    long long na = resume ? h->iter + (h->s_conv ? 1 : 0)
+                          : (h->first ? 0 : 1 + h->iter + (h->s_conv ? 1 : 0));
+    *curp = cur0 ^ (int)(na & 1);
+  }
 }
 
 static opc poisson_op(const bbb_geom &G)
@@ -1280,6 +1301,10 @@ __global__ void __launch_bounds__(NTHR) k_outer_resid(boxc B, opc O,
       si->tol = fmax(inner_tol, need) * rn;
       si->maxit = inner_maxit;
       si->done = s->done;
+      if(s->done) {
+        /* no inner sweep follows: it reports no iterations or passes */
+        si->iter = 0; si->first = 1; si->s_conv = 0;
+      }
     }
   }
 }
@@ -1319,11 +1344,68 @@ __global__ void __launch_bounds__(256) k_inner_setup(long long n,
       si->iter = 0;
       si->first = 1;
       si->pad = 0;
+      si->keep = 1;
+      si->rstart = INFINITY;
       si->s_conv = 0;
       si->alpha = si->omega = si->beta = 0.;
       si->converged = (rn <= si->tol);
       si->done = si->converged || si->maxit <= 0 || !isfinite(rn);
       si->status = isfinite(rn) ? 0 : BBB_ERR_NONFINITE;
+    }
+  }
+}
+
+/* Residual replacement inside a running inner solve (reliable update):
+ * r = rf - mean (rf the FP64 residual b - A x of the accumulated solution,
+ * rounded to FP32), e = 0; the Krylov state p, v, rh stays.  rho = (rh, r)
+ * and alpha = rho / (rh, v) restart the recurrences from the true residual
+ * -- the group-wise residual replacement of Sleijpen and van der Vorst
+ * ("Reliable updated residuals in hybrid Bi-CG methods", Computing 56,
+ * 1996), which keeps the FP32 recursion's residual gap below what the
+ * FP64 stopping test needs without discarding the Krylov space. */
+template <int V>
+__global__ void __launch_bounds__(256) k_reliable_setup(long long n,
+  const float *__restrict__ rf, const float *__restrict__ rh, float *r, float *e,
+  bbb_kry *si, double *partials)
+{
+  if(((volatile bbb_kry *)si)->done) return;
+  __shared__ double sh[32 * 2];
+  float mean = (float)si->sumx;
+  double red[2] = {0., 0.};
+  long long nv = n / V;
+  for(long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nv;
+      q += (long long)gridDim.x * blockDim.x) {
+    long long c = q * V;
+    float rv[V], hv[V], z[V];
+    ldv<float, V>(rf, c, rv);
+    ldv<float, V>(rh, c, hv);
+#pragma unroll
+    for(int a = 0; a < V; a++) {
+      rv[a] = rv[a] - mean;
+      z[a] = 0.f;
+      red[0] += (double)rv[a] * (double)rv[a];
+      red[1] += (double)hv[a] * (double)rv[a];
+    }
+    stv<float, V>(r, c, rv);
+    stv<float, V>(e, c, z);
+  }
+  if(bbb_grid_partial<2>(red, partials, &si->ticket, sh)) {
+    bbb_grid_finish_sum<2>(red, partials, &si->ticket, sh);
+    if(threadIdx.x == 0) {
+      double rn = sqrt(red[0]);
+      si->rnorm = rn;
+      si->rho = red[1];
+      si->alpha = red[1] / si->rhv;
+      si->iter = 0;
+      si->first = 0;
+      si->pad = 0;
+      si->keep = 1;
+      si->rstart = rn;
+      si->s_conv = 0;
+      si->converged = (rn <= si->tol);
+      si->done = si->converged || si->maxit <= 0 || !isfinite(rn)
+        || !isfinite(si->alpha);
+      si->status = isfinite(rn) && isfinite(si->alpha) ? 0 : BBB_ERR_NONFINITE;
     }
   }
 }
@@ -1380,31 +1462,65 @@ static int poisson_mixed(const boxc &BD, const boxc &BF, const opc &O,
   BBB_CK(cudaStreamSynchronize(g_dev.stream));
   init.bnorm = g_dev.kry_host->bnorm;
   init.tol = pp_residual * init.bnorm;
-  init.maxit = g_opt.max_outer > 0 ? g_opt.max_outer : 20;
+  init.maxit = g_opt.max_outer > 0 ? g_opt.max_outer : 40;
   BBB_CK(cudaMemcpyAsync(s, &init, sizeof(bbb_kry), cudaMemcpyHostToDevice,
     g_dev.stream));
   int project = (nparts == 0) && (bc.pW == bc.pE) && (bc.pS == bc.pN)
     && (bc.pB == bc.pT);
   double itol = g_opt.inner_tol > 0 ? g_opt.inner_tol : 1e-4;
-  int inner_total = 0;
+  int inner_total = 0, cur = 0, fresh = 1, resume_failed = 0;
   for(int outer = 0; outer <= init.maxit; outer++) {
     k_outer_resid<VD><<<grdD, blk, 0, g_dev.stream>>>(BD, O, g_dev.mask_p,
       g_dev.kb, g_dev.kx, g_dev.fb, s, si, g_dev.partials, itol, pp_max_iter,
       project, n);
     BBB_LAUNCHED();
-    k_inner_setup<VF><<<NPW, 256, 0, g_dev.stream>>>(n, g_dev.fb, g_dev.fs,
-      g_dev.fx, g_dev.frh, si, g_dev.partials);
+    /* a sweep starts the FP32 BiCGSTAB from e = 0; with reliable updates
+     * later sweeps replace its residual by the FP64 one and carry on
+     * (restarting only after an inner breakdown).  On the 256x256x512
+     * sedimentation box both take about the FP64 form's iteration count
+     * (restarts at 1e-4: ~500 per step; reliable at 1e-2: ~480 with twice
+     * the sweeps), so restarting is the default. */
+    if(fresh) {
+      k_inner_setup<VF><<<NPW, 256, 0, g_dev.stream>>>(n, g_dev.fb, g_dev.fs,
+        g_dev.fx, g_dev.frh, si, g_dev.partials);
+      cur = 0;
+    } else {
+      k_reliable_setup<VF><<<NPW, 256, 0, g_dev.stream>>>(n, g_dev.fb, g_dev.frh,
+        g_dev.fr, g_dev.fx, si, g_dev.partials);
+    }
     BBB_LAUNCHED();
     bicgstab_iterations<float, VF>(BF, O, n, g_dev.mask_p, g_dev.fr, g_dev.frh,
       g_dev.fp[0], g_dev.fp[1], g_dev.fv[0], g_dev.fv[1], g_dev.fs, g_dev.ft,
-      g_dev.fx, si, pp_max_iter, 4);
+      g_dev.fx, si, pp_max_iter, 4, &cur, !fresh);
     if(bbb_last_status() == BBB_ERR_CUDA) return -1;
     inner_total += g_dev.kry_host->iter;
+    if(g_opt.verbose)
+      fprintf(stderr, "poisson mixed sweep %d (%s): %d inner iterations, "
+        "converged %d, s_conv %d, status %d, ||r_inner|| %.3e (tol %.3e)\n",
+        outer, fresh ? "fresh" : "resumed", g_dev.kry_host->iter,
+        g_dev.kry_host->converged, g_dev.kry_host->s_conv,
+        g_dev.kry_host->status, g_dev.kry_host->rnorm, g_dev.kry_host->tol);
+    /* a breakdown (non-finite scalar, or a resumed sweep whose residual
+     * grew 1e3-fold: the shadow residual no longer correlates with the
+     * replaced one) or a sweep that ran out of iterations: the next sweep
+     * restarts from the FP64 residual, and after a failed resumption the
+     * rest of this solve restarts every sweep */
+    int broke = g_dev.kry_host->status != 0;
+    if(broke) {
+      /* the FP64 solution is untouched by a failed sweep's e */
+      cudaMemsetAsync(g_dev.fx, 0, sizeof(float) * (size_t)n, g_dev.stream);
+      if(!fresh) resume_failed = 1;
+    }
+    fresh = !g_opt.reliable || broke || resume_failed
+      || !g_dev.kry_host->converged || g_dev.kry_host->s_conv;
     k_accumulate<VF><<<NPW, 256, 0, g_dev.stream>>>(n, g_dev.kx, g_dev.fx, s);
     BBB_LAUNCHED();
     BBB_CK(cudaMemcpyAsync(g_dev.kry_host, s, sizeof(bbb_kry),
       cudaMemcpyDeviceToHost, g_dev.stream));
     BBB_CK(cudaStreamSynchronize(g_dev.stream));
+    if(g_opt.verbose)
+      fprintf(stderr, "poisson mixed sweep %d: FP64 ||r|| %.3e (tol %.3e)\n",
+        outer, g_dev.kry_host->rnorm, g_dev.kry_host->tol);
     if(g_dev.kry_host->done) break;
   }
   bbb_kry *h = g_dev.kry_host;

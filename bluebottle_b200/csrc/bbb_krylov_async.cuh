@@ -602,11 +602,13 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
         double rn = sconv ? s->rnorm : sqrt(r4[1]);
         s->rnorm = rn;
         s->rho = r4[2];
+        s->rhv = r4[0];
         s->alpha = r4[2] / r4[0];
         s->first = 0;
         s->converged = sconv || (rn <= s->tol);
         if(!isfinite(rn)) { s->status = BBB_ERR_NONFINITE; s->done = 1; }
         if(s->converged || s->iter >= s->maxit) s->done = 1;
+        if(s->keep && !(rn <= 1e3 * s->rstart)) { s->status = -1; s->done = 1; }
         if(((volatile bbb_kry *)s)->pad) { s->status = BBB_ERR_CUDA; s->done = 1; }
       }
     }
@@ -618,7 +620,7 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
         s->t_t = red[1];
         s->s_s = red[2];
         double sn = sqrt(red[2]);
-        int sconv = (sn <= s->tol);
+        int sconv = (sn <= s->tol) && (!s->keep || sn == 0.);
         s->s_conv = sconv;
         if(sconv) {
           s->rnorm = sn;

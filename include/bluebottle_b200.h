@@ -161,6 +161,11 @@ typedef struct bbb_options {
   int gravity_balance;     /* 1: set gradP.z so the box's net weight is 0  */
   int lamb_max_iter_override; /* >0: replaces lamb_max_iter               */
   int verbose;
+  int reliable;            /* mixed form: 1 carries the FP32 BiCGSTAB's
+                              Krylov state across the FP64 residual
+                              replacements (reliable updates, falling back
+                              to a restart on breakdown); 0 restarts it at
+                              every sweep                                  */
 } bbb_options;
 
 void bbb_default_options(bbb_options *opt);
