@@ -120,7 +120,8 @@ cuda_store_coeffs cuda_find_dt cuda_compute_energy cuda_div_U
 cuda_dom_turb_planes_push cuda_dom_turb_planes_pull cuda_compute_turb_forcing
 cuda_yank_turb_planes bbb_default_options bbb_set_options bbb_get_options
 bbb_read_input bbb_domain_init bbb_parts_init bbb_seed_particles
-bbb_init_taylor_green bbb_host_free bbb_prepare bbb_release
+bbb_init_taylor_green bbb_host_free bbb_out_restart bbb_in_restart
+bbb_prepare bbb_release
 bbb_set_record_dir bbb_step bbb_advance_clock bbb_get_stats bbb_last_status
 bbb_status_string bbb_clear_status bbb_set_exit_on_failure bbb_device_count
 bbb_divergence bbb_kernel_launches bbb_reset_kernel_launches
@@ -154,8 +155,11 @@ def load():
                  "bbb_device_count", "bbb_prepare", "bbb_learn_enable",
                  "bbb_learn_crops", "bbb_learn_param_count",
                  "bbb_learn_get_params", "bbb_learn_set_params",
-                 "bbb_learn_forward", "bbb_PP_bicgstab_static"):
+                 "bbb_learn_forward", "bbb_PP_bicgstab_static",
+                 "bbb_out_restart", "bbb_in_restart"):
         getattr(lib, name).restype = C.c_int
+    lib.bbb_out_restart.argtypes = [C.c_char_p]
+    lib.bbb_in_restart.argtypes = [C.c_char_p]
     lib.bbb_kernel_launches.restype = C.c_longlong
     lib.bbb_status_string.restype = C.c_char_p
     lib.bbb_read_input.argtypes = [C.c_char_p]

@@ -146,6 +146,17 @@ class Sim:
         self.lib.cuda_dom_pull()
         self.lib.cuda_part_pull()
 
+    # -------------------------------------------------------- restart
+    def out_restart(self, path):
+        """Write the reference's restart file from the host copies (pull
+        first when the simulation has run on the device)."""
+        self._check(self.lib.bbb_out_restart(os.fsencode(path)), "out_restart")
+
+    def in_restart(self, path):
+        """Read a restart file into the host copies (push, or prepare,
+        afterwards to run from it)."""
+        self._check(self.lib.bbb_in_restart(os.fsencode(path)), "in_restart")
+
     def push(self):
         self.lib.cuda_dom_push()
         self.lib.cuda_part_push()

@@ -111,6 +111,12 @@ extern BC bc;
 extern gradP_struct gradP;
 extern long int cpumem, gpumem;
 extern real pid_int, pid_back, Kp, Ki, Kd;
+/* recorder clocks and precursor plane positions that the restart file
+ * carries (src/bluebottle.c:127-182) */
+extern int rec_paraview_stepnum_out;
+extern real rec_flow_field_ttime_out, rec_paraview_ttime_out,
+  rec_particle_ttime_out, rec_restart_ttime_out, rec_prec_ttime_out;
+extern real bc_plane_pos[9];
 extern int *phase, *phase_shell, *flag_u, *flag_v, *flag_w;
 extern int nparts;
 extern real interactionLengthRatio;
@@ -189,6 +195,18 @@ int bbb_seed_particles(int n, real a, real min_gap, real rho, int order,
  * w = 0 on the staggered faces (domain assumed [0, 2pi)^3 scaled). */
 void bbb_init_taylor_green(real U);
 void bbb_host_free(void);
+
+/* The reference's restart file (out_restart / in_restart,
+ * src/domain.c:3223, :3318): the same bytes from and into the host copies
+ * of the state.  path NULL or "" means ./input/restart.config, the
+ * reference's fixed name.  The diffusion histories are in the file only
+ * when the step is explicit (option implicit = 0), as in a reference built
+ * without -DIMPLICIT.  Pull the device state before writing and push it
+ * after reading.  Return BBB_OK, BBB_ERR_STATE (no domain set up) or
+ * BBB_ERR_CONFIG (the file cannot be opened, is short, or holds another
+ * coefficient stride). */
+int bbb_out_restart(const char *path);
+int bbb_in_restart(const char *path);
 
 /* Device set-up after the host initialisation, in the order of
  * src/bluebottle.c:415-543: cuda_dom_malloc, cuda_part_malloc, the pushes,

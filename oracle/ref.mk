@@ -13,7 +13,7 @@ OUT := $(HERE)_ref
 CC = gcc
 CFLAGS = -std=gnu99 -O2 -fPIC -fopenmp -DDOUBLE -w -I$(OUT) -I$(REF)
 
-all: $(OUT)/libref_host.so
+all: $(OUT)/libref_host.so $(OUT)/libref_host_implicit.so
 
 $(OUT)/cgnslib.h:
 	mkdir -p $(OUT)
@@ -29,6 +29,14 @@ $(OUT)/ref_globals.o: $(OUT)/ref_globals.c
 	$(CC) $(CFLAGS) -c $< -o $@
 
 $(OUT)/libref_host.so: $(OUT)/domain.o $(OUT)/particle.o $(OUT)/rng.o $(OUT)/ref_globals.o
+	$(CC) -shared -fopenmp -o $@ $^ -lm -Wl,--no-undefined
+
+# the same sources built as the Crank-Nicolson (-DIMPLICIT) program, whose
+# restart file omits the diffusion histories (src/domain.c:3242)
+$(OUT)/%_i.o: $(REF)/%.c $(OUT)/cgnslib.h
+	$(CC) $(CFLAGS) -DIMPLICIT -c $< -o $@
+
+$(OUT)/libref_host_implicit.so: $(OUT)/domain_i.o $(OUT)/particle_i.o $(OUT)/rng_i.o $(OUT)/ref_globals.o
 	$(CC) -shared -fopenmp -o $@ $^ -lm -Wl,--no-undefined
 
 clean:
