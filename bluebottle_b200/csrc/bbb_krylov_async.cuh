@@ -75,9 +75,9 @@ struct as_layout {
   static constexpr int SMEM = SH_OFF + 32 * 5 * 8 + 128;
   /* resident blocks per SM the register budget targets */
   static constexpr int MINB = ESZ == 4 ? (PASS == 1 ? 3 : 2) : (PASS == 1 ? 2 : 1);
-  /* plane-aligned block runs (retile): measured faster for the FP32 pass A
-   * only -- the latency-bound passes lose more to the idle slots */
-  static constexpr bool ALIGN = ESZ == 4 && PASS == 0;
+  /* plane-aligned group runs (retile): off -- grouping neighbouring tiles
+   * gets the same L2 reuse without idle slots */
+  static constexpr bool ALIGN = false;
   /* bytes a stage receives: the boxes always, the wrap slots at edges */
   static constexpr int TX_BASE = NA * BOXH * ROWP + BOXH * MROWP + NO * 8 * OWNB;
   static constexpr int TX_XSIDE = (NA + 1) * 8 * 16;
@@ -440,16 +440,22 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
   double red[5] = {0., 0., 0., 0., 0.};
   int bad = 0;
   long long nload = 0;
-  const long long bxl = blockIdx.x;
-  long long u0 = bxl * B.q + (bxl < B.r ? bxl : B.r);
-  const long long u1 = u0 + B.q + (bxl < B.r ? 1 : 0);
+  /* this block's group, its tile inside the group, the group's units */
+  const int G = B.gx * B.gy;
+  const long long grp = blockIdx.x / G;
+  const int mem = (int)(blockIdx.x % G);
+  long long u0 = grp * B.q + (grp < B.r ? grp : B.r);
+  const long long u1 = u0 + B.q + (grp < B.r ? 1 : 0);
+  const int gtx = B.tiles_x / B.gx;     /* groups along x */
   const int col = tx * 4;
   while(u0 < u1) {
-    const long long tile = u0 / B.nz;
-    const int k0 = (int)(u0 - tile * B.nz);
+    const long long gt = u0 / B.nz;
+    const int k0 = (int)(u0 - gt * B.nz);
     const long long left_ = u1 - u0;
     const int k1 = left_ < (long long)(B.nz - k0) ? k0 + (int)left_ : B.nz;
-    const int i0 = (int)(tile % B.tiles_x) * AS_W, j0 = (int)(tile / B.tiles_x) * 8;
+    const int ti = (int)(gt % gtx) * B.gx + mem % B.gx;
+    const int tj = (int)(gt / gtx) * B.gy + mem / B.gx;
+    const int i0 = ti * AS_W, j0 = tj * 8;
     const int j = j0 + w;
     const bool valid = j < B.ny;
     const as_edges E = as_tile_edges(B, i0, j0);
