@@ -323,6 +323,8 @@ extern "C" void cuda_part_free(void)
   dfree(g_dev.node_up); dfree(g_dev.perr);
   dfree(g_dev.lf_idx); dfree(g_dev.lf_part); dfree(g_dev.lf_geo);
   dfree(g_dev.lf_count);
+  dfree(g_dev.lf_pcnt); dfree(g_dev.lf_pstart); dfree(g_dev.lf_pfill);
+  g_dev.lf_np = 0;
   g_dev.lf_cap = 0; g_dev.lf_n = 0; g_dev.lf_valid = 0; g_dev.lf_geo_valid = 0;
   g_dev.np = 0;
 }

@@ -101,6 +101,9 @@ struct bbb_dev {
   int *lf_idx, *lf_part;
   double *lf_geo;
   unsigned int *lf_count;
+  int *lf_pcnt, *lf_pstart, *lf_pfill;   /* faces per particle, list
+                                            offsets, fill cursors      */
+  int lf_np;                             /* particles they are sized for */
   int lf_valid, lf_geo_valid;
   real *red_host;                  /* pinned scratch for host reductions */
   double *red_dev;                 /* device scratch for small reductions */

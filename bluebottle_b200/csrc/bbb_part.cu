@@ -498,6 +498,7 @@ __device__ __forceinline__ double d_wrap_rel(double x, double a, double L)
 
 #define LF_NGEO 14   /* x y z r ct st cp1 sp1 cp2 sp2 cp3 sp3 cp4 sp4 */
 __constant__ double c_Nnm[6][6];
+__constant__ double c_od2np3[6], c_odnp1[6];   /* 1/(2n+3), 1/(n+1) */
 static int g_nnm_ready = 0;
 
 static void upload_nnm(void)
@@ -511,6 +512,10 @@ static void upload_nnm(void)
     t[n][m] = m <= n ? sqrt((2. * n + 1.) / 4. / PI * top / bot) : 0.;
   }
   BBB_CK(cudaMemcpyToSymbol(c_Nnm, t, sizeof(t)));
+  double a[6], b[6];
+  for(int n = 0; n < 6; n++) { a[n] = 1. / (2. * n + 3.); b[n] = 1. / (n + 1.); }
+  BBB_CK(cudaMemcpyToSymbol(c_od2np3, a, sizeof(a)));
+  BBB_CK(cudaMemcpyToSymbol(c_odnp1, b, sizeof(b)));
   g_nnm_ready = 1;
 }
 
@@ -532,27 +537,53 @@ __device__ __forceinline__ int lf_owner(int comp, int i, int j, int k,
   return P0 > -1 ? P0 : (P1 > -1 ? P1 : -1);
 }
 
-/* pass 0 counts, pass 1 fills (slot order is irrelevant: every face is
- * written by exactly one entry) */
+/* pass 0 counts the faces per particle, pass 1 fills each particle's
+ * faces into its own run of the list, so that the threads of a warp
+ * evaluating the list mostly share one particle and its coefficients (the
+ * order inside a run is irrelevant: every face is written by exactly one
+ * entry).  The threads of a warp that hold faces of one particle update
+ * its counter with one atomic. */
 __global__ void k_lf_collect(const int *phs, const int *fu, const int *fv,
-  const int *fw, bbb_geom G, int pass, unsigned int *count, int *idx,
-  int *part, long long cap)
+  const int *fw, bbb_geom G, int pass, int *pcnt, const int *pstart,
+  int *pfill, int *idx, int *part, long long cap)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
   int k = blockIdx.z;
-  if(i > G.nx + 1 || j > G.ny + 1 || k > G.nz + 1) return;
+  int lane = (threadIdx.x + blockDim.x * threadIdx.y) & 31;
+  bool in = !(i > G.nx + 1 || j > G.ny + 1 || k > G.nz + 1);
+  unsigned alive = __ballot_sync(0xffffffffu, in);
+  if(!in) return;
   for(int comp = 0; comp < 3; comp++) {
-    if((comp == 0 && i < 1) || (comp == 1 && j < 1) || (comp == 2 && k < 1)) continue;
-    long long C;
-    int P = lf_owner(comp, i, j, k, phs, fu, fv, fw, G, &C);
+    bool skip = (comp == 0 && i < 1) || (comp == 1 && j < 1) || (comp == 2 && k < 1);
+    long long C = 0;
+    int P = skip ? -1 : lf_owner(comp, i, j, k, phs, fu, fv, fw, G, &C);
+    unsigned faces = __ballot_sync(alive, P >= 0);
     if(P < 0) continue;
-    unsigned int slot = atomicAdd(count, 1u);
-    if(pass == 1 && slot < cap) {
-      idx[slot] = (int)(((unsigned int)comp << 30) | (unsigned int)C);
-      part[slot] = P;
+    unsigned peers = __match_any_sync(faces, P);
+    int lead = __ffs(peers) - 1, n = __popc(peers);
+    if(pass == 0) {
+      if(lane == lead) atomicAdd(&pcnt[P], n);
+    } else {
+      int base = 0;
+      if(lane == lead) base = atomicAdd(&pfill[P], n);
+      base = __shfl_sync(peers, base, lead);
+      long long slot = (long long)pstart[P] + base
+        + __popc(peers & ((1u << lane) - 1u));
+      if(slot < cap) {
+        idx[slot] = (int)(((unsigned int)comp << 30) | (unsigned int)C);
+        part[slot] = P;
+      }
     }
   }
+}
+
+/* total of the per-particle face counts (after their scan) */
+__global__ void k_lf_total(const int *pcnt, const int *pstart, int np,
+  unsigned int *count)
+{
+  if(threadIdx.x == 0 && blockIdx.x == 0)
+    *count = np > 0 ? (unsigned int)(pstart[np - 1] + pcnt[np - 1]) : 0u;
 }
 
 /* particle-frame geometry of every listed face, from the current
@@ -649,13 +680,23 @@ __global__ void __launch_bounds__(256) k_lf_eval(long long n, const int *idx,
                  *cre = cf.c[4], *cim = cf.c[5];
     int base = P * stride;
     /* n = 0 terms */
-    double Y0 = c_Nnm[0][0] * (-1. * ct / stc * 1. + 1. / stc * lf_P(1, 0, ct, st)) * pre[base];
+    /* one division per face: the reference divides by sin(theta) in
+     * every (n, m) term; multiplying by its reciprocal differs by at most
+     * an ulp per term and takes the ~50 FP64 divisions per face (most of
+     * this kernel's time) out of the loop */
+    const double inv_stc = 1. / stc;
+    double Y0 = c_Nnm[0][0] * (-1. * ct * inv_stc * 1. + inv_stc * lf_P(1, 0, ct, st)) * pre[base];
     double ur = 0.;
     double ut = 0.5 * ra * Y0;
     double up = 0.;
     double ran = 1., arn = 1.;   /* ra^(n-1), ar^n at the loop head */
     int c0 = 1;
-    for(int nn_ = 1; nn_ <= order; nn_++) {
+    /* both loops unrolled over the orders the tables hold (n <= 5): every
+     * P_n^m becomes a fixed polynomial and cos(m phi), sin(m phi) stay in
+     * registers; the guard keeps the particle's own order */
+#pragma unroll
+    for(int nn_ = 1; nn_ <= 5; nn_++) {
+      if(nn_ > order) break;
       double n = nn_;
       arn *= ar;
       double powranm1 = ran;
@@ -663,14 +704,15 @@ __global__ void __launch_bounds__(256) k_lf_eval(long long n, const int *idx,
       double powarn = arn;
       double powarnp1 = arn * ar;
       double powarnp2 = powarnp1 * ar;
-      double od2np3 = 1. / (2. * n + 3.);
-      double odnp1 = 1. / (n + 1.);
+      double od2np3 = c_od2np3[nn_];    /* 1 / (2n + 3), 1 / (n + 1) */
+      double odnp1 = c_odnp1[nn_];
       double Xp = 0., Xf = 0., Yp = 0., Yf = 0., Yc = 0., Zp = 0., Zf = 0., Zc = 0.;
+#pragma unroll
       for(int m = 0; m <= nn_; m++) {
         int c = base + c0 + m;
         double N = c_Nnm[nn_][m];
         double Pn = lf_P(nn_, m, ct, st);
-        double dY = -(n + 1) * ct / stc * Pn + (nn_ - m + 1) / stc * lf_P(nn_ + 1, m, ct, st);
+        double dY = -(n + 1) * ct * inv_stc * Pn + (nn_ - m + 1) * inv_stc * lf_P(nn_ + 1, m, ct, st);
         double w = m == 0 ? 1. : 2.;
         double Rp = pre[c] * cm[m] - pim[c] * sm[m];
         double Rf = fre[c] * cm[m] - fim[c] * sm[m];
@@ -681,7 +723,7 @@ __global__ void __launch_bounds__(256) k_lf_eval(long long n, const int *idx,
         Yf += w * N * dY * Rf;
         Yc += w * N * dY * Rc;
         if(m > 0) {
-          double zf = -2. * m / stc * N * Pn;
+          double zf = -2. * m * inv_stc * N * Pn;
           Zp += zf * (pre[c] * sm[m] + pim[c] * cm[m]);
           Zf += zf * (fre[c] * sm[m] + fim[c] * cm[m]);
           Zc += zf * (cre[c] * sm[m] + cim[c] * cm[m]);
@@ -727,6 +769,8 @@ __global__ void __launch_bounds__(256) k_lf_eval(long long n, const int *idx,
   }
 }
 
+__global__ void k_bin_scan(const int *cnt, int *start, int n);
+
 static void lf_build(void)
 {
   bbb_geom G = bbb_make_geom();
@@ -737,13 +781,35 @@ static void lf_build(void)
       return;
     }
   }
+  if(g_dev.lf_np != nparts) {
+    if(g_dev.lf_pcnt) cudaFree(g_dev.lf_pcnt);
+    if(g_dev.lf_pstart) cudaFree(g_dev.lf_pstart);
+    if(g_dev.lf_pfill) cudaFree(g_dev.lf_pfill);
+    g_dev.lf_pcnt = g_dev.lf_pstart = g_dev.lf_pfill = NULL;
+    g_dev.lf_np = 0;
+    size_t b = sizeof(int) * (size_t)(nparts > 0 ? nparts : 1);
+    if(cudaMalloc((void **)&g_dev.lf_pcnt, b) != cudaSuccess
+      || cudaMalloc((void **)&g_dev.lf_pstart, b) != cudaSuccess
+      || cudaMalloc((void **)&g_dev.lf_pfill, b) != cudaSuccess) {
+      bbb_set_status(BBB_ERR_CUDA, "cudaMalloc face list");
+      return;
+    }
+    g_dev.lf_np = nparts;
+  }
+  size_t pb = sizeof(int) * (size_t)nparts;
   for(int pass = 0; pass < 2; pass++) {
-    BBB_CK(cudaMemsetAsync(g_dev.lf_count, 0, sizeof(unsigned int), g_dev.stream));
+    if(pass == 0) BBB_CK(cudaMemsetAsync(g_dev.lf_pcnt, 0, pb, g_dev.stream));
+    else BBB_CK(cudaMemsetAsync(g_dev.lf_pfill, 0, pb, g_dev.stream));
     k_lf_collect<<<grd, blk, 0, g_dev.stream>>>(g_dev.phase, g_dev.flag_u,
-      g_dev.flag_v, g_dev.flag_w, G, pass, g_dev.lf_count, g_dev.lf_idx,
-      g_dev.lf_part, g_dev.lf_cap);
+      g_dev.flag_v, g_dev.flag_w, G, pass, g_dev.lf_pcnt, g_dev.lf_pstart,
+      g_dev.lf_pfill, g_dev.lf_idx, g_dev.lf_part, g_dev.lf_cap);
     BBB_LAUNCHED();
     if(pass == 0) {
+      k_bin_scan<<<1, 1024, 0, g_dev.stream>>>(g_dev.lf_pcnt, g_dev.lf_pstart, nparts);
+      BBB_LAUNCHED();
+      k_lf_total<<<1, 32, 0, g_dev.stream>>>(g_dev.lf_pcnt, g_dev.lf_pstart, nparts,
+        g_dev.lf_count);
+      BBB_LAUNCHED();
       unsigned int cnt = 0;
       BBB_CK(cudaMemcpyAsync(&cnt, g_dev.lf_count, sizeof(cnt),
         cudaMemcpyDeviceToHost, g_dev.stream));
