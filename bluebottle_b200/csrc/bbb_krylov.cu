@@ -1469,6 +1469,36 @@ static void ensure_fp32(void)
   }
 }
 
+/* The FP64 outer residual of a defect-correction sweep, r = b - A x into
+ * FP32 rf with the sweep's scalars: the tensor-map staged pass where the
+ * rows are a multiple of 128 cells, else the register-tiled kernel. */
+template <int VD>
+static void outer_resid(const boxc &BD, const opc &O, const uint8_t *mask,
+  const double *b, const double *x, float *rf, bbb_kry *s, bbb_kry *si,
+  double itol, int imaxit, int project, long long n)
+{
+  if(BBB_ASYNC_ON && BD.nx % AS_W == 0 && as_per_sm<double, 2>() > 0) {
+    boxc B2 = retile(BD, as_per_sm<double, 2>(), false);
+    as_maps M;
+    const double *h[4] = {x, NULL, NULL, NULL}, *o[2] = {b, NULL};
+    if(as_pass_maps<double, 2>(&M, B2, mask, h, o)) {
+      as_args<double> A;
+      memset(&A, 0, sizeof(A));
+      A.mask = mask; A.h[0] = x; A.s = s; A.partials = g_dev.partials;
+      A.rf = rf; A.si = si; A.itol = itol; A.imaxit = imaxit;
+      A.project = project; A.n = n;
+      k_bicg_async<double, 2><<<B2.nblk, AS_THREADS, as_layout<double, 2>::SMEM,
+        g_dev.stream>>>(B2, O, A, M);
+      BBB_LAUNCHED();
+      return;
+    }
+  }
+  dim3 grd = box_grid(BD), blk(TX, TY);
+  k_outer_resid<VD><<<grd, blk, 0, g_dev.stream>>>(BD, O, mask, b, x, rf, s, si,
+    g_dev.partials, itol, imaxit, project, n);
+  BBB_LAUNCHED();
+}
+
 /* runs after k_pp_rhs has filled b, x and s->bnorm */
 template <int VD, int VF>
 static int poisson_mixed(const boxc &BD, const boxc &BF, const opc &O,
@@ -1492,10 +1522,8 @@ static int poisson_mixed(const boxc &BD, const boxc &BF, const opc &O,
   double itol = g_opt.inner_tol > 0 ? g_opt.inner_tol : 1e-4;
   int inner_total = 0, cur = 0, fresh = 1, resume_failed = 0;
   for(int outer = 0; outer <= init.maxit; outer++) {
-    k_outer_resid<VD><<<grdD, blk, 0, g_dev.stream>>>(BD, O, g_dev.mask_p,
-      g_dev.kb, g_dev.kx, g_dev.fb, s, si, g_dev.partials, itol, pp_max_iter,
-      project, n);
-    BBB_LAUNCHED();
+    outer_resid<VD>(BD, O, g_dev.mask_p, g_dev.kb, g_dev.kx, g_dev.fb, s, si,
+      itol, pp_max_iter, project, n);
     /* a sweep starts the FP32 BiCGSTAB from e = 0; with reliable updates
      * later sweeps replace its residual by the FP64 one and carry on
      * (restarting only after an inner breakdown).  On the 256x256x512
@@ -1941,9 +1969,8 @@ static int helmholtz_mixed(const boxc &BD, const boxc &BF, const opc &O,
   dim3 grdD = box_grid(BD), grdF = box_grid(BF), blk(TX, TY);
   int inner_total = 0;
   for(int outer = 0; outer <= max_outer; outer++) {
-    k_outer_resid<VD><<<grdD, blk, 0, g_dev.stream>>>(BD, O, mask, g_dev.kb,
-      g_dev.kx, g_dev.fr, s, si, g_dev.partials, itol, pp_max_iter, 0, n);
-    BBB_LAUNCHED();
+    outer_resid<VD>(BD, O, mask, g_dev.kb, g_dev.kx, g_dev.fr, s, si, itol,
+      pp_max_iter, 0, n);
     k_cg_inner_setup<VF><<<NPW, 256, 0, g_dev.stream>>>(n, O, mask, g_dev.fr,
       g_dev.fx, g_dev.fp[0], si, g_dev.partials);
     BBB_LAUNCHED();

@@ -51,7 +51,7 @@ template <typename T, int PASS>
 struct as_layout {
   static constexpr int ESZ = (int)sizeof(T);
   static constexpr int CH = 16 / ESZ;
-  static constexpr int NA = PASS == 0 ? 4 : 2;
+  static constexpr int NA = PASS == 0 ? 4 : (PASS == 1 ? 2 : 1);
   static constexpr int NO = PASS == 0 ? 2 : 1;
   static constexpr int BOXW = AS_W + 2 * CH;        /* halo-array box  */
   static constexpr int BOXH = 10;
@@ -74,7 +74,7 @@ struct as_layout {
   /* + 128: the dynamic window is aligned up to 128 bytes at run time */
   static constexpr int SMEM = SH_OFF + 32 * 5 * 8 + 128;
   /* resident blocks per SM the register budget targets */
-  static constexpr int MINB = ESZ == 4 ? (PASS == 1 ? 3 : 2) : (PASS == 1 ? 2 : 1);
+  static constexpr int MINB = ESZ == 4 ? (PASS == 1 ? 3 : 2) : (PASS == 0 ? 1 : 2);
   /* plane-aligned group runs (retile): off -- grouping neighbouring tiles
    * gets the same L2 reuse without idle slots */
   static constexpr bool ALIGN = false;
@@ -101,6 +101,13 @@ struct as_args {
   T *x;                   /* pass A: x, updated in place                 */
   bbb_kry *s;
   double *partials;
+  /* outer residual (pass 2): r = b - A x rounded to FP32, and the inner
+   * solve's scalars it sets up */
+  float *rf;
+  bbb_kry *si;
+  double itol;
+  int imaxit, project;
+  long long n;
 };
 
 __device__ __forceinline__ uint32_t as_saddr(const void *p)
@@ -312,13 +319,16 @@ __device__ __forceinline__ void as_q4(const uint8_t *h, unsigned mw,
         q[a] = dinv[mbyte(mw, a)] * pn;
       }
     }
-  } else {
+  } else if constexpr(PASS == 1) {
     T rr[4], vv[4];
     T al = (T)S.alpha;
     as_ld4<T>(h, rr);
     as_ld4<T>(h + 1 * L::AREG, vv);
 #pragma unroll
     for(int a = 0; a < 4; a++) q[a] = dinv[mbyte(mw, a)] * (rr[a] - al * vv[a]);
+  } else {
+    as_ld4<T>(h, q);                   /* outer residual: q = x */
+    (void)mw; (void)dinv; (void)S;
   }
 }
 
@@ -362,7 +372,7 @@ __device__ __forceinline__ void as_own4(const uint8_t *h, unsigned mw,
     as_dot4<T>(red[2], raw0, rr);
     as_st4<T>(A.w0 + gc, rr);
     as_st4<T>(A.w1 + gc, pn);
-  } else {
+  } else if constexpr(PASS == 1) {
     T rr[4], vv[4];
     T al = (T)S.alpha;
     as_ld4<T>(h, rr);
@@ -375,6 +385,12 @@ __device__ __forceinline__ void as_own4(const uint8_t *h, unsigned mw,
     as_ld4<T>(o, raw1);
     as_dot4<T>(red[2], raw0, raw0);
     as_st4<T>(A.w0 + gc, raw0);
+  } else {
+    /* outer residual: q = x (sum x over the owned cells), raw0 = b */
+    as_ld4<T>(h, q);
+    as_sum4<T>(red[1], q);
+    as_ld4<T>(o, raw0);
+    (void)mw; (void)dinv; (void)S; (void)gc; (void)A; (void)raw1;
   }
 }
 
@@ -396,10 +412,13 @@ __device__ __forceinline__ T as_q1(const uint8_t *h, int stride, unsigned m,
       pn = rr + (T)S.beta * pp + (T)S.bo * vv;
     }
     return dinv[m] * pn;
-  } else {
+  } else if constexpr(PASS == 1) {
     T rr = *reinterpret_cast<const T *>(h);
     T vv = *reinterpret_cast<const T *>(h + stride);
     return dinv[m] * (rr - (T)S.alpha * vv);
+  } else {
+    (void)stride; (void)m; (void)dinv; (void)S;
+    return *reinterpret_cast<const T *>(h);
   }
 }
 
@@ -564,12 +583,21 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
         if constexpr(PASS == 0) {
           as_st4<T>(A.w2 + ge, Aq);
           as_dot4<T>(red[0], r0c, Aq);
-        } else {
+        } else if constexpr(PASS == 1) {
           as_st4<T>(A.w1 + ge, Aq);
           as_dot4<T>(red[0], Aq, r0c);
           as_dot4<T>(red[1], Aq, Aq);
           as_dot4<T>(red[3], r1c, r0c);
           as_dot4<T>(red[4], r1c, Aq);
+        } else {
+          /* outer residual r = b - A x in FP64, stored rounded to FP32 */
+          T rr[4];
+#pragma unroll
+          for(int v = 0; v < 4; v++) rr[v] = r0c[v] - Aq[v];
+          *reinterpret_cast<float4 *>(A.rf + ge) =
+            make_float4((float)rr[0], (float)rr[1], (float)rr[2], (float)rr[3]);
+          as_dot4<T>(red[0], rr, rr);
+          as_sum4<T>(red[2], rr);
         }
       }
 #pragma unroll
@@ -594,8 +622,35 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
       }
     if(tid == 0) atomicOr(&s->pad, 1);
   }
-  /* the pass's reductions and scalar updates, as k_bicgA / k_bicgB */
-  if constexpr(PASS == 0) {
+  /* the pass's reductions and scalar updates, as k_bicgA / k_bicgB /
+   * k_outer_resid */
+  if constexpr(PASS == 2) {
+    double r3[3] = {red[0], red[1], red[2]};
+    if(bbb_grid_partial<3>(r3, A.partials, &s->ticket, sh)) {
+      bbb_grid_finish_sum<3>(r3, A.partials, &s->ticket, sh);
+      if(tid == 0) {
+        bbb_kry *si = A.si;
+        double rn = sqrt(r3[0]);
+        s->rnorm = rn;
+        s->sumx = r3[1];
+        s->converged = (rn <= s->tol);
+        s->s_conv = 0;
+        if(!isfinite(rn)) { s->status = BBB_ERR_NONFINITE; s->done = 1; }
+        if(s->converged || s->iter >= s->maxit) s->done = 1;
+        if(((volatile bbb_kry *)s)->pad) { s->status = BBB_ERR_CUDA; s->done = 1; }
+        double mean = A.project ? r3[2] / (double)A.n : 0.;
+        si->sumx = mean;                 /* subtracted by the inner set-up */
+        double need = rn > 0. ? 0.5 * s->tol / rn : 1.;
+        si->tol = fmax(A.itol, need) * rn;
+        si->maxit = A.imaxit;
+        si->done = s->done;
+        if(s->done) {
+          /* no inner sweep follows: it reports no iterations or passes */
+          si->iter = 0; si->first = 1; si->s_conv = 0;
+        }
+      }
+    }
+  } else if constexpr(PASS == 0) {
     double r4[4] = {red[0], red[1], red[2], red[3]};
     if(bbb_grid_partial<4>(r4, A.partials, &s->ticket, sh)) {
       bbb_grid_finish_sum<4>(r4, A.partials, &s->ticket, sh);
