@@ -1780,8 +1780,32 @@ __global__ void __launch_bounds__(256) k_cg2(long long n, opc O,
   optab_fill<T>(tab, O);
   T a = (T)s->alpha;
   double red[2] = {0., 0.};
-  for(long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
-      c += (long long)gridDim.x * blockDim.x) {
+  /* 16 bytes per array and thread per step (the vectors start 256-byte
+   * aligned); the n % V cells past the last full vector by the first
+   * threads */
+  constexpr int V = 16 / (int)sizeof(T);
+  const long long nv = n / V;
+  const long long tid0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for(long long q = tid0; q < nv; q += stride) {
+    const long long c = q * V;
+    T pv[V], xv[V], yv[V], rv[V];
+    ldv<T, V>(p, c, pv); ldv<T, V>(x, c, xv);
+    ldv<T, V>(y, c, yv); ldv<T, V>(r, c, rv);
+    unsigned mw;
+    if constexpr(V == 4) mw = *reinterpret_cast<const unsigned *>(mask + c);
+    else mw = *reinterpret_cast<const unsigned short *>(mask + c);
+#pragma unroll
+    for(int v = 0; v < V; v++) {
+      xv[v] = a * pv[v] + xv[v];
+      rv[v] = -a * yv[v] + rv[v];
+      T z = tab.dinv[(mw >> (8 * v)) & 0xffu] * rv[v];
+      red[0] += (double)rv[v] * (double)z;
+      red[1] += (double)rv[v] * (double)rv[v];
+    }
+    stv<T, V>(x, c, xv); stv<T, V>(r, c, rv);
+  }
+  for(long long c = nv * V + tid0; c < n; c += stride) {
     T pv = p[c];
     x[c] = a * pv + x[c];
     T rv = -a * y[c] + r[c];
