@@ -496,8 +496,22 @@ __global__ void k_mask_p(const int *fu, const int *fv, const int *fw,
  * mixed staggered positions the reference uses (src/bicgstab_kernel.cu:
  * 829-944), identity where the component's own flag < 0
  * (src/bicgstab_kernel.cu:730-827) */
+/* the face (i, j, k) (1-based, ghosted grid) of dense index t of a
+ * component system stored x-fastest in an X x Y x Z box, or, when `tr`,
+ * y-fastest (the box's x axis is the grid's y axis) */
+__device__ __forceinline__ void helm_ijk(long long t, int X, int Y, int tr,
+  int &i, int &j, int &k)
+{
+  int a = (int)(t % X);
+  long long r = t / X;
+  int b = (int)(r % Y);
+  k = (int)(r / Y) + 1;
+  i = (tr ? b : a) + 1;
+  j = (tr ? a : b) + 1;
+}
+
 __global__ void k_mask_face(const int *fu, const int *fv, const int *fw,
-  bbb_geom G, int comp, int nx, int ny, int nz, uint8_t *mask)
+  bbb_geom G, int comp, int nx, int ny, int nz, int tr, uint8_t *mask)
 {
   long long n = (long long)nx * ny * nz;
   const int *fs = comp == 0 ? fu : (comp == 1 ? fv : fw);
@@ -505,9 +519,8 @@ __global__ void k_mask_face(const int *fu, const int *fv, const int *fw,
   int s2 = comp == 0 ? G.fx_s2 : (comp == 1 ? G.fy_s2 : G.fz_s2);
   for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
       t += (long long)gridDim.x * blockDim.x) {
-    int i = (int)(t % nx) + 1;
-    long long r = t / nx;
-    int j = (int)(r % ny) + 1, k = (int)(r / ny) + 1;
+    int i, j, k;
+    helm_ijk(t, nx, ny, tr, i, j, k);
     long long W = i + (long long)j * G.fx_s1 + (long long)k * G.fx_s2;
     long long S = i + (long long)j * G.fy_s1 + (long long)k * G.fy_s2;
     long long Bq = i + (long long)j * G.fz_s1 + (long long)k * G.fz_s2;
@@ -519,8 +532,25 @@ __global__ void k_mask_face(const int *fu, const int *fv, const int *fw,
     m |= fw[Bq] != 0 ? BBB_MB : 0;
     m |= fw[Bq + G.fz_s2] != 0 ? BBB_MT : 0;
     if(fs[i + (long long)j * s1 + (long long)k * s2] < 0) m |= BBB_MID;
+    if(tr) {
+      /* the box's W/E faces are the grid's S/N and the other way round */
+      uint8_t q = m & (BBB_MB | BBB_MT | BBB_MID);
+      q |= (m & BBB_MS) ? BBB_MW : 0;
+      q |= (m & BBB_MN) ? BBB_ME : 0;
+      q |= (m & BBB_MW) ? BBB_MS : 0;
+      q |= (m & BBB_ME) ? BBB_MN : 0;
+      m = q;
+    }
     mask[t] = m;
   }
+}
+
+/* the u system is stored y-fastest where its rows (nx + 1 faces) cannot
+ * take the vector kernels and the grid's y rows can */
+static int helm_tr(int comp, const bbb_geom &G)
+{
+  return comp == 0 && pick_vec(G.nx + 1, sizeof(float)) == 1
+    && pick_vec(G.ny, sizeof(float)) == 4 && pick_vec(G.ny, sizeof(double)) == 2;
 }
 
 void bbb_build_masks(void)
@@ -530,14 +560,16 @@ void bbb_build_masks(void)
   k_mask_p<<<NPW, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
     g_dev.flag_w, g_dev.phase, G, g_dev.mask_p);
   BBB_LAUNCHED();
+  int tu = helm_tr(0, G);
   k_mask_face<<<NPW, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
-    g_dev.flag_w, G, 0, G.nx + 1, G.ny, G.nz, g_dev.mask_u);
+    g_dev.flag_w, G, 0, tu ? G.ny : G.nx + 1, tu ? G.nx + 1 : G.ny, G.nz, tu,
+    g_dev.mask_u);
   BBB_LAUNCHED();
   k_mask_face<<<NPW, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
-    g_dev.flag_w, G, 1, G.nx, G.ny + 1, G.nz, g_dev.mask_v);
+    g_dev.flag_w, G, 1, G.nx, G.ny + 1, G.nz, 0, g_dev.mask_v);
   BBB_LAUNCHED();
   k_mask_face<<<NPW, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
-    g_dev.flag_w, G, 2, G.nx, G.ny, G.nz + 1, g_dev.mask_w);
+    g_dev.flag_w, G, 2, G.nx, G.ny, G.nz + 1, 0, g_dev.mask_w);
   BBB_LAUNCHED();
   g_dev.masks_valid = 1;
 }
@@ -1831,7 +1863,7 @@ __global__ void __launch_bounds__(256) k_cg2(long long n, opc O,
 
 /* b = u* on the interior faces of the component, x = 0, r = b, p = M r */
 __global__ void k_cg_setup(const real *star, bbb_geom G, int comp, int nx,
-  int ny, int nz, opc O, const uint8_t *mask, double *x, double *r,
+  int ny, int nz, int tr, opc O, const uint8_t *mask, double *x, double *r,
   double *p, bbb_kry *s, double *partials, double rtol, int maxit)
 {
   __shared__ double sh[32 * 2];
@@ -1843,9 +1875,8 @@ __global__ void k_cg_setup(const real *star, bbb_geom G, int comp, int nx,
   double red[2] = {0., 0.};
   for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
       t += (long long)gridDim.x * blockDim.x) {
-    int i = (int)(t % nx) + 1;
-    long long rr = t / nx;
-    int j = (int)(rr % ny) + 1, k = (int)(rr / ny) + 1;
+    int i, j, k;
+    helm_ijk(t, nx, ny, tr, i, j, k);
     double bv = star[i + (long long)j * s1 + (long long)k * s2];
     x[t] = 0.;
     r[t] = bv;
@@ -1874,18 +1905,48 @@ __global__ void k_cg_setup(const real *star, bbb_geom G, int comp, int nx,
 }
 
 __global__ void k_cg_writeback(const double *x, real *star, bbb_geom G,
-  int comp, int nx, int ny, int nz)
+  int comp, int nx, int ny, int nz, int tr)
 {
   int s1 = comp == 0 ? G.fx_s1 : (comp == 1 ? G.fy_s1 : G.fz_s1);
   int s2 = comp == 0 ? G.fx_s2 : (comp == 1 ? G.fy_s2 : G.fz_s2);
   long long n = (long long)nx * ny * nz;
   for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
       t += (long long)gridDim.x * blockDim.x) {
-    int i = (int)(t % nx) + 1;
-    long long rr = t / nx;
-    int j = (int)(rr % ny) + 1, k = (int)(rr / ny) + 1;
+    int i, j, k;
+    helm_ijk(t, nx, ny, tr, i, j, k);
     star[i + (long long)j * s1 + (long long)k * s2] = x[t];
   }
+}
+
+/* The Crank-Nicolson system of velocity component `comp`: its box (the
+ * component's faces, x-fastest, or for the u system y-fastest where
+ * helm_tr says so), periodic and duplicated-face flags per box axis, and
+ * the operator weights 0.5 nu dt / h^2 along the box axes. */
+struct helm_box {
+  int nx, ny, nz, px, py, pz, dx, dy, dz, tr;
+  opc O;
+};
+
+static helm_box helm_system(int comp, const bbb_geom &G)
+{
+  helm_box h;
+  int per[3][3] = {{bc.uW, bc.uS, bc.uB}, {bc.vW, bc.vS, bc.vB}, {bc.wW, bc.wS, bc.wB}};
+  int fx = G.nx + (comp == 0), fy = G.ny + (comp == 1), fz = G.nz + (comp == 2);
+  int px = per[comp][0] == BBB_PERIODIC, py = per[comp][1] == BBB_PERIODIC;
+  double wx = 0.5 * nu * dt * (1. / (G.dx * G.dx));
+  double wy = 0.5 * nu * dt * (1. / (G.dy * G.dy));
+  h.tr = helm_tr(comp, G);
+  h.nx = h.tr ? fy : fx; h.ny = h.tr ? fx : fy; h.nz = fz;
+  h.px = h.tr ? py : px; h.py = h.tr ? px : py;
+  h.pz = per[comp][2] == BBB_PERIODIC;
+  h.dx = h.tr ? comp == 1 : comp == 0;
+  h.dy = h.tr ? comp == 0 : comp == 1;
+  h.dz = comp == 2;
+  h.O.wx = h.tr ? wy : wx;
+  h.O.wy = h.tr ? wx : wy;
+  h.O.wz = 0.5 * nu * dt * (1. / (G.dz * G.dz));
+  h.O.helm = 1;
+  return h;
 }
 
 /* ------------------------------------------------ mixed-precision CG
@@ -1898,7 +1959,7 @@ __global__ void k_cg_writeback(const double *x, real *star, bbb_geom G,
 /* b = u* (dense FP64), x = 0, ||b||; the finaliser sets up the outer
  * scalars */
 __global__ void k_helm_b(const real *star, bbb_geom G, int comp, int nx,
-  int ny, int nz, double *b, double *x, bbb_kry *s, double *partials,
+  int ny, int nz, int tr, double *b, double *x, bbb_kry *s, double *partials,
   double rtol, int max_outer)
 {
   __shared__ double sh[32];
@@ -1908,9 +1969,8 @@ __global__ void k_helm_b(const real *star, bbb_geom G, int comp, int nx,
   double red[1] = {0.};
   for(long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
       t += (long long)gridDim.x * blockDim.x) {
-    int i = (int)(t % nx) + 1;
-    long long rr = t / nx;
-    int j = (int)(rr % ny) + 1, k = (int)(rr / ny) + 1;
+    int i, j, k;
+    helm_ijk(t, nx, ny, tr, i, j, k);
     double bv = star[i + (long long)j * s1 + (long long)k * s2];
     b[t] = bv;
     x[t] = 0.;
@@ -1980,14 +2040,14 @@ __global__ void __launch_bounds__(256) k_cg_inner_setup(long long n, opc O,
 
 template <int VD, int VF>
 static int helmholtz_mixed(const boxc &BD, const boxc &BF, const opc &O,
-  const uint8_t *mask, long long n, bbb_geom G, int comp, real *star)
+  const uint8_t *mask, long long n, bbb_geom G, int comp, int tr, real *star)
 {
   ensure_fp32();
   bbb_kry *s = g_dev.kry, *si = g_dev.kry_inner;
   int max_outer = g_opt.max_outer > 0 ? g_opt.max_outer : 20;
   double itol = g_opt.inner_tol > 0 ? g_opt.inner_tol : 1e-4;
   int nx = BD.nx, ny = BD.ny, nz = BD.nz;
-  k_helm_b<<<NPW, 256, 0, g_dev.stream>>>(star, G, comp, nx, ny, nz, g_dev.kb,
+  k_helm_b<<<NPW, 256, 0, g_dev.stream>>>(star, G, comp, nx, ny, nz, tr, g_dev.kb,
     g_dev.kx, s, g_dev.partials, pp_residual, max_outer);
   BBB_LAUNCHED();
   dim3 grdD = box_grid(BD), grdF = box_grid(BF), blk(TX, TY);
@@ -2018,7 +2078,7 @@ static int helmholtz_mixed(const boxc &BD, const boxc &BF, const opc &O,
     if(g_dev.kry_host->done) break;
   }
   k_cg_writeback<<<NPW, 256, 0, g_dev.stream>>>(g_dev.kx, star, G, comp,
-    nx, ny, nz);
+    nx, ny, nz, tr);
   BBB_LAUNCHED();
   return inner_total;
 }
@@ -2030,10 +2090,9 @@ int bbb_helmholtz_solve(int comp)
   if(g_opt.precision == BBB_PREC_MIXED) {
     bbb_build_masks();
     bbb_geom G = bbb_make_geom();
-    int nx = G.nx + (comp == 0), ny = G.ny + (comp == 1), nz = G.nz + (comp == 2);
-    int per[3][3] = {{bc.uW, bc.uS, bc.uB}, {bc.vW, bc.vS, bc.vB}, {bc.wW, bc.wS, bc.wB}};
-    int px = per[comp][0] == BBB_PERIODIC, py = per[comp][1] == BBB_PERIODIC,
-        pz = per[comp][2] == BBB_PERIODIC;
+    helm_box hb = helm_system(comp, G);
+    int nx = hb.nx, ny = hb.ny, nz = hb.nz, tr = hb.tr;
+    int px = hb.px, py = hb.py, pz = hb.pz;
     int VD = pick_vec(nx, sizeof(double)), VF = pick_vec(nx, sizeof(float));
     static int smd[3], smf[3];
     if(!smd[0]) {
@@ -2041,22 +2100,18 @@ int bbb_helmholtz_solve(int comp)
       smf[1] = resident(k_cg1<float, 1>); smf[2] = resident(k_cg1<float, 4>);
       smd[0] = 1;
     }
-    boxc BD = make_box(nx, ny, nz, px, py, pz, comp == 0, comp == 1, comp == 2,
+    boxc BD = make_box(nx, ny, nz, px, py, pz, hb.dx, hb.dy, hb.dz,
       VD, smd[VD == 2 ? 2 : 1]);
-    boxc BF = make_box(nx, ny, nz, px, py, pz, comp == 0, comp == 1, comp == 2,
+    boxc BF = make_box(nx, ny, nz, px, py, pz, hb.dx, hb.dy, hb.dz,
       VF, smf[VF == 4 ? 2 : 1]);
-    opc O;
-    O.wx = 0.5 * nu * dt * (1. / (G.dx * G.dx));
-    O.wy = 0.5 * nu * dt * (1. / (G.dy * G.dy));
-    O.wz = 0.5 * nu * dt * (1. / (G.dz * G.dz));
-    O.helm = 1;
+    opc O = hb.O;
     const uint8_t *mask = comp == 0 ? g_dev.mask_u : (comp == 1 ? g_dev.mask_v : g_dev.mask_w);
     real *star = comp == 0 ? g_dev.us : (comp == 1 ? g_dev.vs : g_dev.ws);
     long long n = (long long)nx * ny * nz;
     int it;
-    if(VD == 2 && VF == 4) it = helmholtz_mixed<2, 4>(BD, BF, O, mask, n, G, comp, star);
-    else if(VD == 2) it = helmholtz_mixed<2, 1>(BD, BF, O, mask, n, G, comp, star);
-    else it = helmholtz_mixed<1, 1>(BD, BF, O, mask, n, G, comp, star);
+    if(VD == 2 && VF == 4) it = helmholtz_mixed<2, 4>(BD, BF, O, mask, n, G, comp, tr, star);
+    else if(VD == 2) it = helmholtz_mixed<2, 1>(BD, BF, O, mask, n, G, comp, tr, star);
+    else it = helmholtz_mixed<1, 1>(BD, BF, O, mask, n, G, comp, tr, star);
     bbb_kry *h = g_dev.kry_host;
     real resid = h->bnorm > 0 ? h->rnorm / h->bnorm : h->rnorm;
     g_stats.helm_iters_total += it > 0 ? it : 0;
@@ -2073,24 +2128,19 @@ int bbb_helmholtz_solve(int comp)
   }
   bbb_build_masks();
   bbb_geom G = bbb_make_geom();
-  int nx = G.nx + (comp == 0), ny = G.ny + (comp == 1), nz = G.nz + (comp == 2);
-  int per[3][3] = {{bc.uW, bc.uS, bc.uB}, {bc.vW, bc.vS, bc.vB}, {bc.wW, bc.wS, bc.wB}};
+  helm_box hb = helm_system(comp, G);
+  int nx = hb.nx, ny = hb.ny, nz = hb.nz, tr = hb.tr;
   int V = pick_vec(nx, sizeof(double));
   static int sm1 = 0, sm2 = 0;
   if(!sm1) { sm1 = resident(k_cg1<double, 1>); sm2 = resident(k_cg1<double, 2>); }
-  boxc B = make_box(nx, ny, nz, per[comp][0] == BBB_PERIODIC,
-    per[comp][1] == BBB_PERIODIC, per[comp][2] == BBB_PERIODIC,
-    comp == 0, comp == 1, comp == 2, V, V == 2 ? sm2 : sm1);
-  opc O;
-  O.wx = 0.5 * nu * dt * (1. / (G.dx * G.dx));
-  O.wy = 0.5 * nu * dt * (1. / (G.dy * G.dy));
-  O.wz = 0.5 * nu * dt * (1. / (G.dz * G.dz));
-  O.helm = 1;
+  boxc B = make_box(nx, ny, nz, hb.px, hb.py, hb.pz, hb.dx, hb.dy, hb.dz, V,
+    V == 2 ? sm2 : sm1);
+  opc O = hb.O;
   const uint8_t *mask = comp == 0 ? g_dev.mask_u : (comp == 1 ? g_dev.mask_v : g_dev.mask_w);
   real *star = comp == 0 ? g_dev.us : (comp == 1 ? g_dev.vs : g_dev.ws);
   long long n = (long long)nx * ny * nz;
   bbb_kry *s = g_dev.kry;
-  k_cg_setup<<<NPW, 256, 0, g_dev.stream>>>(star, G, comp, nx, ny, nz, O,
+  k_cg_setup<<<NPW, 256, 0, g_dev.stream>>>(star, G, comp, nx, ny, nz, tr, O,
     mask, g_dev.kx, g_dev.kr, g_dev.kp[0], s, g_dev.partials, pp_residual,
     pp_max_iter);
   BBB_LAUNCHED();
@@ -2110,7 +2160,7 @@ int bbb_helmholtz_solve(int comp)
     cur ^= 1;
   }, pp_max_iter, 1);
   k_cg_writeback<<<NPW, 256, 0, g_dev.stream>>>(g_dev.kx, star, G, comp,
-    nx, ny, nz);
+    nx, ny, nz, tr);
   BBB_LAUNCHED();
   bbb_kry *h = g_dev.kry_host;
   real resid = h->bnorm > 0 ? h->rnorm / h->bnorm : h->rnorm;

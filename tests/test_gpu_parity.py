@@ -179,3 +179,31 @@ def test_mixed_precision_vector_paths_with_particles(gpu, reliable, itol):
     finally:
         sim.close()
         orc.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_u_system_stored_y_fastest(gpu, precision):
+    """33 faces per x row but 128 cells per y row: the u Crank-Nicolson
+    system is stored y-fastest (so its passes take the 4-wide FP32 / 2-wide
+    FP64 kernels and the staged outer residual), the v, w systems and the
+    Poisson system x-fastest; fields and spheres within what the 1e-10
+    stopping rule allows of the FP64 oracle, in both precision forms."""
+    wl = configs.sedimentation((32, 128, 32), (8.0, 32.0, 8.0), 4, nu=0.1,
+                               tol=1e-10, lamb_max_iter=2, seed=9, prec=precision)
+    sim, orc, stats = _run_pair(wl, 2, options=dict(precision=precision,
+                                                     lamb_max_iter_override=2))
+    try:
+        d = sim.dom
+        for name in ("u", "v", "w", "p"):
+            e = rel_err(field_interior(d, name, sim.array(name)),
+                        field_interior(d, name, orc.field(name)))
+            assert e < 1e-7, (name, e)
+        for g, _ in stats:
+            assert g.helm_iters_total > 0
+        for pg, po in zip(sim.parts(), orc.field("parts")):
+            for k in ("x", "z", "u", "w", "Fz"):
+                a, b = getattr(pg, k), getattr(po, k)
+                assert abs(a - b) <= 1e-7 * max(1.0, abs(b)), (k, a, b)
+    finally:
+        sim.close()
+        orc.close()
