@@ -8,13 +8,15 @@
  * array one box of 10 rows x (128 + two 16-byte x-halo chunks), the mask
  * likewise, the block's own 8 rows of the arrays only it reads -- into a
  * shared-memory stage whose mbarrier completes when all bytes have landed.
- * Three stages rotate, so two planes are in flight while the block computes
- * the third; the warps synchronise only through the stages' barriers and
- * release counts, never block-wide inside a run of planes.
+ * AS_NS stages rotate, so the next plane is in flight while the block
+ * computes this one (two stages measured faster than three, four or five
+ * on 256x256x512: pass A 2%, pass B 5%, the FP64 pass B 7%); the warps
+ * synchronise only through the stages' barriers and release counts, never
+ * block-wide inside a run of planes.
  *
  * Every warp owns one tile row and computes the Jacobi-scaled stencil input
  * q for its row and for the rows just south and north of it straight from
- * the stage (no shared ring, so three stages fit twice per SM in FP32); the
+ * the stage (no shared ring, so the stages of two blocks fit per SM); the
  * row's x-halo q comes from the stage's halo chunks.  q of the plane below
  * and of the plane being stencilled stay in registers.
  *
@@ -34,7 +36,7 @@
 #include <cuda.h>
 
 #define AS_W 128
-#define AS_NS 3
+#define AS_NS 2
 #define AS_THREADS 256
 
 __host__ __device__ constexpr int as_rup(int v, int a) { return (v + a - 1) / a * a; }
@@ -427,7 +429,7 @@ __device__ __forceinline__ T as_q1(const uint8_t *h, int stride, unsigned m,
  * Per plane: wait for the stage; each warp forms q of its row (with the
  * pointwise work where the plane is the block's) and of its south / north
  * rows and x-halo cells; releases the stage (the last warp to release it
- * refills it with the plane three ahead); then the stencil and epilogue of
+ * refills it with the plane AS_NS ahead); then the stencil and epilogue of
  * the plane below, from registers. */
 template <typename T, int PASS>
 __global__ void __launch_bounds__(AS_THREADS, as_layout<T, PASS>::MINB)
@@ -555,7 +557,7 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
         }
       }
       /* release the stage: the last of the 8 warps to finish reading it
-       * refills it with the plane three ahead (no block-wide barrier, so
+       * refills it with the plane AS_NS ahead (no block-wide barrier, so
        * warps drift apart by up to the stage depth) */
       __syncwarp();
       if(tx == 0) {
