@@ -36,6 +36,20 @@ WEAK real rec_flow_field_ttime_out, rec_paraview_ttime_out,
   rec_particle_ttime_out, rec_restart_ttime_out, rec_prec_ttime_out;
 WEAK real bc_plane_pos[9];
 
+/* the rest of src/bluebottle.c's globals that the reference's own host
+ * files (src/domain.c, src/particle.c, src/vtk.c) read: the other
+ * recorder counters and the precursor's inflow planes and forcing
+ * (src/bluebottle.h:1118-1281, 1653-1791, 2347-2360).  With them those
+ * files link against this library unchanged; the library itself only
+ * carries them. */
+WEAK int rec_flow_field_stepnum_out, rec_prec_stepnum_out,
+  rec_particle_stepnum_out;
+WEAK real rec_prec_flow_field_ttime_out;
+WEAK real *u_WE, *u_SN_S, *u_SN_N, *u_BT_B, *u_BT_T;
+WEAK real *v_WE_W, *v_WE_E, *v_SN, *v_BT_B, *v_BT_T;
+WEAK real *w_WE_W, *w_WE_E, *w_SN_S, *w_SN_N, *w_BT;
+WEAK real turbA, turbl;
+
 extern bbb_options g_opt;
 void bbb_set_status(int status, const char *where);
 

@@ -13,7 +13,7 @@ OUT := $(HERE)_ref
 CC = gcc
 CFLAGS = -std=gnu99 -O2 -fPIC -fopenmp -DDOUBLE -w -I$(OUT) -I$(REF)
 
-all: $(OUT)/libref_host.so $(OUT)/libref_host_implicit.so
+all: $(OUT)/libref_host.so $(OUT)/libref_host_implicit.so $(OUT)/libref_dropin.so
 
 $(OUT)/cgnslib.h:
 	mkdir -p $(OUT)
@@ -41,3 +41,16 @@ $(OUT)/libref_host_implicit.so: $(OUT)/domain_i.o $(OUT)/particle_i.o $(OUT)/rng
 
 clean:
 	rm -f $(OUT)/*.o $(OUT)/*.so $(OUT)/ref_globals.c $(OUT)/cgnslib.h
+
+# The drop-in link: the reference's own host files (set-up, readers, the
+# VTK writer) compiled unmodified and linked against libbbb200.so, whose
+# globals they then use -- the way src/bluebottle.c's program links the
+# library.  Built after the library (python -m bluebottle_b200.build).
+LIB := $(HERE)../bluebottle_b200
+$(OUT)/%_d.o: $(REF)/%.c $(OUT)/cgnslib.h
+	$(CC) $(CFLAGS) -c $< -o $@
+
+$(OUT)/libref_dropin.so: $(OUT)/domain_d.o $(OUT)/particle_d.o $(OUT)/rng_d.o $(OUT)/vtk_d.o $(LIB)/libbbb200.so
+	$(CC) -shared -fopenmp -o $@ $(OUT)/domain_d.o $(OUT)/particle_d.o $(OUT)/rng_d.o \
+	  $(OUT)/vtk_d.o -L$(LIB) -lbbb200 -lm -Wl,--no-undefined \
+	  -Wl,-rpath,'$$ORIGIN/../../bluebottle_b200'
