@@ -29,6 +29,7 @@ sys.path.insert(0, ROOT)
 METRIC = ("timesteps/s at 256x256x512+8000 spheres, learned/FP32 vs plain "
           "FP64, same tol")
 LAMB_ITERS = 3          # Lamb sub-iterations per step, fixed for the bench
+LEARN_ITERS = 200       # Adam steps of the learned guess before timing
 
 
 def dist_env():
@@ -139,17 +140,31 @@ def workload(name, prec):
     return wl
 
 
-def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5"):
-    """One fresh simulation of the workload in precision form `prec`."""
+def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
+             learned=False):
+    """One fresh simulation of the workload in precision form `prec`.  With
+    `learned`, the warm-up steps record training crops of the first Poisson
+    solve of each step, the net is trained on them (outside the timed
+    region), and the timed steps start that solve from the gated learned
+    guess."""
     from bluebottle_b200 import Sim
     import ctypes as C
     wl = workload(wl_name, prec)
-    sim = Sim(wl, options=dict(lamb_max_iter_override=LAMB_ITERS))
+    sim = Sim(wl, options=dict(lamb_max_iter_override=LAMB_ITERS,
+                               learned_guess=1 if learned else 0))
     lib = sim.lib
     sim.prepare()
     for _ in range(warmup):
         sim.step()
     out = {}
+    if learned:
+        lib.bbb_learn_train.restype = C.c_double
+        lib.bbb_learn_train.argtypes = [C.c_int, C.c_double]
+        out["learn_crops"] = lib.bbb_learn_crops()
+        out["learn_loss"] = lib.bbb_learn_train(LEARN_ITERS, 1e-3)
+        lib.bbb_learn_enable(2)
+        sim.step()                 # one untimed step with the guess in use
+    used, ratios = 0, []
     lib.bbb_profile_reset()
     lib.bbb_profile_enable(1 if profile else 0)
     launches0 = lib.bbb_kernel_launches()
@@ -157,8 +172,14 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5"):
     lib.bbb_mark(0)
     for _ in range(steps):
         sim.step()
-        iters += sim.stats().pp_iters_total
+        st = sim.stats()
+        iters += st.pp_iters_total
+        used += st.guess_used
+        if st.extrap_r0 > 0 and st.guess_r0 > 0:
+            ratios.append(st.guess_r0 / st.extrap_r0)
     lib.bbb_mark(1)
+    out["guess_used_steps"] = used
+    out["guess_r0_ratio"] = (sum(ratios) / len(ratios)) if ratios else None
     ms = lib.bbb_mark_elapsed(0, 1)
     lib.bbb_profile_enable(0)
     out["ms"] = ms
@@ -241,6 +262,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="time the FP32 form without the learned initial guess")
     ap.add_argument("--workload", default="c5", choices=["c5", "small"],
                     help="c5: the headline 256x256x512 + 8000 spheres; small: "
                     "128x128x256 + 1000 spheres for profiler captures")
@@ -281,7 +304,8 @@ def main():
     sampler = ClockSampler(local if world > 1 else 0)
     dist.barrier()
     sampler.start()
-    mixed = run_form(1, steps, warmup, e2e_steps=steps, wl_name=args.workload)
+    mixed = run_form(1, steps, warmup, e2e_steps=steps, wl_name=args.workload,
+                     learned=not args.no_learned)
     clocks = sampler.stop()
     ms = dist.max(mixed["ms"])
     e2e_ms = dist.max(mixed["e2e_ms"])
@@ -325,6 +349,13 @@ def main():
                            "CN+Helmholtz CG, Jacobi-BiCGSTAB tol 1e-8, FP32 inner "
                            "in FP64 defect correction",
                            "lamb_iters_per_step": LAMB_ITERS,
+                           "learned_guess": None if args.no_learned else {
+                               "train_crops": mixed.get("learn_crops"),
+                               "adam_steps": LEARN_ITERS,
+                               "last_batch_rel_mse": mixed.get("learn_loss"),
+                               "steps_guess_used": mixed.get("guess_used_steps"),
+                               "guess_r0_over_extrapolation_r0":
+                                   mixed.get("guess_r0_ratio")},
                            "bicgstab_iters_per_step": mixed["pp_iters_per_step"],
                            "fp64_bicgstab_iters_per_step":
                                fp64["pp_iters_per_step"] if fp64 else None,

@@ -38,6 +38,8 @@ def main():
         ref.parts_init.restype = C.c_int
         assert ref.domain_init() == 0
         assert ref.parts_init() == 0
+        ref.binDom_init.restype = C.c_int
+        assert ref.binDom_init() == 0       # src/bluebottle.c:397-398
     else:
         assert lib.bbb_read_input(b"input") == 0
         assert lib.bbb_domain_init() == 0

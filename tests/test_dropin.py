@@ -34,7 +34,7 @@ def _case(tmp_path):
     configs.write_flow_config(str(d / "input" / "flow.config"), n=(32, 16, 24),
                               lo=(0.0, 0.0, 0.0), hi=(8.0, 4.0, 6.0), nu=0.1,
                               periodic=(True, True, False), pp_residual=1e-10,
-                              lamb_max_iter=2)
+                              lamb_max_iter=2, g=(0.0, 0.0, -1.0))
     configs.write_part_config(str(d / "input" / "part.config"),
                               [dict(r=0.8, x=3.0, y=2.0, z=3.0, rho=2.0),
                                dict(r=0.7, x=6.0, y=2.2, z=2.5, rho=2.0)])
