@@ -17,14 +17,16 @@
  *
  * Data layout: activations channels-last BF16, 16 channels = 32 bytes per
  * cell, x fastest.  Convolutions are implicit GEMMs on the 5th-generation
- * tensor cores: a tile is 128 consecutive cells of one x-row (M = 128), N =
- * 16 output channels, K = 16 input channels per tap, 27 taps accumulated in
- * TMEM (FP32).  The 9 neighbouring x-rows of the tile (+1 halo cell each
- * side) are staged once in shared memory in the no-swizzle K-major
- * core-matrix layout, so every tap's A operand is the same rows at a
- * 16-byte shifted start address.  One thread issues the 27 tcgen05.mma,
- * tcgen05.commit signals an mbarrier, and four warps read the 128x16
- * accumulator back with tcgen05.ld for the fused bias + GELU epilogue.
+ * tensor cores: a tile is 128 consecutive cells of one x-row (M = 128), K =
+ * 16 input channels, FP32 accumulators in TMEM.  A block marches along z
+ * over a tile of LG_TY rows; the rows of each plane (+1 halo cell each
+ * side, +1 halo row each side) are staged once in shared memory in the
+ * no-swizzle K-major core-matrix layout, so a dx shift is the same rows at
+ * a 16-byte shifted start address.  Each staged row meets the weights of
+ * its three dy taps in one N = 48 MMA that adds into three output rows'
+ * accumulators; one thread issues the MMAs, tcgen05.commit signals an
+ * mbarrier, and eight warps read the accumulators back with tcgen05.ld for
+ * the fused bias + GELU epilogue.
  * The backward data gradient is the same kernel with the taps flipped and
  * the channel roles swapped; the weight gradient (a reduction over cells
  * of outer products, M = 16) runs on the CUDA cores in FP32.
@@ -46,13 +48,12 @@
 #define LG_RC (LG_M + 2)          /* staged cells per row              */
 #define LG_HALF (LG_RC * 16)      /* bytes between the two K halves    */
 #define LG_ROWB (2 * LG_HALF)     /* bytes per staged row              */
-#define LG_WTAP 512               /* bytes of one tap's packed weights */
-#define LG_WLAYER (LG_T * LG_WTAP)
+#define LG_WGRP 1536              /* bytes of one (dz, dx) weight group */
+#define LG_WLAYER (9 * LG_WGRP)
 #define LG_NWL (LG_T * LG_C * LG_C)   /* weights per layer ([t][cout][cin]) */
 #define LG_NW (LG_L * LG_NWL)
 #define LG_NP (LG_NW + LG_L * LG_C)   /* weights + biases                */
-#define LG_SMEM (9 * LG_ROWB + LG_WLAYER + 64)
-#define LG_THREADS 128
+#define LG_THREADS 256
 #define LG_NIN 4                  /* live input channels              */
 #define NPW_LG 1184
 
@@ -92,8 +93,8 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo,
 }
 
 /* instruction descriptor, kind::f16: D F32, A and B BF16, both K-major,
- * N = 16, M = 128 */
-#define LG_IDESC ((1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(LG_C >> 3) << 17) \
+ * M = 128, N = 48 (three output rows of 16 channels) */
+#define LG_IDESC ((1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(48 >> 3) << 17) \
                   | ((uint32_t)(LG_M >> 4) << 24))
 
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a,
@@ -176,126 +177,259 @@ __device__ __forceinline__ int wrap_or(int g, int n, int per)
  * MODE 1: output layer: out32[cell] = conv[0] + bias[0].
  * MODE 2: backward data gradient: g = conv (flipped, transposed weights,
  *         no bias) -> act = bf16(g * gelu'(pre)) with pre the previous
- *         layer's pre-activation. */
+ *         layer's pre-activation.
+ *
+ * A block owns a tile of 128 cells (the MMA's M) x LG_TY rows and marches
+ * along z through a run of planes.  Each plane's LG_TY + 2 staged rows stay
+ * in a ring of four plane slots, so a plane is read from global memory once
+ * per tile.  The GEMM is organised around the staged rows: staged row r of
+ * input plane k - 1 + dz, shifted by dx cells, feeds output rows r - 2,
+ * r - 1 and r at once -- one M = 128, N = 48, K = 16 tcgen05.mma whose B
+ * holds the three dy taps of (dz, dx) and whose D is the 48-column window
+ * of the output plane's accumulator rows in TMEM.  9 (dz, dx) groups x
+ * (LG_TY + 2) rows = 54 MMAs per plane instead of 27 per output row, so
+ * each staged row is read from shared memory 9 times instead of 27.  The
+ * accumulator holds LG_TY + 4 rows (-2 .. LG_TY + 1, the four outside the
+ * tile are never read) in two sets: while one thread issues plane k's MMAs
+ * into one set, the eight warps stream plane k + 2 into the free ring slot
+ * with cp.async and run plane k - 1's epilogue from the other set. */
+#define LG_TY 4
+#define LG_SLOTB ((LG_TY + 2) * LG_ROWB)
+#define LG_ACC ((LG_TY + 4) * LG_C)   /* TMEM columns of one accumulator set */
+#define LG_ZSMEM (4 * LG_SLOTB + LG_WLAYER + 64)   /* 2 barriers, TMEM slot */
+
+struct lg_zbox {
+  lg_box b;
+  int nty;                        /* row groups along y                */
+  long long units, q, r;          /* (tile, plane) units, split evenly */
+  int nblk;                       /* blocks: one wave                  */
+};
+
+static lg_zbox make_lg_zbox(const lg_box &b, int nblk_max)
+{
+  lg_zbox z;
+  z.b = b;
+  z.nty = (b.ny + LG_TY - 1) / LG_TY;
+  z.units = (long long)b.ntx * z.nty * b.nz;
+  long long nb = z.units / 4 < nblk_max ? z.units / 4 : nblk_max;
+  if(nb < 1) nb = 1;
+  z.nblk = (int)nb;
+  z.q = z.units / nb;
+  z.r = z.units % nb;
+  return z;
+}
+
+__device__ __forceinline__ void lg_cp16(uint32_t dst, const void *src, int bytes)
+{
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;"
+               :: "r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+
+/* stage plane kk's LG_TY + 2 rows of tile (i0, j0) into the ring slot */
+__device__ __forceinline__ void lg_stage_plane(const lg_box &B, const bf16 *in,
+  uint32_t slot, int i0, int j0, int kk)
+{
+  int gk = wrap_or(kk, B.nz, B.pz);
+  for(int q = threadIdx.x; q < (LG_TY + 2) * LG_RC * 2; q += LG_THREADS) {
+    int ry = q / (LG_RC * 2), rem = q - ry * (LG_RC * 2);
+    int c = rem >> 1, h = rem & 1;
+    int gi = wrap_or(i0 - 1 + c, B.nx, B.px);
+    int gj = wrap_or(j0 - 1 + ry, B.ny, B.py);
+    const uint4 *src = reinterpret_cast<const uint4 *>(in);
+    int bytes = 0;
+    if(gi >= 0 && gj >= 0 && gk >= 0) {
+      long long cell = gi + (long long)B.nx * (gj + (long long)B.ny * gk);
+      src += cell * 2 + h;
+      bytes = 16;
+    }
+    lg_cp16(slot + ry * LG_ROWB + h * LG_HALF + c * 16, src, bytes);
+  }
+}
+
+/* the 9 x (LG_TY + 2) MMAs of one plane: A rows from the three ring slots
+ * (planes k - 1, k, k + 1, descriptors da[0..2] of their first staged row),
+ * B from the layer's packed (dz, dx) groups (descriptor db of group 0), D
+ * the window of accumulator rows r - 2 .. r at TMEM columns d + 16 r.  The
+ * first group's windows r = 0, 3, 6, .. start their rows from zero and go
+ * first; every other MMA accumulates.  Fully unrolled: every operand is a
+ * base descriptor plus a constant (the start address lives in the
+ * descriptor's low 14 bits, in 16-byte units). */
+__device__ __forceinline__ void lg_issue_plane(uint32_t d, const uint64_t (&da)[3],
+  uint64_t db)
+{
+#pragma unroll
+  for(int g = 0; g < 9; g++) {
+    const int dz = g / 3, dx = g % 3;
+#pragma unroll
+    for(int o = 0; o < LG_TY + 2; o++) {
+      /* group 0: rows 0, 3, .. first (fresh), then the rest */
+      const int n3 = (LG_TY + 2 + 2) / 3;
+      const int r = g > 0 ? o : (o < n3 ? 3 * o : (o - n3) + (o - n3) / 2 + 1);
+      uint64_t a = da[dz] + (uint64_t)((r * LG_ROWB + dx * 16) >> 4);
+      uint64_t b = db + (uint64_t)((g * LG_WGRP) >> 4);
+      umma_bf16(d + (uint32_t)(r * LG_C), a, b, (g == 0 && o < n3) ? 0u : 1u);
+    }
+  }
+}
+
+/* the epilogue of one plane from the accumulator set at TMEM column d:
+ * bias, activation, stores.  Warp w reads TMEM lanes 32 (w % 4) .. + 31
+ * (cells 32 (w % 4) .. of the tile, the lanes its warpgroup position may
+ * access) of rows y = w / 4, w / 4 + 2, .. (row y at columns d + 16 (y + 2)) */
 template <int MODE>
-__global__ void __launch_bounds__(LG_THREADS) k_conv_tc(lg_box B,
+__device__ __forceinline__ void lg_epilogue(const lg_box &B, uint32_t d, int i0,
+  int j0, int k, const float (&bv)[16], float *pre, bf16 *act, float *out32)
+{
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int quad = warp & 3;
+  const int i = i0 + quad * 32 + lane;
+#pragma unroll 1
+  for(int y = warp >> 2; y < LG_TY; y += LG_THREADS / 128) {
+    float v[16];
+    tmem_ld16(d + ((uint32_t)(quad * 32) << 16) + (uint32_t)((y + 2) * LG_C), v);
+    int j = j0 + y;
+    if(i >= B.nx || j >= B.ny) continue;
+    long long cell = i + (long long)B.nx * (j + (long long)B.ny * k);
+    if(MODE == 1) {
+      out32[cell] = v[0] + bv[0];
+    } else {
+      float o[16];
+      if(MODE == 0) {
+#pragma unroll
+        for(int a = 0; a < 16; a++) {
+          float z = v[a] + bv[a];
+          if(pre) pre[cell * 16 + a] = z;
+          o[a] = gelu(z);
+        }
+      } else {
+#pragma unroll
+        for(int a = 0; a < 16; a++) o[a] = v[a] * gelu_d(pre[cell * 16 + a]);
+      }
+      uint4 w0, w1;
+      uint32_t *p0 = &w0.x, *p1 = &w1.x;
+#pragma unroll
+      for(int a = 0; a < 4; a++) {
+        __nv_bfloat162 lo = __floats2bfloat162_rn(o[2 * a], o[2 * a + 1]);
+        __nv_bfloat162 hi = __floats2bfloat162_rn(o[8 + 2 * a], o[8 + 2 * a + 1]);
+        p0[a] = *reinterpret_cast<uint32_t *>(&lo);
+        p1[a] = *reinterpret_cast<uint32_t *>(&hi);
+      }
+      reinterpret_cast<uint4 *>(act)[cell * 2] = w0;
+      reinterpret_cast<uint4 *>(act)[cell * 2 + 1] = w1;
+    }
+  }
+}
+
+/* Pipeline per plane k of a run: one thread issues plane k's MMAs into
+ * accumulator set k & 1; the block waits for plane k - 1's MMAs, streams
+ * plane k + 2 into the slot plane k - 2 left, and runs plane k - 1's
+ * epilogue from the other accumulator set while plane k's MMAs execute. */
+template <int MODE>
+__global__ void __launch_bounds__(LG_THREADS, 2) k_conv_z(lg_zbox Z,
   const bf16 *__restrict__ in, const uint8_t *__restrict__ wpack,
   const float *__restrict__ bias, float *pre, bf16 *act, float *out32,
   int *err)
 {
   extern __shared__ __align__(1024) uint8_t lg_sm[];
-  uint8_t *stage = lg_sm;
-  uint8_t *wsm = lg_sm + 9 * LG_ROWB;
-  uint64_t *mbar = (uint64_t *)(wsm + LG_WLAYER);
+  const lg_box &B = Z.b;
+  uint8_t *ring = lg_sm;
+  uint8_t *wsm = lg_sm + 4 * LG_SLOTB;
+  uint64_t *mbar = (uint64_t *)(wsm + LG_WLAYER);      /* two barriers */
   uint32_t *tslot = (uint32_t *)(wsm + LG_WLAYER + 16);
-  int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  int tid = threadIdx.x, warp = tid >> 5;
 
-  /* weights of the layer into shared memory (already in UMMA layout) */
   for(int q = tid; q < LG_WLAYER / 16; q += LG_THREADS)
     reinterpret_cast<uint4 *>(wsm)[q] = reinterpret_cast<const uint4 *>(wpack)[q];
-  if(tid == 0) mbar_init(smem_u32(mbar), 1);
+  if(tid == 0) { mbar_init(smem_u32(&mbar[0]), 1); mbar_init(smem_u32(&mbar[1]), 1); }
   if(warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;"
-                 :: "r"(smem_u32(tslot)) : "memory");
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(tslot)), "n"(2 * LG_ACC) : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  uint32_t tmem = *tslot;
+  const uint32_t tmem = *tslot;
   float bv[16];
 #pragma unroll
   for(int a = 0; a < 16; a++) bv[a] = (MODE == 2 || bias == nullptr) ? 0.f : bias[a];
+  const uint32_t rbase = smem_u32(ring);
+  const uint64_t db = umma_desc(smem_u32(wsm), LG_WGRP / 2, 128);
 
-  uint32_t phase = 0;
+  uint32_t ph[2] = {0u, 0u};
   bool ok = true;
-  for(long long tile = blockIdx.x; tile < B.ntiles && ok; tile += gridDim.x) {
-    int itx = (int)(tile % B.ntx);
-    long long rest = tile / B.ntx;
-    int j = (int)(rest % B.ny), k = (int)(rest / B.ny);
-    int i0 = itx * LG_M;
-    /* stage 9 rows x 130 cells x 2 halves of 16 bytes */
-    for(int q = tid; q < 9 * LG_RC * 2; q += LG_THREADS) {
-      int r = q / (LG_RC * 2), rem = q - r * (LG_RC * 2);
-      int c = rem >> 1, h = rem & 1;
-      int dz = r / 3 - 1, dy = r % 3 - 1;
-      int gi = wrap_or(i0 - 1 + c, B.nx, B.px);
-      int gj = wrap_or(j + dy, B.ny, B.py);
-      int gk = wrap_or(k + dz, B.nz, B.pz);
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if(gi >= 0 && gj >= 0 && gk >= 0) {
-        long long cell = gi + (long long)B.nx * (gj + (long long)B.ny * gk);
-        v = reinterpret_cast<const uint4 *>(in)[cell * 2 + h];
-      }
-      *reinterpret_cast<uint4 *>(stage + r * LG_ROWB + h * LG_HALF + c * 16) = v;
-    }
+  long long bxl = blockIdx.x;
+  long long u0 = bxl * Z.q + (bxl < Z.r ? bxl : Z.r);
+  const long long u1 = u0 + Z.q + (bxl < Z.r ? 1 : 0);
+  while(u0 < u1 && ok) {
+    long long tile = u0 / B.nz;
+    int k0 = (int)(u0 - tile * B.nz);
+    long long left_ = u1 - u0;
+    int k1 = left_ < (long long)(B.nz - k0) ? k0 + (int)left_ : B.nz;
+    int i0 = (int)(tile % B.ntx) * LG_M;
+    int j0 = (int)(tile / B.ntx) * LG_TY;
+    for(int kk = k0 - 1; kk <= k0 + 1; kk++)
+      lg_stage_plane(B, in, rbase + ((kk + 4) & 3) * LG_SLOTB, i0, j0, kk);
+    asm volatile("cp.async.wait_all;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     __syncthreads();
-    if(tid == 0) {
-      tc_fence_after();
-      uint32_t sbase = smem_u32(stage), wbase = smem_u32(wsm);
-#pragma unroll 1
-      for(int t = 0; t < LG_T; t++) {
-        int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-        int r = (dz + 1) * 3 + (dy + 1);
-        uint64_t a = umma_desc(sbase + r * LG_ROWB + (dx + 1) * 16, LG_HALF, 128);
-        uint64_t b = umma_desc(wbase + t * LG_WTAP, 256, 128);
-        umma_bf16(tmem, a, b, t > 0 ? 1u : 0u);
+    for(int k = k0; k < k1; k++) {
+      const int buf = k & 1;
+      if(tid == 0) {
+        tc_fence_after();
+        uint64_t da[3];
+#pragma unroll
+        for(int dz = 0; dz < 3; dz++)
+          da[dz] = umma_desc(rbase + ((k - 1 + dz + 4) & 3) * LG_SLOTB, LG_HALF, 128);
+        lg_issue_plane(tmem + (uint32_t)(buf * LG_ACC), da, db);
+        umma_commit(smem_u32(&mbar[buf]));
       }
-      umma_commit(smem_u32(mbar));
+      __syncwarp();
+      if(k > k0) {
+        /* plane k - 1's MMAs: after them the slot of plane k - 2 is free */
+        ok = __syncthreads_and(mbar_wait(smem_u32(&mbar[buf ^ 1]), ph[buf ^ 1]) ? 1 : 0) != 0;
+        ph[buf ^ 1] ^= 1u;
+        tc_fence_after();
+      }
+      if(ok && k + 1 < k1)
+        lg_stage_plane(B, in, rbase + ((k + 2 + 4) & 3) * LG_SLOTB, i0, j0, k + 2);
+      if(ok && k > k0)
+        lg_epilogue<MODE>(B, tmem + (uint32_t)((buf ^ 1) * LG_ACC), i0, j0,
+          k - 1, bv, pre, act, out32);
+      asm volatile("cp.async.wait_all;" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      tc_fence_before();
+      __syncthreads();
+      if(!ok) break;
     }
-    __syncwarp();
-    ok = __syncthreads_and(mbar_wait(smem_u32(mbar), phase) ? 1 : 0) != 0;
-    if(!ok && tid == 0) atomicExch(err, 1);
-    phase ^= 1u;
-    tc_fence_after();
+    /* the run's last plane */
     if(ok) {
-      float v[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16), v);
-      int m = warp * 32 + lane;
-      int i = i0 + m;
-      if(i < B.nx) {
-        long long cell = i + (long long)B.nx * (j + (long long)B.ny * k);
-        if(MODE == 1) {
-          out32[cell] = v[0] + bv[0];
-        } else {
-          float o[16];
-          if(MODE == 0) {
-#pragma unroll
-            for(int a = 0; a < 16; a++) {
-              float z = v[a] + bv[a];
-              if(pre) pre[cell * 16 + a] = z;
-              o[a] = gelu(z);
-            }
-          } else {
-#pragma unroll
-            for(int a = 0; a < 16; a++) o[a] = v[a] * gelu_d(pre[cell * 16 + a]);
-          }
-          uint4 w0, w1;
-          uint32_t *p0 = &w0.x, *p1 = &w1.x;
-#pragma unroll
-          for(int a = 0; a < 4; a++) {
-            __nv_bfloat162 lo = __floats2bfloat162_rn(o[2 * a], o[2 * a + 1]);
-            __nv_bfloat162 hi = __floats2bfloat162_rn(o[8 + 2 * a], o[8 + 2 * a + 1]);
-            p0[a] = *reinterpret_cast<uint32_t *>(&lo);
-            p1[a] = *reinterpret_cast<uint32_t *>(&hi);
-          }
-          reinterpret_cast<uint4 *>(act)[cell * 2] = w0;
-          reinterpret_cast<uint4 *>(act)[cell * 2 + 1] = w1;
-        }
-      }
+      const int buf = (k1 - 1) & 1;
+      ok = __syncthreads_and(mbar_wait(smem_u32(&mbar[buf]), ph[buf]) ? 1 : 0) != 0;
+      ph[buf] ^= 1u;
+      tc_fence_after();
+      if(ok)
+        lg_epilogue<MODE>(B, tmem + (uint32_t)(buf * LG_ACC), i0, j0, k1 - 1,
+          bv, pre, act, out32);
+      tc_fence_before();
+      __syncthreads();
     }
-    tc_fence_before();
-    __syncthreads();
+    if(!ok && tid == 0) atomicExch(err, 1);
+    u0 += k1 - k0;
   }
-  /* a wait that ran out may leave an MMA in flight: give it a bounded
-   * second chance before the accumulator is released */
-  if(!ok) mbar_wait(smem_u32(mbar), phase ^ 1u);
+  /* copies are waited for above; MMAs whose wait ran out get a bounded
+   * second chance before the accumulators are released */
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  if(!ok) {
+    mbar_wait(smem_u32(&mbar[0]), ph[0]);
+    mbar_wait(smem_u32(&mbar[1]), ph[1]);
+  }
   tc_fence_after();
+  __syncthreads();
   if(warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" :: "r"(tmem)
-                 : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                 :: "r"(tmem), "n"(2 * LG_ACC) : "memory");
 }
 
 /* ------------------------------------------------ reference convolution
@@ -445,10 +579,20 @@ __global__ void k_dw_reduce(const float *partials, int nblk, float *gw,
 }
 
 /* ------------------------------------------------ parameters
- * FP32 master weights [layer][tap][cout][cin] and biases [layer][cout];
- * BF16 packs per layer in the UMMA B layout: tap t at t * 512 bytes,
- * byte (cin / 8) * 256 + cout * 16 + (cin % 8) * 2.  The transposed pack
- * of the data gradient swaps cout and cin and flips the tap (26 - t). */
+ * FP32 master weights [layer][tap][cout][cin] (tap t = 9 dz + 3 dy + dx,
+ * offsets dz - 1, dy - 1, dx - 1) and biases [layer][cout]; BF16 packs per
+ * layer in the UMMA B layout of the convolution's (dz, dx) groups: group
+ * g = 3 dz + dx at g * LG_WGRP bytes holds N = 48 rows n = 16 j + cout for
+ * the taps dy = 2 - j, K = cin, at byte (cin / 8) * 768 + n * 16 +
+ * (cin % 8) * 2.  The transposed pack of the data gradient swaps cout and
+ * cin and flips the tap (26 - t). */
+__device__ __forceinline__ int lg_pack_off(int t, int o, int c)
+{
+  int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+  int n = (2 - dy) * 16 + o;
+  return (dz * 3 + dx) * LG_WGRP + (c / 8) * (LG_WGRP / 2) + n * 16 + (c % 8) * 2;
+}
+
 __global__ void k_pack(const float *w, uint8_t *pack, uint8_t *packT)
 {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -458,9 +602,8 @@ __global__ void k_pack(const float *w, uint8_t *pack, uint8_t *packT)
   bf16 v = __float2bfloat16_rn(w[q]);
   uint8_t *P = pack + (long long)l * LG_WLAYER;
   uint8_t *PT = packT + (long long)l * LG_WLAYER;
-  *reinterpret_cast<bf16 *>(P + t * LG_WTAP + (c / 8) * 256 + o * 16 + (c % 8) * 2) = v;
-  int tt = 26 - t;
-  *reinterpret_cast<bf16 *>(PT + tt * LG_WTAP + (o / 8) * 256 + c * 16 + (o % 8) * 2) = v;
+  *reinterpret_cast<bf16 *>(P + lg_pack_off(t, o, c)) = v;
+  *reinterpret_cast<bf16 *>(PT + lg_pack_off(26 - t, c, o)) = v;
 }
 
 __global__ void k_adam(float *p, const float *g, float *m, float *v, int n,
@@ -722,9 +865,9 @@ static int lg_setup(void)
   if(!g_dev.ready) return -1;
   static int attr = 0;
   if(!attr) {
-    cudaFuncSetAttribute(k_conv_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, LG_SMEM);
-    cudaFuncSetAttribute(k_conv_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, LG_SMEM);
-    cudaFuncSetAttribute(k_conv_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, LG_SMEM);
+    cudaFuncSetAttribute(k_conv_z<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, LG_ZSMEM);
+    cudaFuncSetAttribute(k_conv_z<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, LG_ZSMEM);
+    cudaFuncSetAttribute(k_conv_z<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, LG_ZSMEM);
     attr = 1;
   }
   if(!L.rng) L.rng = 0x5DEECE66DULL;
@@ -776,11 +919,10 @@ static void lg_conv(int mode, const lg_box &B, const bf16 *in, int layer,
   const float *bias = L.w + LG_NW + layer * LG_C;
   if(!g_lg_ref) {
     const uint8_t *wp = (transposed ? L.packT : L.pack) + (long long)layer * LG_WLAYER;
-    int grid = (int)(B.ntiles < 148LL * 4 ? B.ntiles : 148LL * 4);
-    if(grid < 1) grid = 1;
-    if(mode == 0) k_conv_tc<0><<<grid, LG_THREADS, LG_SMEM, g_dev.stream>>>(B, in, wp, bias, pre, act, out32, L.err);
-    else if(mode == 1) k_conv_tc<1><<<grid, LG_THREADS, LG_SMEM, g_dev.stream>>>(B, in, wp, bias, pre, act, out32, L.err);
-    else k_conv_tc<2><<<grid, LG_THREADS, LG_SMEM, g_dev.stream>>>(B, in, wp, bias, pre, act, out32, L.err);
+    lg_zbox Z = make_lg_zbox(B, 148 * 2);
+    if(mode == 0) k_conv_z<0><<<Z.nblk, LG_THREADS, LG_ZSMEM, g_dev.stream>>>(Z, in, wp, bias, pre, act, out32, L.err);
+    else if(mode == 1) k_conv_z<1><<<Z.nblk, LG_THREADS, LG_ZSMEM, g_dev.stream>>>(Z, in, wp, bias, pre, act, out32, L.err);
+    else k_conv_z<2><<<Z.nblk, LG_THREADS, LG_ZSMEM, g_dev.stream>>>(Z, in, wp, bias, pre, act, out32, L.err);
   } else {
     /* FP32 weights: the transposed form is built on the fly by the host
      * into the gradient buffer's spare space */
