@@ -146,7 +146,10 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
     `learned`, the warm-up steps record training crops of the first Poisson
     solve of each step, the net is trained on them (outside the timed
     region), and the timed steps start that solve from the gated learned
-    guess."""
+    guess.  The evaluation itself is cost-gated (bbb_learn_enable bit 4):
+    the untimed step after training measures the guess's cost and its
+    estimated saving, and while the saving stays below the cost the guess
+    is evaluated only every 8 .. 256 steps."""
     from bluebottle_b200 import Sim
     import ctypes as C
     wl = workload(wl_name, prec)
@@ -162,9 +165,15 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
         lib.bbb_learn_train.argtypes = [C.c_int, C.c_double]
         out["learn_crops"] = lib.bbb_learn_crops()
         out["learn_loss"] = lib.bbb_learn_train(LEARN_ITERS, 1e-3)
-        lib.bbb_learn_enable(2)
+        lib.bbb_learn_enable(2 | 4)
         sim.step()                 # one untimed step with the guess in use
-    used, ratios = 0, []
+        st = sim.stats()
+        out["probe"] = dict(evaluated=st.guess_evaluated, used=st.guess_used,
+                            cost_ms=st.guess_cost_ms,
+                            benefit_ms=st.guess_benefit_ms,
+                            r0_ratio=(st.guess_r0 / st.extrap_r0
+                                      if st.extrap_r0 > 0 else None))
+    used, evaluated, ratios = 0, 0, []
     lib.bbb_profile_reset()
     lib.bbb_profile_enable(1 if profile else 0)
     launches0 = lib.bbb_kernel_launches()
@@ -175,10 +184,12 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
         st = sim.stats()
         iters += st.pp_iters_total
         used += st.guess_used
-        if st.extrap_r0 > 0 and st.guess_r0 > 0:
+        evaluated += st.guess_evaluated
+        if st.guess_evaluated and st.extrap_r0 > 0 and st.guess_r0 > 0:
             ratios.append(st.guess_r0 / st.extrap_r0)
     lib.bbb_mark(1)
     out["guess_used_steps"] = used
+    out["guess_evaluated_steps"] = evaluated
     out["guess_r0_ratio"] = (sum(ratios) / len(ratios)) if ratios else None
     ms = lib.bbb_mark_elapsed(0, 1)
     lib.bbb_profile_enable(0)
@@ -353,9 +364,12 @@ def main():
                                "train_crops": mixed.get("learn_crops"),
                                "adam_steps": LEARN_ITERS,
                                "last_batch_rel_mse": mixed.get("learn_loss"),
-                               "steps_guess_used": mixed.get("guess_used_steps"),
-                               "guess_r0_over_extrapolation_r0":
-                                   mixed.get("guess_r0_ratio")},
+                               "timed_steps_guess_evaluated":
+                                   mixed.get("guess_evaluated_steps"),
+                               "timed_steps_guess_used": mixed.get("guess_used_steps"),
+                               "timed_guess_r0_over_extrapolation_r0":
+                                   mixed.get("guess_r0_ratio"),
+                               "probe_step": mixed.get("probe")},
                            "bicgstab_iters_per_step": mixed["pp_iters_per_step"],
                            "fp64_bicgstab_iters_per_step":
                                fp64["pp_iters_per_step"] if fp64 else None,

@@ -98,7 +98,8 @@ class Stats(C.Structure):
                 ("pp_outer_last", C.c_int), ("helm_iters_total", C.c_int),
                 ("lamb_iters", C.c_int), ("lamb_err", C.c_double),
                 ("guess_used", C.c_int), ("guess_r0", C.c_double),
-                ("extrap_r0", C.c_double)]
+                ("extrap_r0", C.c_double), ("guess_evaluated", C.c_int),
+                ("guess_cost_ms", C.c_double), ("guess_benefit_ms", C.c_double)]
 
 
 PERIODIC, DIRICHLET, NEUMANN, PRECURSOR = 0, 1, 2, 3
@@ -130,7 +131,7 @@ bbb_part_state_push
 bbb_part_state_pull bbb_mark bbb_mark_elapsed bbb_PP_bicgstab_static
 bbb_learn_enable bbb_learn_train bbb_learn_crops bbb_learn_param_count
 bbb_learn_get_params bbb_learn_set_params bbb_learn_forward
-bbb_learn_use_reference_conv bbb_learn_grad""".split()
+bbb_learn_use_reference_conv bbb_learn_grad bbb_learn_gate_decide""".split()
 
 _lib = None
 
@@ -194,6 +195,8 @@ def load():
     lib.bbb_learn_set_params.argtypes = [C.POINTER(C.c_float), C.c_int]
     lib.bbb_learn_forward.argtypes = [C.c_int] * 6 + [vp, vp, C.c_int]
     lib.bbb_learn_use_reference_conv.argtypes = [C.c_int]
+    lib.bbb_learn_gate_decide.argtypes = [R] * 5 + [C.POINTER(C.c_int), C.POINTER(R)]
+    lib.bbb_learn_gate_decide.restype = C.c_int
     lib.bbb_learn_grad.argtypes = [C.c_int] * 5 + [vp, vp, C.POINTER(C.c_float)]
     lib.bbb_learn_grad.restype = R
     for name in ("cuda_ustar_helmholtz", "cuda_vstar_helmholtz",

@@ -157,6 +157,7 @@ double bbb_poisson_resid_norm(const double *x);
 /* learned initial guess (bbb_learn.cu) */
 int bbb_learn_pre_solve(void);
 void bbb_learn_post_solve(void);
+void bbb_learn_solve_done(double r_final);
 void bbb_learn_step_boundary(void);
 void bbb_learn_release(void);
 void bbb_bins_free(void);

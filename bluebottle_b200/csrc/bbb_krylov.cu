@@ -1282,6 +1282,7 @@ int bbb_poisson_solve(int record)
   g_stats.pp_iters_last = h->iter;
   g_stats.pp_resid_last = resid;
   g_stats.pp_outer_last = 1;
+  bbb_learn_solve_done(h->rnorm);
   if(record) bbb_record_solver("solver_expd.rec", h->iter, resid);
   if(h->status == BBB_ERR_NONFINITE) bbb_set_status(BBB_ERR_NONFINITE, "pressure-Poisson");
   if(!h->converged) {
@@ -1644,6 +1645,7 @@ int bbb_poisson_solve_mixed(int record)
   BBB_LAUNCHED();
   bbb_learn_post_solve();
   bbb_kry *h = g_dev.kry_host;
+  bbb_learn_solve_done(h->rnorm);
   if(h->status == BBB_ERR_NONFINITE) bbb_set_status(BBB_ERR_NONFINITE, "pressure-Poisson");
   if(!h->converged) {
     bbb_set_status(BBB_ERR_NOT_CONVERGED, "pressure-Poisson (mixed)");

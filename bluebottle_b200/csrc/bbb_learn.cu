@@ -789,6 +789,11 @@ static struct {
   int *err;
   int pending_record;
   double last_loss;
+  /* cost gate (mode bit 4) */
+  cudaEvent_t ev[4];              /* guess start/end, solve start/end   */
+  int timing;                     /* the solve after an evaluation runs */
+  double t_guess, r_ext, r_start;
+  int gate_fail, gate_skip;
 } L;
 
 template <typename T>
@@ -871,6 +876,7 @@ static int lg_setup(void)
     attr = 1;
   }
   if(!L.rng) L.rng = 0x5DEECE66DULL;
+  for(int a = 0; a < 4; a++) cudaEventCreate(&L.ev[a]);
   L.w = lg_alloc<float>(LG_NP); L.g = lg_alloc<float>(LG_NP);
   L.m = lg_alloc<float>(LG_NP); L.v = lg_alloc<float>(LG_NP);
   L.live = lg_alloc<int>(LG_NP);
@@ -979,27 +985,61 @@ void bbb_learn_step_boundary(void)
   L.first_pending = 1;
 }
 
+/* The cost gate's decision after an evaluated solve.  The guess saved
+ * about ln(r_ext / r_start) / ln(r_start / r_final) of the solve's
+ * Krylov work (the solve reduces its residual geometrically from r_start
+ * to r_final; starting from the extrapolation it would have had the
+ * extra factor r_ext / r_start to remove), so its benefit in time is that
+ * fraction of t_solve_ms.  When the benefit does not exceed the cost of
+ * evaluating the guess (features, net, the two residual norms), the next
+ * evaluations are skipped: 8 steps after the first such solve, doubling
+ * per consecutive one up to 256; a paying evaluation resets the count.
+ * Returns the number of steps to skip; *benefit_ms gets the estimate. */
+extern "C" int bbb_learn_gate_decide(double t_guess_ms, double t_solve_ms,
+  double r_ext, double r_start, double r_final, int *fails, double *benefit_ms)
+{
+  double benefit = 0.;
+  if(r_start < r_ext && r_final > 0. && r_start > r_final && t_solve_ms > 0.)
+    benefit = t_solve_ms * log(r_ext / r_start) / log(r_start / r_final);
+  if(benefit_ms) *benefit_ms = benefit;
+  if(benefit > t_guess_ms) {
+    *fails = 0;
+    return 0;
+  }
+  int f = ++*fails;
+  return 8 << (f - 1 < 5 ? f - 1 : 5);
+}
+
 /* called after b (kb), x = phi_prev (kx) are set: features, the guess and
- * the gate.  Returns 1 when the guess replaced x. */
+ * the gate.  Returns 1 when the guess replaced x.  With mode bit 4 the
+ * evaluation itself is gated on its measured cost (bbb_learn_gate_decide):
+ * the evaluation and the solve after it are timed with CUDA events. */
 int bbb_learn_pre_solve(void)
 {
   L.pending_record = 0;
   if(!L.mode || !L.first_pending) return 0;
   L.first_pending = 0;
+  int record = (L.mode & 1) != 0;
+  int use = (L.mode & 2) != 0;
+  if(use && (L.mode & 4) && L.gate_skip > 0) {
+    L.gate_skip--;
+    use = 0;
+  }
+  if(!record && !use) return 0;
   if(lg_setup() != 0) return 0;
   lg_full_buffers();
   bbb_geom G = bbb_make_geom();
   double h2 = G.dx * G.dx;
+  if(use) cudaEventRecord(L.ev[0], g_dev.stream);
   k_feat_stats<<<NPW_LG, 256, 0, g_dev.stream>>>(g_dev.phi, g_dev.kb, g_dev.p0,
     g_dev.phase, G, h2, g_dev.partials, g_dev.red_ticket + 8, L.scales);
   BBB_LAUNCHED();
-  int record = (L.mode & 1) != 0;
   k_features<<<NPW_LG, 256, 0, g_dev.stream>>>(g_dev.phi, g_dev.kb, g_dev.p0,
     g_dev.phase, G, h2, L.scales, L.feat, record ? L.phiprev : NULL);
   BBB_LAUNCHED();
   L.pending_record = record;
   int used = 0;
-  if(L.mode & 2) {
+  if(use) {
     lg_box B = make_lg_box(G.nx, G.ny, G.nz, bc.pW == BBB_PERIODIC,
       bc.pS == BBB_PERIODIC, bc.pB == BBB_PERIODIC);
     lg_forward(B, L.feat, L.act[0], L.act[1], L.act[0], NULL, L.out);
@@ -1008,11 +1048,17 @@ int bbb_learn_pre_solve(void)
     BBB_LAUNCHED();
     double r_ext = bbb_poisson_resid_norm(g_dev.kx);
     double r_gs = bbb_poisson_resid_norm(L.xc);
+    cudaEventRecord(L.ev[1], g_dev.stream);
     g_stats.extrap_r0 = r_ext;
     g_stats.guess_r0 = r_gs;
     int err = 0;
     cudaMemcpyAsync(&err, L.err, sizeof(int), cudaMemcpyDeviceToHost, g_dev.stream);
     cudaStreamSynchronize(g_dev.stream);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, L.ev[0], L.ev[1]);
+    g_stats.guess_evaluated = 1;
+    g_stats.guess_cost_ms = ms;
+    g_stats.guess_benefit_ms = 0.;
     if(err) bbb_set_status(BBB_ERR_CUDA, "learned guess: tensor-core wait ran out");
     if(!err && isfinite(r_gs) && r_gs < r_ext) {
       BBB_CK(cudaMemcpyAsync(g_dev.kx, L.xc, sizeof(double) * L.n,
@@ -1020,8 +1066,31 @@ int bbb_learn_pre_solve(void)
       g_stats.guess_used++;
       used = 1;
     }
+    if(L.mode & 4) {
+      L.timing = 1;
+      L.t_guess = ms;
+      L.r_ext = r_ext;
+      L.r_start = used ? r_gs : r_ext;
+      cudaEventRecord(L.ev[2], g_dev.stream);
+    }
   }
   return used;
+}
+
+/* called once a solve's final residual norm r_final is on the host: the
+ * gate's decision after an evaluated solve */
+void bbb_learn_solve_done(double r_final)
+{
+  if(!L.timing) return;
+  L.timing = 0;
+  cudaEventRecord(L.ev[3], g_dev.stream);
+  cudaEventSynchronize(L.ev[3]);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, L.ev[2], L.ev[3]);
+  double benefit = 0.;
+  L.gate_skip = bbb_learn_gate_decide(L.t_guess, ms, L.r_ext, L.r_start, r_final,
+    &L.gate_fail, &benefit);
+  g_stats.guess_benefit_ms = benefit;
 }
 
 /* called after the solve wrote phi: record crops of (features, target) */

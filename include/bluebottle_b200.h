@@ -238,6 +238,9 @@ typedef struct bbb_stats {
   int guess_used;          /* learned guess accepted (1) / rejected (0)    */
   real guess_r0;           /* initial residual norm from the chosen guess  */
   real extrap_r0;          /* initial residual norm of the extrapolation   */
+  int guess_evaluated;     /* the guess was computed for this step (1/0)   */
+  real guess_cost_ms;      /* device time of that evaluation               */
+  real guess_benefit_ms;   /* estimated solve time it saved (cost gate)    */
 } bbb_stats;
 void bbb_get_stats(bbb_stats *st);
 
@@ -290,7 +293,13 @@ double bbb_mark_elapsed(int a, int b);
  * residual is below the extrapolation's (counted in bbb_stats.guess_used,
  * with both initial residuals in guess_r0 / extrap_r0).
  *   bbb_learn_enable(mode): bit 1 record crops of (features, converged
- *     correction) at the first solve of each step; bit 2 use the guess.
+ *     correction) at the first solve of each step; bit 2 use the guess;
+ *     bit 4 gate the evaluation on its cost: the evaluation and the solve
+ *     after it are timed on the device, and while the guess's estimated
+ *     saving (bbb_stats.guess_benefit_ms) stays below its cost
+ *     (guess_cost_ms) it is evaluated only every 8, 16, .. 256 steps.
+ *   bbb_learn_gate_decide: that decision as a pure host function (steps
+ *     to skip; *fails counts consecutive evaluations that did not pay).
  *   bbb_learn_train(iters, lr): Adam steps on batches of 8 recorded crops;
  *     returns the relative MSE of the last batch (-1 without crops).
  *   bbb_learn_get/set_params: FP32 weights [layer][tap][cout][cin] then
@@ -301,6 +310,8 @@ double bbb_mark_elapsed(int a, int b);
  *   bbb_learn_use_reference_conv(on): route every convolution (inference
  *     and training) through the FP32 CUDA-core kernels. */
 int bbb_learn_enable(int mode);
+int bbb_learn_gate_decide(double t_guess_ms, double t_solve_ms, double r_ext,
+  double r_start, double r_final, int *fails, double *benefit_ms);
 double bbb_learn_train(int iters, double lr);
 int bbb_learn_crops(void);
 int bbb_learn_param_count(void);

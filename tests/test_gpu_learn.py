@@ -224,3 +224,37 @@ def test_online_record_train_use_keeps_parity(gpu):
     finally:
         sim.close()
         orc.close()
+
+
+def test_cost_gate_times_and_skips(gpu):
+    """Mode bit 4: the evaluated step reports the guess's device cost and
+    the estimated saving of the solve after it; when the saving does not
+    exceed the cost the next steps skip the evaluation (the solve starts
+    from phi_prev, as the reference's does), otherwise they evaluate."""
+    wl = configs.sedimentation((128, 32, 32), (32.0, 8.0, 8.0), 4, nu=0.1,
+                               tol=1e-10, lamb_max_iter=2, seed=4)
+    sim = Sim(wl, options=dict(lamb_max_iter_override=2, learned_guess=1))
+    try:
+        sim.prepare()
+        lib = sim.lib
+        for _ in range(3):
+            sim.step()
+        lib.bbb_learn_train(30, 1e-3)
+        assert lib.bbb_learn_enable(2 | 4) == 0
+        sim.step()
+        st = sim.stats()
+        assert st.guess_evaluated == 1 and st.guess_cost_ms > 0
+        assert st.guess_benefit_ms >= 0
+        if st.guess_used == 0:
+            assert st.guess_benefit_ms == 0
+        pays = st.guess_benefit_ms > st.guess_cost_ms
+        for _ in range(2):
+            sim.step()
+            st = sim.stats()
+            assert st.guess_evaluated == (1 if pays else 0)
+            if not pays:
+                assert st.guess_used == 0
+            pays = pays and st.guess_benefit_ms > st.guess_cost_ms
+        assert sim.status() == 0
+    finally:
+        sim.close()

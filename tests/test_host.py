@@ -112,3 +112,31 @@ def test_options_round_trip():
     assert g.precision == 1 and g.inner_tol == 3e-6
     lib.bbb_default_options(C.byref(o))
     lib.bbb_set_options(C.byref(o))
+
+
+def test_learned_guess_cost_gate():
+    """bbb_learn_gate_decide: the saving of a guess whose residual is a
+    factor f below the extrapolation's, in a solve that reduced its
+    residual by a factor F in t ms, is t ln f / ln F; the evaluation is
+    skipped for 8, 16, .. 256 steps while that stays below its cost."""
+    import ctypes as C
+    lib = abi.load()
+    fails, ben = C.c_int(0), C.c_double(0.)
+
+    def decide(cost, t, r_ext, r_start, r_final):
+        return lib.bbb_learn_gate_decide(cost, t, r_ext, r_start, r_final,
+                                         C.byref(fails), C.byref(ben))
+
+    # a 10x better start of a solve that removes 1e8 in 100 ms saves 12.5 ms
+    assert decide(10.0, 100.0, 1.0, 0.1, 1e-9) == 0
+    assert math.isclose(ben.value, 100.0 / 8.0) and fails.value == 0
+    # a 1.3x better start saves ~1.4 ms: skipped 8, then 16, .. up to 256 steps
+    skips = [decide(10.0, 100.0, 1.3, 1.0, 1e-8) for _ in range(8)]
+    assert skips == [8, 16, 32, 64, 128, 256, 256, 256]
+    assert math.isclose(ben.value, 100.0 * math.log(1.3) / math.log(1e8))
+    # a guess that was not used saves nothing; a paying one resets the count
+    assert decide(0.1, 100.0, 1.0, 1.0, 1e-8) == 256 and ben.value == 0.0
+    assert decide(1.0, 100.0, 1.0, 0.01, 1e-8) == 0 and fails.value == 0
+    # degenerate solves (already converged, no time) save nothing
+    assert decide(0.0, 100.0, 1.0, 1e-9, 1e-8) == 8 and ben.value == 0.0
+    assert decide(0.0, 0.0, 1.0, 0.1, 1e-8) == 16
