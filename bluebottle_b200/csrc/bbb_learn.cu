@@ -53,7 +53,8 @@
 #define LG_NWL (LG_T * LG_C * LG_C)   /* weights per layer ([t][cout][cin]) */
 #define LG_NW (LG_L * LG_NWL)
 #define LG_NP (LG_NW + LG_L * LG_C)   /* weights + biases                */
-#define LG_THREADS 256
+#define LG_EPI 256                /* staging + epilogue threads        */
+#define LG_THREADS (LG_EPI + 32)  /* + one warp that issues the MMAs   */
 #define LG_NIN 4                  /* live input channels              */
 #define NPW_LG 1184
 
@@ -230,7 +231,7 @@ __device__ __forceinline__ void lg_stage_plane(const lg_box &B, const bf16 *in,
   uint32_t slot, int i0, int j0, int kk)
 {
   int gk = wrap_or(kk, B.nz, B.pz);
-  for(int q = threadIdx.x; q < (LG_TY + 2) * LG_RC * 2; q += LG_THREADS) {
+  for(int q = threadIdx.x; q < (LG_TY + 2) * LG_RC * 2; q += LG_EPI) {
     int ry = q / (LG_RC * 2), rem = q - ry * (LG_RC * 2);
     int c = rem >> 1, h = rem & 1;
     int gi = wrap_or(i0 - 1 + c, B.nx, B.px);
@@ -284,7 +285,7 @@ __device__ __forceinline__ void lg_epilogue(const lg_box &B, uint32_t d, int i0,
   const int quad = warp & 3;
   const int i = i0 + quad * 32 + lane;
 #pragma unroll 1
-  for(int y = warp >> 2; y < LG_TY; y += LG_THREADS / 128) {
+  for(int y = warp >> 2; y < LG_TY; y += LG_EPI / 128) {
     float v[16];
     tmem_ld16(d + ((uint32_t)(quad * 32) << 16) + (uint32_t)((y + 2) * LG_C), v);
     int j = j0 + y;
@@ -320,10 +321,12 @@ __device__ __forceinline__ void lg_epilogue(const lg_box &B, uint32_t d, int i0,
   }
 }
 
-/* Pipeline per plane k of a run: one thread issues plane k's MMAs into
- * accumulator set k & 1; the block waits for plane k - 1's MMAs, streams
- * plane k + 2 into the slot plane k - 2 left, and runs plane k - 1's
- * epilogue from the other accumulator set while plane k's MMAs execute. */
+/* Pipeline per plane k of a run: one thread of the ninth warp issues plane
+ * k's MMAs into accumulator set k & 1 while the eight other warps stream
+ * plane k + 2 into the slot plane k - 2 left and run plane k - 1's
+ * epilogue from the other set; then the block waits for plane k's MMAs.
+ * The issuing warp takes no part in the epilogue, so the epilogue never
+ * waits behind the MMA issue. */
 template <int MODE>
 __global__ void __launch_bounds__(LG_THREADS, 2) k_conv_z(lg_zbox Z,
   const bf16 *__restrict__ in, const uint8_t *__restrict__ wpack,
@@ -368,15 +371,19 @@ __global__ void __launch_bounds__(LG_THREADS, 2) k_conv_z(lg_zbox Z,
     int k1 = left_ < (long long)(B.nz - k0) ? k0 + (int)left_ : B.nz;
     int i0 = (int)(tile % B.ntx) * LG_M;
     int j0 = (int)(tile / B.ntx) * LG_TY;
-    for(int kk = k0 - 1; kk <= k0 + 1; kk++)
-      lg_stage_plane(B, in, rbase + ((kk + 4) & 3) * LG_SLOTB, i0, j0, kk);
-    asm volatile("cp.async.wait_all;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if(tid < LG_EPI) {
+      for(int kk = k0 - 1; kk <= k0 + 1; kk++)
+        lg_stage_plane(B, in, rbase + ((kk + 4) & 3) * LG_SLOTB, i0, j0, kk);
+      asm volatile("cp.async.wait_all;" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
     tc_fence_before();
     __syncthreads();
     for(int k = k0; k < k1; k++) {
       const int buf = k & 1;
-      if(tid == 0) {
+      if(tid == LG_EPI) {
+        /* planes k - 1 .. k + 1 are staged and set buf is free (plane
+         * k - 2's epilogue is done): plane k's MMAs */
         tc_fence_after();
         uint64_t da[3];
 #pragma unroll
@@ -384,32 +391,28 @@ __global__ void __launch_bounds__(LG_THREADS, 2) k_conv_z(lg_zbox Z,
           da[dz] = umma_desc(rbase + ((k - 1 + dz + 4) & 3) * LG_SLOTB, LG_HALF, 128);
         lg_issue_plane(tmem + (uint32_t)(buf * LG_ACC), da, db);
         umma_commit(smem_u32(&mbar[buf]));
+      } else if(tid < LG_EPI) {
+        /* meanwhile: plane k + 2 into the slot plane k - 2 left (its last
+         * reader, plane k - 1's MMAs, completed), plane k - 1's epilogue
+         * from the other accumulator set */
+        if(k + 1 < k1)
+          lg_stage_plane(B, in, rbase + ((k + 2 + 4) & 3) * LG_SLOTB, i0, j0, k + 2);
+        if(k > k0)
+          lg_epilogue<MODE>(B, tmem + (uint32_t)((buf ^ 1) * LG_ACC), i0, j0,
+            k - 1, bv, pre, act, out32);
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       }
-      __syncwarp();
-      if(k > k0) {
-        /* plane k - 1's MMAs: after them the slot of plane k - 2 is free */
-        ok = __syncthreads_and(mbar_wait(smem_u32(&mbar[buf ^ 1]), ph[buf ^ 1]) ? 1 : 0) != 0;
-        ph[buf ^ 1] ^= 1u;
-        tc_fence_after();
-      }
-      if(ok && k + 1 < k1)
-        lg_stage_plane(B, in, rbase + ((k + 2 + 4) & 3) * LG_SLOTB, i0, j0, k + 2);
-      if(ok && k > k0)
-        lg_epilogue<MODE>(B, tmem + (uint32_t)((buf ^ 1) * LG_ACC), i0, j0,
-          k - 1, bv, pre, act, out32);
-      asm volatile("cp.async.wait_all;" ::: "memory");
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       tc_fence_before();
-      __syncthreads();
+      ok = __syncthreads_and(mbar_wait(smem_u32(&mbar[buf]), ph[buf]) ? 1 : 0) != 0;
+      ph[buf] ^= 1u;
+      tc_fence_after();
       if(!ok) break;
     }
     /* the run's last plane */
     if(ok) {
       const int buf = (k1 - 1) & 1;
-      ok = __syncthreads_and(mbar_wait(smem_u32(&mbar[buf]), ph[buf]) ? 1 : 0) != 0;
-      ph[buf] ^= 1u;
-      tc_fence_after();
-      if(ok)
+      if(tid < LG_EPI)
         lg_epilogue<MODE>(B, tmem + (uint32_t)(buf * LG_ACC), i0, j0, k1 - 1,
           bv, pre, act, out32);
       tc_fence_before();
