@@ -140,8 +140,16 @@ def workload(name, prec):
     return wl
 
 
+def profiler_range(on):
+    """cuProfilerStart / cuProfilerStop on the current context: with
+    `ncu --profile-from-start off` only the bracketed launches are seen"""
+    import ctypes as C
+    cu = C.CDLL("libcuda.so.1")
+    (cu.cuProfilerStart if on else cu.cuProfilerStop)()
+
+
 def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
-             learned=False):
+             learned=False, prof_range=False):
     """One fresh simulation of the workload in precision form `prec`.  With
     `learned`, the warm-up steps record training crops of the first Poisson
     solve of each step, the net is trained on them (outside the timed
@@ -178,6 +186,8 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
     lib.bbb_profile_enable(1 if profile else 0)
     launches0 = lib.bbb_kernel_launches()
     iters = 0                      # bbb_step resets its stats every step
+    if prof_range:
+        profiler_range(True)
     lib.bbb_mark(0)
     for _ in range(steps):
         sim.step()
@@ -188,6 +198,8 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
         if st.guess_evaluated and st.extrap_r0 > 0 and st.guess_r0 > 0:
             ratios.append(st.guess_r0 / st.extrap_r0)
     lib.bbb_mark(1)
+    if prof_range:
+        profiler_range(False)
     out["guess_used_steps"] = used
     out["guess_evaluated_steps"] = evaluated
     out["guess_r0_ratio"] = (sum(ratios) / len(ratios)) if ratios else None
@@ -275,6 +287,9 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-learned", action="store_true",
                     help="time the FP32 form without the learned initial guess")
+    ap.add_argument("--profile-range", action="store_true",
+                    help="bracket the timed steps of the FP32 form with "
+                    "cuProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--workload", default="c5", choices=["c5", "small"],
                     help="c5: the headline 256x256x512 + 8000 spheres; small: "
                     "128x128x256 + 1000 spheres for profiler captures")
@@ -316,6 +331,7 @@ def main():
     dist.barrier()
     sampler.start()
     mixed = run_form(1, steps, warmup, e2e_steps=steps, wl_name=args.workload,
+                     prof_range=args.profile_range,
                      learned=not args.no_learned)
     clocks = sampler.stop()
     ms = dist.max(mixed["ms"])
