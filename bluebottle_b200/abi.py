@@ -121,6 +121,7 @@ cuda_store_coeffs cuda_find_dt cuda_compute_energy cuda_div_U
 cuda_dom_turb_planes_push cuda_dom_turb_planes_pull cuda_compute_turb_forcing
 cuda_yank_turb_planes bbb_default_options bbb_set_options bbb_get_options
 bbb_read_input bbb_domain_init bbb_parts_init bbb_seed_particles
+bbb_write_part_config
 bbb_init_taylor_green bbb_host_free bbb_out_restart bbb_in_restart
 bbb_prepare bbb_release
 bbb_set_record_dir bbb_step bbb_advance_clock bbb_get_stats bbb_last_status
@@ -197,6 +198,8 @@ def load():
     lib.bbb_learn_use_reference_conv.argtypes = [C.c_int]
     lib.bbb_learn_gate_decide.argtypes = [R] * 5 + [C.POINTER(C.c_int), C.POINTER(R)]
     lib.bbb_learn_gate_decide.restype = C.c_int
+    lib.bbb_write_part_config.argtypes = [C.c_char_p]
+    lib.bbb_write_part_config.restype = C.c_int
     lib.bbb_learn_grad.argtypes = [C.c_int] * 5 + [vp, vp, C.POINTER(C.c_float)]
     lib.bbb_learn_grad.restype = R
     for name in ("cuda_ustar_helmholtz", "cuda_vstar_helmholtz",

@@ -698,8 +698,15 @@ int bbb_parts_init(void)
 /* ------------------------------------------------ seeded particle pack
  * Replaces src/seeder.c's unseeded generator (srand(time(NULL)),
  * src/seeder.c:234) with a reproducible one: splitmix64 stream, uniform
- * centres, rejection against every earlier sphere and its periodic images
- * through a cell list. */
+ * centres, rejection against every earlier sphere through a cell list.
+ * The placement rules are the reference seeder's: centres inside the
+ * domain less its screens bc.dsW .. bc.dsT (src/seeder.c:246-257), at
+ * least a from a non-periodic wall of that region (:259-285; here a plus
+ * half the surface gap), and a sphere's periodic images counted only along
+ * the periodic axes (:390-700, whose velocity conditions bc.uW, bc.vS,
+ * bc.wB decide).  Images are one domain length apart (the reference
+ * shifts by the screened length, which differs only where a periodic axis
+ * has a screen). */
 static uint64_t sm64(uint64_t *s)
 {
   uint64_t z = (*s += 0x9E3779B97F4A7C15ULL);
@@ -708,6 +715,35 @@ static uint64_t sm64(uint64_t *s)
   return z ^ (z >> 31);
 }
 static real urand(uint64_t *s) { return (sm64(s) >> 11) * (1.0 / 9007199254740992.0); }
+
+/* one axis of the pack: the sampled interval, the periodic length (0 when
+ * not periodic) and the cell list's cells */
+typedef struct {
+  real lo, len;          /* centres in [lo, lo + len)                  */
+  real origin, L;        /* domain start and length                    */
+  int per, nc;
+} pk_axis;
+
+static int pk_axis_init(pk_axis *ax, real xs, real xl, real ds_lo, real ds_hi,
+  int per, real wall, real dmin)
+{
+  ax->origin = xs;
+  ax->L = xl;
+  ax->per = per;
+  ax->lo = xs + ds_lo + (per ? 0. : wall);
+  ax->len = xl - ds_lo - ds_hi - (per ? 0. : 2. * wall);
+  ax->nc = (int)floor(xl / dmin);
+  if(ax->nc < 1) ax->nc = 1;
+  return ax->len > 0.;
+}
+
+static int pk_cell(const pk_axis *ax, real x)
+{
+  int c = (int)((x - ax->origin) / ax->L * ax->nc);
+  if(c < 0) c = 0;
+  if(c >= ax->nc) c = ax->nc - 1;
+  return c;
+}
 
 int bbb_seed_particles(int n, real a, real min_gap, real rho, int order,
   real rsr, unsigned long long seed)
@@ -718,48 +754,62 @@ int bbb_seed_particles(int n, real a, real min_gap, real rho, int order,
   nparts = 0;
   uint64_t s = (uint64_t)seed;
   real dmin = 2. * a + min_gap * a;
-  /* cell list with cell size >= dmin */
-  int cx = (int)floor(Dom.xl / dmin), cy = (int)floor(Dom.yl / dmin),
-      cz = (int)floor(Dom.zl / dmin);
-  if(cx < 1) cx = 1;
-  if(cy < 1) cy = 1;
-  if(cz < 1) cz = 1;
-  long ncell = (long)cx * cy * cz;
+  real wall = a + 0.5 * min_gap * a;
+  pk_axis X[3];
+  int fits = pk_axis_init(&X[0], Dom.xs, Dom.xl, bc.dsW, bc.dsE, bc.uW == BBB_PERIODIC, wall, dmin);
+  fits &= pk_axis_init(&X[1], Dom.ys, Dom.yl, bc.dsS, bc.dsN, bc.vS == BBB_PERIODIC, wall, dmin);
+  fits &= pk_axis_init(&X[2], Dom.zs, Dom.zl, bc.dsB, bc.dsT, bc.wB == BBB_PERIODIC, wall, dmin);
+  if(!fits && n > 0) {
+    bbb_set_status(BBB_ERR_CONFIG, "particle pack: no room between the walls");
+    return BBB_ERR_CONFIG;
+  }
+  long ncell = (long)X[0].nc * X[1].nc * X[2].nc;
   int *head = (int *)malloc(sizeof(int) * (size_t)ncell);
   int *next = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
   for(long c = 0; c < ncell; c++) head[c] = -1;
   long tries = 0, max_tries = 2000L * (n > 0 ? n : 1) + 100000L;
   while(nparts < n && tries < max_tries) {
     tries++;
-    real x = Dom.xs + urand(&s) * Dom.xl;
-    real y = Dom.ys + urand(&s) * Dom.yl;
-    real z = Dom.zs + urand(&s) * Dom.zl;
-    int ix = (int)((x - Dom.xs) / Dom.xl * cx), iy = (int)((y - Dom.ys) / Dom.yl * cy),
-        iz = (int)((z - Dom.zs) / Dom.zl * cz);
-    if(ix >= cx) ix = cx - 1;
-    if(iy >= cy) iy = cy - 1;
-    if(iz >= cz) iz = cz - 1;
+    real p[3];
+    int ic[3];
+    for(int d = 0; d < 3; d++) {
+      p[d] = X[d].lo + urand(&s) * X[d].len;
+      ic[d] = pk_cell(&X[d], p[d]);
+    }
     int ok = 1;
     for(int dz = -1; dz <= 1 && ok; dz++) for(int dy = -1; dy <= 1 && ok; dy++)
     for(int dx = -1; dx <= 1 && ok; dx++) {
-      int jx = ((ix + dx) % cx + cx) % cx, jy = ((iy + dy) % cy + cy) % cy,
-          jz = ((iz + dz) % cz + cz) % cz;
-      for(int q = head[jx + (long)cx * (jy + (long)cy * jz)]; q >= 0; q = next[q]) {
-        real rx = x - parts[q].x, ry = y - parts[q].y, rz = z - parts[q].z;
-        rx -= Dom.xl * round(rx / Dom.xl);
-        ry -= Dom.yl * round(ry / Dom.yl);
-        rz -= Dom.zl * round(rz / Dom.zl);
-        if(rx * rx + ry * ry + rz * rz < dmin * dmin) { ok = 0; break; }
+      int off[3] = {dx, dy, dz}, jc[3], inside = 1;
+      for(int d = 0; d < 3; d++) {
+        jc[d] = ic[d] + off[d];
+        if(X[d].per) jc[d] = (jc[d] % X[d].nc + X[d].nc) % X[d].nc;
+        else if(jc[d] < 0 || jc[d] >= X[d].nc) inside = 0;
+      }
+      /* with fewer than 3 cells along an axis the wrapped neighbours
+       * repeat: visit each cell once */
+      for(int d = 0; d < 3 && inside; d++)
+        if(X[d].per && X[d].nc < 3 && off[d] != 0 && (X[d].nc == 1 || off[d] == 1))
+          inside = 0;
+      if(!inside) continue;
+      for(int q = head[jc[0] + (long)X[0].nc * (jc[1] + (long)X[1].nc * jc[2])];
+          q >= 0; q = next[q]) {
+        real r[3] = {p[0] - parts[q].x, p[1] - parts[q].y, p[2] - parts[q].z};
+        real r2 = 0.;
+        for(int d = 0; d < 3; d++) {
+          if(X[d].per) r[d] -= X[d].L * round(r[d] / X[d].L);
+          r2 += r[d] * r[d];
+        }
+        if(r2 < dmin * dmin) { ok = 0; break; }
       }
     }
     if(!ok) continue;
     part_struct *q = &parts[nparts];
     memset(q, 0, sizeof(*q));
-    q->r = a; q->x = x; q->y = y; q->z = z;
+    q->r = a; q->x = p[0]; q->y = p[1]; q->z = p[2];
     q->rho = rho; q->E = 1.e6; q->sigma = 0.5; q->e_dry = 1.; q->coeff_fric = 0.5;
     q->order = order; q->rs = rsr;
     q->translating = 1; q->rotating = 1;
-    long cell = ix + (long)cx * (iy + (long)cy * iz);
+    long cell = ic[0] + (long)X[0].nc * (ic[1] + (long)X[1].nc * ic[2]);
     next[nparts] = head[cell];
     head[cell] = nparts;
     nparts++;
@@ -768,6 +818,49 @@ int bbb_seed_particles(int n, real a, real min_gap, real rho, int order,
   free(next);
   if(nparts < n) {
     bbb_set_status(BBB_ERR_CONFIG, "particle pack too dense for the box");
+    return BBB_ERR_CONFIG;
+  }
+  return BBB_OK;
+}
+
+/* The particle list as the reference's part.config (the layout
+ * src/seeder.c:786-815 writes and src/particle.c:79-159 reads), numbers
+ * with 17 significant digits so the file reads back to the same doubles
+ * (the reference's seeder prints %f).  path NULL or empty: the seeder's
+ * own ./input/part_seeder.config. */
+int bbb_write_part_config(const char *path)
+{
+  const char *fn = (path && path[0]) ? path : "./input/part_seeder.config";
+  FILE *f = fopen(fn, "w");
+  if(!f) {
+    bbb_set_status(BBB_ERR_CONFIG, "write_part_config: cannot create the file");
+    return BBB_ERR_CONFIG;
+  }
+  fprintf(f, "n %d\n", nparts);
+  fprintf(f, "(l/a) %.17g\n", interactionLengthRatio);
+  for(int i = 0; i < nparts; i++) {
+    const part_struct *q = &parts[i];
+    fprintf(f, "\n");
+    fprintf(f, "r %.17g\n", q->r);
+    fprintf(f, "(x, y, z) %.17g %.17g %.17g\n", q->x, q->y, q->z);
+    fprintf(f, "(aFx, aFy, aFz) %.17g %.17g %.17g\n", q->aFx, q->aFy, q->aFz);
+    fprintf(f, "(aLx, aLy, aLz) %.17g %.17g %.17g\n", q->aLx, q->aLy, q->aLz);
+    fprintf(f, "rho %.17g\n", q->rho);
+    fprintf(f, "E %.17g\n", q->E);
+    fprintf(f, "sigma %.17g\n", q->sigma);
+    fprintf(f, "e_dry %.17g\n", q->e_dry);
+    fprintf(f, "coeff_fric %.17g\n", q->coeff_fric);
+    fprintf(f, "order %d\n", q->order);
+    fprintf(f, "rs/r %.17g\n", q->rs);
+    fprintf(f, "spring_k %.17g\n", q->spring_k);
+    fprintf(f, "spring (x, y, z) %.17g %.17g %.17g\n", q->spring_x, q->spring_y,
+      q->spring_z);
+    fprintf(f, "spring_l %.17g\n", q->spring_l);
+    fprintf(f, "translating %d\n", q->translating);
+    fprintf(f, "rotating %d\n", q->rotating);
+  }
+  if(fclose(f) != 0) {
+    bbb_set_status(BBB_ERR_CONFIG, "write_part_config: write failed");
     return BBB_ERR_CONFIG;
   }
   return BBB_OK;

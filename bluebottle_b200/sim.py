@@ -152,6 +152,11 @@ class Sim:
         first when the simulation has run on the device)."""
         self._check(self.lib.bbb_out_restart(os.fsencode(path)), "out_restart")
 
+    def write_part_config(self, path):
+        """Write the particle list as the reference's part.config."""
+        self._check(self.lib.bbb_write_part_config(os.fsencode(path)),
+                    "write_part_config")
+
     def in_restart(self, path):
         """Read a restart file into the host copies (push, or prepare,
         afterwards to run from it)."""

@@ -185,12 +185,19 @@ void bbb_get_options(bbb_options *opt);
 int bbb_read_input(const char *dir);
 int bbb_domain_init(void);
 int bbb_parts_init(void);
-/* Replace the particle list by a seeded random pack: n spheres of radius a
- * at uniform non-overlapping centres with surface gap >= min_gap*a
- * (periodic images included), density rho, Lamb order `order`, rs/r = rsr.
- * Returns BBB_OK or BBB_ERR_CONFIG when the pack cannot be placed. */
+/* Replace the particle list by a seeded random pack (the reference's
+ * seeder, src/seeder.c:220, made reproducible): n spheres of radius a at
+ * uniform non-overlapping centres with surface gap >= min_gap*a (periodic
+ * images along the periodic axes included), inside the domain less its
+ * screens bc.dsW .. bc.dsT and at least a + min_gap*a/2 from a non-periodic
+ * wall; density rho, Lamb order `order`, rs/r = rsr.  Returns BBB_OK or
+ * BBB_ERR_CONFIG when the pack cannot be placed. */
 int bbb_seed_particles(int n, real a, real min_gap, real rho, int order,
   real rsr, unsigned long long seed);
+/* The particle list as the reference's part.config (src/seeder.c:786-815
+ * layout, read by src/particle.c:79), numbers to 17 digits; path NULL:
+ * ./input/part_seeder.config.  BBB_OK or BBB_ERR_CONFIG. */
+int bbb_write_part_config(const char *path);
 /* 3-D Taylor-Green start: u = U sin x cos y cos z, v = -U cos x sin y cos z,
  * w = 0 on the staggered faces (domain assumed [0, 2pi)^3 scaled). */
 void bbb_init_taylor_green(real U);

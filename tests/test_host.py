@@ -140,3 +140,110 @@ def test_learned_guess_cost_gate():
     # degenerate solves (already converged, no time) save nothing
     assert decide(0.0, 100.0, 1.0, 1e-9, 1e-8) == 8 and ben.value == 0.0
     assert decide(0.0, 0.0, 1.0, 0.1, 1e-8) == 16
+
+
+def _walled_sim(tmp_path, periodic, screens=(0.0, 0.0)):
+    """a 16 x 16 x 12 box without particles; non-periodic axes are walls,
+    the bottom/top screens (bc.dsB, bc.dsT) as given"""
+    d = str(tmp_path)
+    os.makedirs(d, exist_ok=True)
+    configs.write_flow_config(os.path.join(d, "flow.config"), n=(32, 32, 24),
+                              hi=(16.0, 16.0, 12.0), periodic=periodic)
+    configs.write_part_config(os.path.join(d, "part.config"), [])
+    sim = Sim(input_dir=d)
+    b = abi.BCStruct.in_dll(sim.lib, "bc")
+    b.dsB, b.dsT = screens
+    return sim
+
+
+def test_seeded_pack_respects_walls_screens_and_periodic_axes(tmp_path):
+    """The reference seeder's placement rules (src/seeder.c:246-700): centres
+    inside the screened domain, a (+ half the gap) from its non-periodic
+    walls, the gap counted through periodic images only along periodic
+    axes."""
+    sim = _walled_sim(tmp_path, (True, True, False), screens=(1.0, 2.0))
+    try:
+        lib = sim.lib
+        assert lib.bbb_seed_particles(120, 1.0, 0.2, 2.0, 4, 1.2, 5) == 0
+        pos = np.array([(q.x, q.y, q.z) for q in sim.parts()])
+        assert pos.shape == (120, 3)
+        wall = 1.0 + 0.1
+        assert pos[:, 2].min() >= 0.0 + 1.0 + wall - 1e-12
+        assert pos[:, 2].max() <= 12.0 - 2.0 - wall + 1e-12
+        assert np.all(pos[:, :2] >= 0) and np.all(pos[:, :2] < 16.0)
+        dd = pos[:, None, :] - pos[None, :, :]
+        dd[..., :2] -= 16.0 * np.round(dd[..., :2] / 16.0)   # x, y periodic
+        r = np.sqrt((dd ** 2).sum(-1)) + np.eye(len(pos)) * 1e9
+        assert r.min() >= 2.0 + 0.2 - 1e-12
+        # no room: centres 1.1 from both screened faces of a 2-wide slab
+        b = abi.BCStruct.in_dll(lib, "bc")
+        b.dsB, b.dsT = 5.0, 5.0
+        assert lib.bbb_seed_particles(1, 1.0, 0.2, 2.0, 4, 1.2, 5) == 3
+    finally:
+        sim.close()
+
+
+def test_pack_reproducible_with_walls(tmp_path):
+    pos = []
+    for k in range(2):
+        sim = _walled_sim(tmp_path / str(k), (False, True, False))
+        try:
+            assert sim.lib.bbb_seed_particles(80, 1.0, 0.1, 2.0, 4, 1.2, 11) == 0
+            pos.append(np.array([(q.x, q.y, q.z) for q in sim.parts()]))
+        finally:
+            sim.close()
+    assert np.array_equal(pos[0], pos[1])
+    assert pos[0][:, 0].min() >= 1.05 - 1e-12 and pos[0][:, 0].max() <= 16.0 - 1.05 + 1e-12
+
+
+def test_written_part_config_reads_back(tmp_path):
+    """bbb_write_part_config writes the reference's part.config layout; the
+    library's reader (the restatement of src/particle.c:79) and, when the
+    reference tree is here, the reference's own parts_read_input read it
+    back to the same doubles."""
+    wl = configs.sedimentation((32, 32, 32), (16.0, 16.0, 16.0), 25, seed=4)
+    sim = Sim(wl)
+    run = tmp_path / "run"
+    (run / "input").mkdir(parents=True)
+    try:
+        sim.set_scalar("interactionLengthRatio", 0.375)
+        want = [(q.r, q.x, q.y, q.z, q.rho, q.E, q.sigma, q.e_dry, q.coeff_fric,
+                 q.order, q.rs, q.translating, q.rotating) for q in sim.parts()]
+        sim.write_part_config(str(run / "input" / "part.config"))
+        configs.write_flow_config(str(run / "input" / "flow.config"), n=(32, 32, 32),
+                                  hi=(16.0, 16.0, 16.0))
+    finally:
+        sim.close()
+    text = open(run / "input" / "part.config").read()
+    assert text.startswith("n 25\n(l/a) 0.375\n\nr 1\n(x, y, z) ")
+    back = Sim(input_dir=str(run / "input"))
+    try:
+        got = [(q.r, q.x, q.y, q.z, q.rho, q.E, q.sigma, q.e_dry, q.coeff_fric,
+                q.order, q.rs, q.translating, q.rotating) for q in back.parts()]
+        assert got == want
+        assert back.scalar("interactionLengthRatio") == 0.375
+    finally:
+        back.close()
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if os.path.isdir("/root/reference/src"):
+        import subprocess
+        subprocess.run(["make", "-s", "-f", os.path.join(root, "oracle", "ref.mk"),
+                        "REF=/root/reference/src"], check=True, cwd=root)
+    ref = os.path.join(root, "oracle", "_ref", "libref_host.so")
+    if not os.path.exists(ref):
+        return
+    import ctypes as C
+    lib = C.CDLL(ref, mode=os.RTLD_LOCAL | getattr(os, "RTLD_DEEPBIND", 0))
+    cwd = os.getcwd()
+    os.chdir(run)
+    try:
+        lib.parts_read_input(0)
+    finally:
+        os.chdir(cwd)
+    assert C.c_int.in_dll(lib, "nparts").value == 25
+    assert C.c_double.in_dll(lib, "interactionLengthRatio").value == 0.375
+    pp = C.POINTER(abi.PartStruct).in_dll(lib, "parts")
+    for i, w in enumerate(want):
+        q = pp[i]
+        assert (q.r, q.x, q.y, q.z, q.rho, q.E, q.sigma, q.e_dry, q.coeff_fric,
+                q.order, q.rs, q.translating, q.rotating) == w
