@@ -671,14 +671,26 @@ __global__ void k_update_p(const real *pp0, real *pp, const real *ph,
   }
 }
 
-__global__ void k_add_const_cc(real *pp, bbb_geom G, const double *val)
+__global__ void k_add_const_cc(real *pp, bbb_geom G, int jmax, const double *val)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   int k = blockIdx.z + 1;
-  if(i > G.nx + 1 || j > G.ny) return;
+  if(i > G.nx + 1 || j > jmax) return;
   double c = -*val;
   pp[i + (long long)j * G.cc_s1 + (long long)k * G.cc_s2] += c;
+}
+
+/* rows (or planes) 1 .. the returned index that forcing_add_c_const
+ * (src/bluebottle_kernel.cu:2042) reaches under the reference's launch
+ * shape (src/cuda_bluebottle.cu:3629-3644: min(n, 16) threads,
+ * ceil(n / threads) blocks, one ghost layer of offset, bounded by the
+ * ghosted count): the interior, plus the far ghost row when n > 16 is not
+ * a multiple of 16 */
+static int add_const_cover(int n)
+{
+  int r = n < 16 ? n : (n + 15) / 16 * 16;
+  return r < n + 1 ? r : n + 1;
 }
 
 extern "C" void cuda_update_p(void)
@@ -689,8 +701,9 @@ extern "C" void cuda_update_p(void)
   k_update_p<<<592, 256, 0, g_dev.stream>>>(g_dev.p0, g_dev.p, g_dev.phi,
     g_dev.phase, G, g_dev.partials, g_dev.red_ticket, g_dev.red_dev + 8);
   BBB_LAUNCHED();
-  dim3 blk(32, 8), grd((G.nx + 2 + 31) / 32, (G.ny + 7) / 8, G.nz);
-  k_add_const_cc<<<grd, blk, 0, g_dev.stream>>>(g_dev.p, G, g_dev.red_dev + 8);
+  int jmax = add_const_cover(G.ny), kmax = add_const_cover(G.nz);
+  dim3 blk(32, 8), grd((G.nx + 2 + 31) / 32, (jmax + 7) / 8, kmax);
+  k_add_const_cc<<<grd, blk, 0, g_dev.stream>>>(g_dev.p, G, jmax, g_dev.red_dev + 8);
   BBB_LAUNCHED();
 }
 

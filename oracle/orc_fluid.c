@@ -969,10 +969,21 @@ void orc_project(orc_state *st)
   }
 }
 
+/* rows (or planes) 1 .. the returned index that forcing_add_c_const
+ * (src/bluebottle_kernel.cu:2042) reaches under the launch shape of
+ * src/cuda_bluebottle.cu:3629-3644: min(n, 16) threads, ceil(n / threads)
+ * blocks, offset by the one ghost layer and bounded by the ghosted count
+ * -- the interior, plus the far ghost row when n > 16 is not a multiple
+ * of 16 */
+static int add_const_cover(int n)
+{
+  int r = n < 16 ? n : (n + 15) / 16 * 16;
+  return r < n + 1 ? r : n + 1;
+}
+
 /* src/cuda_bluebottle.cu:3616-3671, src/bluebottle_kernel.cu:1326-1338 and
- * forcing_add_c_const :2042, which under its launch shape (row and plane
- * counts multiples of 16) reaches the interior rows and planes, all
- * columns; ghosts are rewritten by the pressure BC before any read */
+ * forcing_add_c_const :2042 (all columns, the rows and planes
+ * add_const_cover names) */
 void orc_update_p(orc_state *st)
 {
   const grid_info *G = &st->dom.Gcc;
@@ -986,7 +997,8 @@ void orc_update_p(orc_state *st)
   for(int k = G->ks; k < G->ke; k++) for(int j = G->js; j < G->je; j++)
   for(int i = G->is; i < G->ie; i++) sum += st->p[CCI(*G, i, j, k)];
   real mean = sum / G->s3;
-  for(int k = G->ks; k < G->ke; k++) for(int j = G->js; j < G->je; j++)
+  int jmax = add_const_cover(G->jn), kmax = add_const_cover(G->kn);
+  for(int k = 1; k <= kmax; k++) for(int j = 1; j <= jmax; j++)
   for(int i = G->isb; i < G->ieb; i++) st->p[CCI(*G, i, j, k)] += -mean;
 }
 

@@ -54,3 +54,27 @@ $(OUT)/libref_dropin.so: $(OUT)/domain_d.o $(OUT)/particle_d.o $(OUT)/rng_d.o $(
 	$(CC) -shared -fopenmp -o $@ $(OUT)/domain_d.o $(OUT)/particle_d.o $(OUT)/rng_d.o \
 	  $(OUT)/vtk_d.o -L$(LIB) -lbbb200 -lm -Wl,--no-undefined \
 	  -Wl,-rpath,'$$ORIGIN/../../bluebottle_b200'
+
+# The reference's own CUDA files -- all but src/cuda_bicgstab.cu (it needs
+# CUSP, which the reference does not ship) and src/cuda_testing.cu --
+# compiled unmodified for sm_100a and linked with the host set-up above
+# into oracle/_ref/libref_gpu.so: the reference's GPU kernels behind its
+# own cuda_* entry points, the checker of this library's non-solver entry
+# points (tests/test_gpu_refkernels.py).  `make -f oracle/ref.mk gpu`.
+NVCC = nvcc
+NVFLAGS = -gencode arch=compute_100a,code=sm_100a -O2 -DDOUBLE -w \
+  -Xcompiler -fPIC,-fopenmp -I$(OUT) -I$(REF)
+CUSRC = bluebottle_kernel particle_kernel quadrature_kernel entrySearch_kernel \
+  cuda_bluebottle cuda_particle cuda_quadrature entrySearch
+
+$(OUT)/%_g.o: $(REF)/%.cu $(OUT)/cgnslib.h
+	$(NVCC) $(NVFLAGS) -c $< -o $@
+
+$(OUT)/libref_gpu.so: $(CUSRC:%=$(OUT)/%_g.o) $(OUT)/domain.o $(OUT)/particle.o \
+  $(OUT)/rng.o $(OUT)/ref_globals.o
+	$(NVCC) -gencode arch=compute_100a,code=sm_100a -shared -Xcompiler -fopenmp \
+	  -o $@ $^ -lgomp -Xlinker --no-undefined
+
+gpu: $(OUT)/libref_gpu.so
+
+.PHONY: all clean gpu

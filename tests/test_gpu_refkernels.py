@@ -1,0 +1,81 @@
+"""This library's non-solver cuda_* entry points against the reference's own
+CUDA kernels: the reference's src/*.cu (all but src/cuda_bicgstab.cu, which
+needs CUSP) compiled unmodified for sm_100a into oracle/_ref/libref_gpu.so
+(oracle/ref.mk, target gpu) and run side by side with the library in a
+child process (tests/refgpu_child.py) through the explicit time step of
+src/bluebottle.c:603-708 without its two solves.  Every stage starts from
+bit-identical host state on both sides; the reference's flag arrays, which
+its cuda_part_pull copies only in a -DDDEBUG build, are read from its device
+pointers.  Each stage must change something on the reference side (so an
+entry point that did nothing on both sides cannot pass).
+
+Tolerances: integer masks and cage indices are equal; FP64 results agree to
+a few ulps of the largest value (the library sums in other orders: fused
+stencils, warp reductions).  The reference's compute_error races between
+particles (its scratch rows overlap), so the Lamb error it returns is
+compared loosely."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+from bluebottle_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REFSRC = "/root/reference/src"
+REFGPU = os.path.join(ROOT, "oracle", "_ref", "libref_gpu.so")
+
+REL = 1e-12          # FP64 agreement, relative to the largest magnitude
+
+
+def _ensure():
+    if os.path.isdir(REFSRC):
+        subprocess.run(["make", "-s", "-j8", "-f", os.path.join(ROOT, "oracle", "ref.mk"),
+                        "REF=" + REFSRC, "gpu"], check=True, cwd=ROOT)
+    if not os.path.exists(REFGPU):
+        pytest.skip("oracle/_ref/libref_gpu.so was not built (needs the reference tree)")
+
+
+def _case(tmp_path):
+    d = tmp_path / "run"
+    (d / "input").mkdir(parents=True)
+    configs.write_flow_config(str(d / "input" / "flow.config"), n=(32, 16, 24),
+                              lo=(0.0, 0.0, 0.0), hi=(8.0, 4.0, 6.0), nu=0.1,
+                              periodic=(True, True, False), pp_residual=1e-10,
+                              lamb_max_iter=2, g=(0.0, 0.0, -1.0))
+    configs.write_part_config(str(d / "input" / "part.config"),
+                              [dict(r=0.8, x=3.0, y=2.0, z=3.0, rho=2.0),
+                               dict(r=0.7, x=6.0, y=2.2, z=2.5, rho=2.0),
+                               dict(r=0.6, x=1.2, y=0.9, z=4.4, rho=2.0)])
+    return d
+
+
+def test_entry_points_match_reference_kernels(gpu, tmp_path):
+    _ensure()
+    run = _case(tmp_path)
+    out = tmp_path / "diff.json"
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "tests", "refgpu_child.py"),
+                        str(run), str(out)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    res = json.load(open(out))
+    bad = []
+    for stage, arrays in res.items():
+        # the stage ran: it changed something on the reference side
+        moved = [e.get("moved", 0.0) for e in arrays.values()]
+        if stage not in ("find_dt",) and max(moved) == 0:
+            bad.append((stage, "nothing changed"))
+        for name, e in arrays.items():
+            if e["kind"] == "int":
+                ok = e["d"] == 0
+            elif name == "return.cuda_lamb_err":
+                ok = True
+            else:
+                ok = e["d"] <= REL * max(e["mag"], 1e-300)
+            if not ok:
+                bad.append((stage, name, e))
+    print(json.dumps(res))
+    assert not bad, bad
