@@ -40,23 +40,38 @@ def _ensure():
         pytest.skip("oracle/_ref/libref_gpu.so was not built (needs the reference tree)")
 
 
-def _case(tmp_path):
+CASES = {
+    # z walls, 3 spheres
+    "walls_z": dict(flow=dict(n=(32, 16, 24), hi=(8.0, 4.0, 6.0), periodic=(True, True, False)),
+                    parts=[dict(r=0.8, x=3.0, y=2.0, z=3.0), dict(r=0.7, x=6.0, y=2.2, z=2.5),
+                           dict(r=0.6, x=1.2, y=0.9, z=4.4)]),
+    # triply periodic, spheres across the west, south and top faces
+    "periodic": dict(flow=dict(n=(24, 20, 18), hi=(6.0, 5.0, 4.5), periodic=(True, True, True)),
+                     parts=[dict(r=0.7, x=0.3, y=2.5, z=2.0), dict(r=0.6, x=3.0, y=0.2, z=2.2),
+                            dict(r=0.65, x=4.2, y=3.4, z=4.3), dict(r=0.5, x=2.0, y=4.0, z=0.9)]),
+    # x and y walls, an odd cell count along x
+    "walls_xy": dict(flow=dict(n=(21, 24, 16), hi=(5.25, 6.0, 4.0), periodic=(False, False, True)),
+                     parts=[dict(r=0.7, x=1.0, y=1.1, z=2.0), dict(r=0.6, x=4.0, y=4.5, z=0.4),
+                            dict(r=0.5, x=2.6, y=3.0, z=3.0)]),
+}
+
+
+def _case(tmp_path, name):
+    c = CASES[name]
     d = tmp_path / "run"
     (d / "input").mkdir(parents=True)
-    configs.write_flow_config(str(d / "input" / "flow.config"), n=(32, 16, 24),
-                              lo=(0.0, 0.0, 0.0), hi=(8.0, 4.0, 6.0), nu=0.1,
-                              periodic=(True, True, False), pp_residual=1e-10,
-                              lamb_max_iter=2, g=(0.0, 0.0, -1.0))
+    configs.write_flow_config(str(d / "input" / "flow.config"), lo=(0.0, 0.0, 0.0),
+                              nu=0.1, pp_residual=1e-10, lamb_max_iter=2,
+                              g=(0.0, 0.0, -1.0), **c["flow"])
     configs.write_part_config(str(d / "input" / "part.config"),
-                              [dict(r=0.8, x=3.0, y=2.0, z=3.0, rho=2.0),
-                               dict(r=0.7, x=6.0, y=2.2, z=2.5, rho=2.0),
-                               dict(r=0.6, x=1.2, y=0.9, z=4.4, rho=2.0)])
+                              [dict(q, rho=2.0) for q in c["parts"]])
     return d
 
 
-def test_entry_points_match_reference_kernels(gpu, tmp_path):
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_entry_points_match_reference_kernels(gpu, tmp_path, case):
     _ensure()
-    run = _case(tmp_path)
+    run = _case(tmp_path, case)
     out = tmp_path / "diff.json"
     r = subprocess.run([sys.executable, os.path.join(ROOT, "tests", "refgpu_child.py"),
                         str(run), str(out)], capture_output=True, text=True, timeout=600)
