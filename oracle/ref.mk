@@ -65,13 +65,18 @@ NVCC = nvcc
 NVFLAGS = -gencode arch=compute_100a,code=sm_100a -O2 -DDOUBLE -w \
   -Xcompiler -fPIC,-fopenmp -I$(OUT) -I$(REF)
 CUSRC = bluebottle_kernel particle_kernel quadrature_kernel entrySearch_kernel \
-  cuda_bluebottle cuda_particle cuda_quadrature entrySearch
+  cuda_bluebottle cuda_particle cuda_quadrature entrySearch bicgstab_kernel
 
 $(OUT)/%_g.o: $(REF)/%.cu $(OUT)/cgnslib.h
 	$(NVCC) $(NVFLAGS) -c $< -o $@
 
-$(OUT)/libref_gpu.so: $(CUSRC:%=$(OUT)/%_g.o) $(OUT)/domain.o $(OUT)/particle.o \
-  $(OUT)/rng.o $(OUT)/ref_globals.o
+# the assembly half of src/cuda_bicgstab.cu's pressure solve, restated
+# (the other half is CUSP)
+$(OUT)/ref_pp_shim.o: $(HERE)ref_pp_shim.cu $(OUT)/cgnslib.h
+	$(NVCC) $(NVFLAGS) -c $< -o $@
+
+$(OUT)/libref_gpu.so: $(CUSRC:%=$(OUT)/%_g.o) $(OUT)/ref_pp_shim.o $(OUT)/domain.o \
+  $(OUT)/particle.o $(OUT)/rng.o $(OUT)/ref_globals.o
 	$(NVCC) -gencode arch=compute_100a,code=sm_100a -shared -Xcompiler -fopenmp \
 	  -o $@ $^ -lgomp -Xlinker --no-undefined
 

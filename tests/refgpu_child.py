@@ -171,6 +171,57 @@ def compare(ref, ours, before, before_parts, parts=False):
     return res
 
 
+def dia_apply(A, off, x):
+    """y = A x for the 13-diagonal matrix in CUSP's dia layout"""
+    n = x.size
+    y = np.zeros(n)
+    for d, o in enumerate(off):
+        lo, hi = max(0, -o), min(n, n - o)
+        if lo < hi:
+            y[lo:hi] += A[d, lo:hi] * x[lo + o:hi + o]
+    return y
+
+
+def pp_system(ref, ours):
+    """This library's pressure solve (cuda_PP_bicgstab) against the system
+    the reference's own kernels assemble from the same state: the relative
+    residual of the library's phi in the reference's system, after the
+    constant shift the mean removal applied (fitted by least squares), and
+    the same for the starting phi (that the system is not trivial)."""
+    copy_state(ref, ours)
+    ref.push()
+    ours.push()
+    g = ours.dom.Gcc
+    inner = (slice(g.ks, g.ke), slice(g.js, g.je), slice(getattr(g, "is"), g.ie))
+    shape = (g.knb, g.jnb, g.inb)
+    x0 = ours.arr("phi", "Gcc").reshape(shape)[inner].ravel().copy()
+    ours.call("cuda_PP_bicgstab", C.c_int(0))
+    ours.pull()
+    x = ours.arr("phi", "Gcc").reshape(shape)[inner].ravel().copy()
+    n = ref.call("refshim_pp_rows", restype=C.c_int)
+    assert n == x.size, (n, x.size)
+    off = (C.c_int * 13)()
+    ref.call("refshim_pp_offsets", off)
+    A = np.zeros((13, n))
+    b = np.zeros(n)
+    rc = ref.call("refshim_pp_system", A.ctypes.data_as(C.c_void_p),
+                  b.ctypes.data_as(C.c_void_p), restype=C.c_int)
+    assert rc == 0, ("refshim_pp_system", rc)
+    a1 = dia_apply(A, list(off), np.ones(n))
+
+    def rel(v):
+        r = b - dia_apply(A, list(off), v)
+        c = float(a1 @ r) / float(a1 @ a1) if float(a1 @ a1) > 0 else 0.0
+        return float(np.linalg.norm(r - c * a1) / max(np.linalg.norm(b), 1e-300))
+
+    st = abi.Stats()
+    ours.lib.bbb_get_stats(C.byref(st))
+    return {"rel_resid": rel(x), "rel_resid_start": rel(x0),
+            "b_norm": float(np.linalg.norm(b)), "kind": "system",
+            "iterations": st.pp_iters_last,
+            "identity_rows": int(np.sum(A[6] == 1.0))}
+
+
 def main():
     run, out = sys.argv[1], sys.argv[2]
     lib = abi.load()
@@ -250,6 +301,7 @@ def main():
     stage("U_star_2", ["cuda_U_star_2"])
     stage("part_BC_star", ["cuda_part_BC_star", "cuda_dom_BC_star"])
     stage("solvability", ["cuda_solvability"])
+    res["PP_system"] = pp_system(ref, ours)
     stage("project", ["cuda_dom_BC_phi", "cuda_project"])
     stage("part_BC", ["cuda_part_BC", "cuda_dom_BC"])
     stage("update_p", ["cuda_update_p"])
