@@ -510,8 +510,14 @@ __device__ __forceinline__ void helm_ijk(long long t, int X, int Y, int tr,
   j = (tr ? a : b) + 1;
 }
 
+/* dlo / dhi: the component's first / last face along its own axis is a
+ * Dirichlet wall, whose rows are identity rows (the reference's
+ * {u,v,w}star_coeffs_dirichlet_{W,E,S,N,B,T} for the wall normal to the
+ * component, src/bicgstab_kernel.cu:946-1003, 1119-1176, 1291-1348; the
+ * tangential walls' kernels zero couplings the face flags already drop) */
 __global__ void k_mask_face(const int *fu, const int *fv, const int *fw,
-  bbb_geom G, int comp, int nx, int ny, int nz, int tr, uint8_t *mask)
+  bbb_geom G, int comp, int nx, int ny, int nz, int tr, int dlo, int dhi,
+  uint8_t *mask)
 {
   long long n = (long long)nx * ny * nz;
   const int *fs = comp == 0 ? fu : (comp == 1 ? fv : fw);
@@ -532,6 +538,9 @@ __global__ void k_mask_face(const int *fu, const int *fv, const int *fw,
     m |= fw[Bq] != 0 ? BBB_MB : 0;
     m |= fw[Bq + G.fz_s2] != 0 ? BBB_MT : 0;
     if(fs[i + (long long)j * s1 + (long long)k * s2] < 0) m |= BBB_MID;
+    const int a = comp == 0 ? i : (comp == 1 ? j : k);
+    const int amax = comp == 0 ? G.nx + 1 : (comp == 1 ? G.ny + 1 : G.nz + 1);
+    if((dlo && a == 1) || (dhi && a == amax)) m |= BBB_MID;
     if(tr) {
       /* the box's W/E faces are the grid's S/N and the other way round */
       uint8_t q = m & (BBB_MB | BBB_MT | BBB_MID);
@@ -563,13 +572,15 @@ void bbb_build_masks(void)
   int tu = helm_tr(0, G);
   k_mask_face<<<NPW, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
     g_dev.flag_w, G, 0, tu ? G.ny : G.nx + 1, tu ? G.nx + 1 : G.ny, G.nz, tu,
-    g_dev.mask_u);
+    bc.uW == BBB_DIRICHLET, bc.uE == BBB_DIRICHLET, g_dev.mask_u);
   BBB_LAUNCHED();
   k_mask_face<<<NPW, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
-    g_dev.flag_w, G, 1, G.nx, G.ny + 1, G.nz, 0, g_dev.mask_v);
+    g_dev.flag_w, G, 1, G.nx, G.ny + 1, G.nz, 0,
+    bc.vS == BBB_DIRICHLET, bc.vN == BBB_DIRICHLET, g_dev.mask_v);
   BBB_LAUNCHED();
   k_mask_face<<<NPW, 256, 0, g_dev.stream>>>(g_dev.flag_u, g_dev.flag_v,
-    g_dev.flag_w, G, 2, G.nx, G.ny, G.nz + 1, 0, g_dev.mask_w);
+    g_dev.flag_w, G, 2, G.nx, G.ny, G.nz + 1, 0,
+    bc.wB == BBB_DIRICHLET, bc.wT == BBB_DIRICHLET, g_dev.mask_w);
   BBB_LAUNCHED();
   g_dev.masks_valid = 1;
 }

@@ -675,6 +675,27 @@ void orc_star_helmholtz(orc_state *st, int comp)
       A.val[0 * n + C] -= cz; A.val[11 * n + C] += cz;
     }
   }
+  /* Dirichlet walls (src/bicgstab_kernel.cu:946-1348, launched by
+   * src/cuda_bicgstab.cu:213-260 and the v, w counterparts): the wall
+   * normal to the component turns its face rows into identity rows; a
+   * tangential wall drops the coupling across it */
+  int dir[6] = {perW == BBB_DIRICHLET, perE == BBB_DIRICHLET, perS == BBB_DIRICHLET,
+                perN == BBB_DIRICHLET, perB == BBB_DIRICHLET, perT == BBB_DIRICHLET};
+  for(int k = 0; k < G->kn; k++) for(int j = 0; j < G->jn; j++)
+  for(int i = 0; i < G->in; i++) {
+    long C = i + (long)j * G->s1 + (long)k * G->s2;
+    int at[6] = {i == 0, i == G->in - 1, j == 0, j == G->jn - 1, k == 0, k == G->kn - 1};
+    static const int cross[6] = {5, 7, 3, 9, 1, 11};
+    for(int f = 0; f < 6; f++) {
+      if(!dir[f] || !at[f]) continue;
+      if(f / 2 == comp) {
+        for(int dd = 0; dd < 13; dd++) A.val[dd * n + C] = 0.;
+        A.val[6 * n + C] = 1.;
+      } else {
+        A.val[cross[f] * n + C] = 0.;
+      }
+    }
+  }
   /* particle identity rows (src/bicgstab_kernel.cu:730-827) */
   for(int k = G->ks; k < G->ke; k++)
   for(int j = G->js; j < G->je; j++)

@@ -222,6 +222,39 @@ def pp_system(ref, ours):
             "identity_rows": int(np.sum(A[6] == 1.0))}
 
 
+def helm_system(ref, ours, comp):
+    """This library's Crank-Nicolson Helmholtz solve (cuda_{u,v,w}star_
+    helmholtz) against the system the reference's own kernels assemble from
+    the same state: the relative residual of the library's u* in it."""
+    copy_state(ref, ours)
+    ref.push()
+    ours.push()
+    name, grid = (("u_star", "Gfx"), ("v_star", "Gfy"), ("w_star", "Gfz"))[comp]
+    g = getattr(ours.dom, grid)
+    inner = (slice(g.ks, g.ke), slice(g.js, g.je), slice(getattr(g, "is"), g.ie))
+    shape = (g.knb, g.jnb, g.inb)
+    ours.call("cuda_%sstar_helmholtz" % "uvw"[comp], C.c_int(0))
+    ours.pull()
+    x = ours.arr(name, grid).reshape(shape)[inner].ravel().copy()
+    n = ref.call("refshim_helm_rows", C.c_int(comp), restype=C.c_int)
+    assert n == x.size, (n, x.size)
+    off = (C.c_int * 13)()
+    ref.call("refshim_helm_offsets", C.c_int(comp), off)
+    A = np.zeros((13, n))
+    b = np.zeros(n)
+    rc = ref.call("refshim_helm_system", C.c_int(comp), A.ctypes.data_as(C.c_void_p),
+                  b.ctypes.data_as(C.c_void_p), restype=C.c_int)
+    assert rc == 0, ("refshim_helm_system", rc)
+    r = b - dia_apply(A, list(off), x)
+    bn = max(float(np.linalg.norm(b)), 1e-300)
+    st = abi.Stats()
+    ours.lib.bbb_get_stats(C.byref(st))
+    return {"rel_resid": float(np.linalg.norm(r)) / bn,
+            "solution_vs_rhs": float(np.linalg.norm(x - b)) / bn,
+            "b_norm": bn, "identity_rows": int(np.sum(A[6] == 1.0)),
+            "cg_iterations": st.helm_iters_total}
+
+
 def main():
     run, out = sys.argv[1], sys.argv[2]
     lib = abi.load()
@@ -298,7 +331,20 @@ def main():
     # src/bluebottle.c:603-708, the explicit step without the two solves
     stage("build_cages", ["cuda_build_cages"], parts=True)
     stage("dom_BC", ["cuda_dom_BC"])
+    # the forcing fields live on the device only: both sides compute them
+    # from the same clock and ramps (src/cuda_bluebottle.cu:3674), then the
+    # right-hand sides below use them
+    for s in (ref, ours):
+        f = s.lib.cuda_compute_forcing
+        f.restype = None
+        f(C.byref(C.c_double.in_dll(s.lib, "pid_int")),
+          C.byref(C.c_double.in_dll(s.lib, "pid_back")),
+          C.c_double(C.c_double.in_dll(s.lib, "Kp").value),
+          C.c_double(C.c_double.in_dll(s.lib, "Ki").value),
+          C.c_double(C.c_double.in_dll(s.lib, "Kd").value))
     stage("U_star_2", ["cuda_U_star_2"])
+    for comp in range(3):
+        res["helmholtz_%s" % "uvw"[comp]] = helm_system(ref, ours, comp)
     stage("part_BC_star", ["cuda_part_BC_star", "cuda_dom_BC_star"])
     stage("solvability", ["cuda_solvability"])
     res["PP_system"] = pp_system(ref, ours)

@@ -3,9 +3,10 @@ CUDA kernels: the reference's src/*.cu (all but src/cuda_bicgstab.cu, which
 needs CUSP) compiled unmodified for sm_100a into oracle/_ref/libref_gpu.so
 (oracle/ref.mk, target gpu) and run side by side with the library in a
 child process (tests/refgpu_child.py) through the explicit time step of
-src/bluebottle.c:603-708; its pressure solve is checked against the system
-the reference's own kernels assemble (oracle/ref_pp_shim.cu restates the
-assembly half of src/cuda_bicgstab.cu's solve, whose other half is CUSP).  Every stage starts from
+src/bluebottle.c:603-708; its pressure solve and the three Crank-Nicolson
+Helmholtz solves are checked against the systems the reference's own
+kernels assemble (oracle/ref_pp_shim.cu restates the assembly half of
+src/cuda_bicgstab.cu's solves, whose other half is CUSP).  Every stage starts from
 bit-identical host state on both sides; the reference's flag arrays, which
 its cuda_part_pull copies only in a -DDDEBUG build, are read from its device
 pointers.  Each stage must change something on the reference side (so an
@@ -87,6 +88,13 @@ def test_entry_points_match_reference_kernels(gpu, tmp_path, case):
     print("PP_system", json.dumps(pp))
     if not (pp["rel_resid"] <= 3e-10 and pp["rel_resid_start"] > 1e-6):
         bad.append(("PP_system", pp))
+    # the Crank-Nicolson Helmholtz solves against the reference's assembled
+    # u*, v*, w* systems (src/cuda_bicgstab.cu:44-712), same tolerance
+    for c in "uvw":
+        h = res.pop("helmholtz_" + c)
+        print("helmholtz_" + c, json.dumps(h))
+        if not (h["rel_resid"] <= 3e-10 and h["solution_vs_rhs"] > 1e-8):
+            bad.append(("helmholtz_" + c, h))
     for stage, arrays in res.items():
         # the stage ran: it changed something on the reference side
         moved = [e.get("moved", 0.0) for e in arrays.values()]
