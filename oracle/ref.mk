@@ -80,6 +80,18 @@ $(OUT)/libref_gpu.so: $(CUSRC:%=$(OUT)/%_g.o) $(OUT)/ref_pp_shim.o $(OUT)/domain
 	$(NVCC) -gencode arch=compute_100a,code=sm_100a -shared -Xcompiler -fopenmp \
 	  -o $@ $^ -lgomp -Xlinker --no-undefined
 
-gpu: $(OUT)/libref_gpu.so
+# the same, built as the Crank-Nicolson (-DIMPLICIT) program
+$(OUT)/%_gi.o: $(REF)/%.cu $(OUT)/cgnslib.h
+	$(NVCC) $(NVFLAGS) -DIMPLICIT -c $< -o $@
+
+$(OUT)/ref_pp_shim_i.o: $(HERE)ref_pp_shim.cu $(OUT)/cgnslib.h
+	$(NVCC) $(NVFLAGS) -DIMPLICIT -c $< -o $@
+
+$(OUT)/libref_gpu_implicit.so: $(CUSRC:%=$(OUT)/%_gi.o) $(OUT)/ref_pp_shim_i.o \
+  $(OUT)/domain_i.o $(OUT)/particle_i.o $(OUT)/rng_i.o $(OUT)/ref_globals.o
+	$(NVCC) -gencode arch=compute_100a,code=sm_100a -shared -Xcompiler -fopenmp \
+	  -o $@ $^ -lgomp -Xlinker --no-undefined
+
+gpu: $(OUT)/libref_gpu.so $(OUT)/libref_gpu_implicit.so
 
 .PHONY: all clean gpu

@@ -12,7 +12,13 @@ so each stage starts from bit-identical inputs; after the stage both pull
 and the child records, per array, the largest difference and the largest
 reference magnitude.
 
-usage: python refgpu_child.py RUNDIR OUT.json
+usage: python refgpu_child.py RUNDIR OUT.json [explicit|implicit]
+  explicit -- oracle/_ref/libref_gpu.so (the default build) and the library
+              with its explicit Adams-Bashforth step
+  implicit -- oracle/_ref/libref_gpu_implicit.so (-DIMPLICIT, the
+              Crank-Nicolson program: no cuda_U_star_2, no diffusion
+              histories, the implicit dt rule) and the library in its
+              Crank-Nicolson form
 """
 import ctypes as C
 import json
@@ -52,8 +58,13 @@ class Side:
         return f(*args)
 
     def arr(self, name, grid, ctype=C.c_double):
+        """the host array (empty where the program does not allocate it:
+        the -DIMPLICIT build has no diffusion histories)"""
         n = getattr(self.dom, grid).s3b
-        return np.ctypeslib.as_array(C.POINTER(ctype).in_dll(self.lib, name), shape=(n,))
+        ptr = C.POINTER(ctype).in_dll(self.lib, name)
+        if not ptr:
+            return np.zeros(0, np.float64 if ctype is C.c_double else np.int32)
+        return np.ctypeslib.as_array(ptr, shape=(n,))
 
     def nparts(self):
         return C.c_int.in_dll(self.lib, "nparts").value
@@ -123,7 +134,8 @@ def copy_state(ref, ours):
     """the reference's host state into this library's host arrays"""
     ra, oa = ref.arrays(), ours.arrays()
     for k in ra:
-        oa[k][:] = ra[k]
+        if ra[k].size and oa[k].size:
+            oa[k][:] = ra[k]
     n = ref.nparts()
     if n:
         C.memmove(C.addressof(ours.parts()), C.addressof(ref.parts()),
@@ -149,7 +161,7 @@ def compare(ref, ours, before, before_parts, parts=False):
     ra, oa = ref.arrays(), ours.arrays()
     for k in ra:
         a, b = ra[k], oa[k]
-        if not a.size:
+        if not a.size or not b.size:
             continue
         diff = np.abs(a.astype(np.float64) - b)
         e = {"d": float(diff.max()), "mag": float(np.abs(a).max()),
@@ -257,15 +269,17 @@ def helm_system(ref, ours, comp):
 
 def main():
     run, out = sys.argv[1], sys.argv[2]
+    implicit = len(sys.argv) > 3 and sys.argv[3] == "implicit"
     lib = abi.load()
-    reflib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_gpu.so"),
+    reflib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_gpu_implicit.so"
+                                 if implicit else "libref_gpu.so"),
                     mode=os.RTLD_LOCAL | getattr(os, "RTLD_DEEPBIND", 0))
     os.chdir(run)
     lib.bbb_set_exit_on_failure(0)
-    # the reference library is the explicit build (no -DIMPLICIT)
+    # the library in the form of the reference build it is checked against
     opts = abi.Options()
     lib.bbb_default_options(C.byref(opts))
-    opts.implicit = 0
+    opts.implicit = 1 if implicit else 0
     lib.bbb_set_options(C.byref(opts))
     ref, ours = Side(reflib), Side(lib)
     for path in ("/usr/local/cuda/lib64/libcudart.so.12", "libcudart.so.12"):
@@ -342,7 +356,8 @@ def main():
           C.c_double(C.c_double.in_dll(s.lib, "Kp").value),
           C.c_double(C.c_double.in_dll(s.lib, "Ki").value),
           C.c_double(C.c_double.in_dll(s.lib, "Kd").value))
-    stage("U_star_2", ["cuda_U_star_2"])
+    if not implicit:
+        stage("U_star_2", ["cuda_U_star_2"])
     for comp in range(3):
         res["helmholtz_%s" % "uvw"[comp]] = helm_system(ref, ours, comp)
     stage("part_BC_star", ["cuda_part_BC_star", "cuda_dom_BC_star"])

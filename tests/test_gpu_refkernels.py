@@ -1,7 +1,9 @@
 """This library's non-solver cuda_* entry points against the reference's own
 CUDA kernels: the reference's src/*.cu (all but src/cuda_bicgstab.cu, which
 needs CUSP) compiled unmodified for sm_100a into oracle/_ref/libref_gpu.so
-(oracle/ref.mk, target gpu) and run side by side with the library in a
+(oracle/ref.mk, target gpu; both the default explicit build and the
+-DIMPLICIT Crank-Nicolson build, libref_gpu_implicit.so, the latter against
+the library's Crank-Nicolson form) and run side by side with the library in a
 child process (tests/refgpu_child.py) through the explicit time step of
 src/bluebottle.c:603-708; its pressure solve and the three Crank-Nicolson
 Helmholtz solves are checked against the systems the reference's own
@@ -30,17 +32,19 @@ pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REFSRC = "/root/reference/src"
-REFGPU = os.path.join(ROOT, "oracle", "_ref", "libref_gpu.so")
+REFGPU = {"explicit": os.path.join(ROOT, "oracle", "_ref", "libref_gpu.so"),
+          "implicit": os.path.join(ROOT, "oracle", "_ref", "libref_gpu_implicit.so")}
 
 REL = 1e-12          # FP64 agreement, relative to the largest magnitude
 
 
-def _ensure():
+def _ensure(build):
     if os.path.isdir(REFSRC):
         subprocess.run(["make", "-s", "-j8", "-f", os.path.join(ROOT, "oracle", "ref.mk"),
                         "REF=" + REFSRC, "gpu"], check=True, cwd=ROOT)
-    if not os.path.exists(REFGPU):
-        pytest.skip("oracle/_ref/libref_gpu.so was not built (needs the reference tree)")
+    if not os.path.exists(REFGPU[build]):
+        pytest.skip("oracle/_ref/%s was not built (needs the reference tree)"
+                    % os.path.basename(REFGPU[build]))
 
 
 CASES = {
@@ -71,13 +75,15 @@ def _case(tmp_path, name):
     return d
 
 
+@pytest.mark.parametrize("build", ["explicit", "implicit"])
 @pytest.mark.parametrize("case", sorted(CASES))
-def test_entry_points_match_reference_kernels(gpu, tmp_path, case):
-    _ensure()
+def test_entry_points_match_reference_kernels(gpu, tmp_path, case, build):
+    _ensure(build)
     run = _case(tmp_path, case)
     out = tmp_path / "diff.json"
     r = subprocess.run([sys.executable, os.path.join(ROOT, "tests", "refgpu_child.py"),
-                        str(run), str(out)], capture_output=True, text=True, timeout=600)
+                        str(run), str(out), build], capture_output=True, text=True,
+                       timeout=600)
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
     res = json.load(open(out))
     bad = []
