@@ -117,3 +117,30 @@ def test_entry_points_match_reference_kernels(gpu, tmp_path, case, build):
                 bad.append((stage, name, e))
     print(json.dumps(res))
     assert not bad, bad
+
+
+def test_reference_kernels_timing(gpu, tmp_path):
+    """The same entry points timed on both sides (tests/refgpu_time_child.py)
+    on a 128^3 periodic box with 500 seeded spheres: a measurement printed
+    for the record, not a pass criterion beyond both sides having run."""
+    _ensure("explicit")
+    from bluebottle_b200 import Sim
+    d = tmp_path / "run"
+    (d / "input").mkdir(parents=True)
+    configs.write_flow_config(str(d / "input" / "flow.config"), n=(128, 128, 128),
+                              hi=(32.0, 32.0, 32.0), nu=0.05, pp_residual=1e-8,
+                              lamb_max_iter=3, g=(0.0, 0.0, -1.0))
+    sim = Sim(configs.sedimentation((128, 128, 128), (32.0, 32.0, 32.0), 500, seed=3))
+    try:
+        sim.write_part_config(str(d / "input" / "part.config"))
+    finally:
+        sim.close()
+    out = tmp_path / "time.json"
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "tests", "refgpu_time_child.py"),
+                        str(d), str(out)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    res = json.load(open(out))
+    print("TIMING", json.dumps(res))
+    for k, row in res.items():
+        if isinstance(row, dict):
+            assert row["reference_ms"] > 0 and row["library_ms"] > 0, k
