@@ -182,6 +182,7 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
                             r0_ratio=(st.guess_r0 / st.extrap_r0
                                       if st.extrap_r0 > 0 else None))
     used, evaluated, ratios = 0, 0, []
+    solves = 0
     lib.bbb_profile_reset()
     lib.bbb_profile_enable(1 if profile else 0)
     launches0 = lib.bbb_kernel_launches()
@@ -193,6 +194,7 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
         sim.step()
         st = sim.stats()
         iters += st.pp_iters_total
+        solves += st.pp_solves
         used += st.guess_used
         evaluated += st.guess_evaluated
         if st.guess_evaluated and st.extrap_r0 > 0 and st.guess_r0 > 0:
@@ -208,6 +210,7 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
     out["ms"] = ms
     out["launches"] = lib.bbb_kernel_launches() - launches0
     out["pp_iters_per_step"] = iters / max(steps, 1)
+    out["pp_iters_per_solve"] = iters / max(solves, 1)
     st = sim.stats()
     out["lamb_iters"] = st.lamb_iters
     out["outer"] = st.pp_outer_last
@@ -387,6 +390,8 @@ def main():
                                    mixed.get("guess_r0_ratio"),
                                "probe_step": mixed.get("probe")},
                            "bicgstab_iters_per_step": mixed["pp_iters_per_step"],
+                           "bicgstab_iters_per_solve": mixed["pp_iters_per_solve"],
+                           "cell_updates_per_s": value * mixed["cells"],
                            "fp64_bicgstab_iters_per_step":
                                fp64["pp_iters_per_step"] if fp64 else None,
                            "l2": "inputs larger than L2 (each vector 134 MB FP32)",
