@@ -824,7 +824,13 @@ __global__ void k_energy_div(const real *uu, const real *vv, const real *ww,
     long long cu = i + (long long)j * G.fx_s1 + (long long)k * G.fx_s2;
     long long cv = i + (long long)j * G.fy_s1 + (long long)k * G.fy_s2;
     long long cw = i + (long long)j * G.fz_s1 + (long long)k * G.fz_s2;
-    v[0] += uu[cu] * uu[cu] + vv[cv] * vv[cv] + ww[cw] * ww[cw];
+    /* the reference's energy: face pairs averaged to the cell centre
+     * (colocate_Gf?, src/bluebottle_kernel.cu:3849-3890), squares summed
+     * u, v, w (energy_multiply :3891) */
+    double uc = 0.5 * (uu[cu] + uu[cu + 1]);
+    double vc = 0.5 * (vv[cv] + vv[cv + G.fy_s1]);
+    double wc = 0.5 * (ww[cw] + ww[cw + G.fz_s2]);
+    v[0] += uc * uc + vc * vc + wc * wc;
     long long cc = i + (long long)j * G.cc_s1 + (long long)k * G.cc_s2;
     if(phs[cc] < 0) {
       double s = (uu[cu + 1] - uu[cu]) * ddx + (vv[cv + G.fy_s1] - vv[cv]) * ddy
@@ -841,7 +847,7 @@ __global__ void k_energy_div(const real *uu, const real *vv, const real *ww,
   if(bbb_grid_partial<3>(v, partials, ticket + 1, sh)) {
     bbb_grid_finish_sum<3>(v, partials, ticket + 1, sh);
     if(threadIdx.x == 0) {
-      out[0] = 0.5 * v[0] * G.dx * G.dy * G.dz;
+      out[0] = v[0] / (double)n * 0.5;
       out[1] = sqrt(v[1]);
     }
   }
@@ -865,7 +871,8 @@ static void energy_div(double *e, double *dl2, double *dmax)
   *dmax = g_dev.red_host[2];
 }
 
-/* src/cuda_bluebottle.cu:3944 (kinetic energy of the flow) */
+/* src/cuda_bluebottle.cu:3944: half the mean over the cells of the
+ * cell-centred |u|^2 */
 extern "C" real cuda_compute_energy(void)
 {
   bbb_dev_require();

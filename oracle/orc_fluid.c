@@ -1070,26 +1070,23 @@ real orc_find_dt(orc_state *st)
   return dtn;
 }
 
-/* kinetic energy 0.5 * sum over interior faces of u^2 (+ v^2 + w^2) times
- * the cell volume, each component on its own faces (the duplicated periodic
- * face counted once) */
+/* src/cuda_bluebottle.cu:3944-4015 with src/bluebottle_kernel.cu:
+ * 3849-3905: half the mean over the cells of |u|^2, each component taken
+ * to the cell centre as the average of its two faces (colocate_Gf?), the
+ * squares summed u, v, w (energy_multiply) */
 real orc_compute_energy(orc_state *st)
 {
   const dom_struct *d = &st->dom;
+  const grid_info *G = &d->Gcc;
   real e = 0.;
-  for(int k = d->Gfx.ks; k < d->Gfx.ke; k++) for(int j = d->Gfx.js; j < d->Gfx.je; j++)
-  for(int i = d->Gfx.is; i < d->Gfx.ie - 1; i++) {
-    real q = st->u[CCI(d->Gfx, i, j, k)]; e += q * q;
+  for(int k = G->ks; k < G->ke; k++) for(int j = G->js; j < G->je; j++)
+  for(int i = G->is; i < G->ie; i++) {
+    real uc = 0.5 * (st->u[CCI(d->Gfx, i, j, k)] + st->u[CCI(d->Gfx, i + 1, j, k)]);
+    real vc = 0.5 * (st->v[CCI(d->Gfy, i, j, k)] + st->v[CCI(d->Gfy, i, j + 1, k)]);
+    real wc = 0.5 * (st->w[CCI(d->Gfz, i, j, k)] + st->w[CCI(d->Gfz, i, j, k + 1)]);
+    e += uc * uc + vc * vc + wc * wc;
   }
-  for(int k = d->Gfy.ks; k < d->Gfy.ke; k++) for(int j = d->Gfy.js; j < d->Gfy.je - 1; j++)
-  for(int i = d->Gfy.is; i < d->Gfy.ie; i++) {
-    real q = st->v[CCI(d->Gfy, i, j, k)]; e += q * q;
-  }
-  for(int k = d->Gfz.ks; k < d->Gfz.ke - 1; k++) for(int j = d->Gfz.js; j < d->Gfz.je; j++)
-  for(int i = d->Gfz.is; i < d->Gfz.ie; i++) {
-    real q = st->w[CCI(d->Gfz, i, j, k)]; e += q * q;
-  }
-  return 0.5 * e * d->dx * d->dy * d->dz;
+  return e / G->s3 * 0.5;
 }
 
 void orc_divergence(orc_state *st, const real *uu, const real *vv,

@@ -373,6 +373,7 @@ def main():
     stage("parts_internal", ["cuda_parts_internal", "cuda_dom_BC"])
     stage("store", ["cuda_store_u", "cuda_store_coeffs"], parts=True)
     stage("find_dt", ["cuda_find_dt"], ret="cuda_find_dt")
+    stage("energy", ["cuda_compute_energy"], ret="cuda_compute_energy")
     for s in (ref, ours):
         s.call("cuda_part_free")
         s.call("cuda_dom_free")

@@ -104,7 +104,7 @@ def test_entry_points_match_reference_kernels(gpu, tmp_path, case, build):
     for stage, arrays in res.items():
         # the stage ran: it changed something on the reference side
         moved = [e.get("moved", 0.0) for e in arrays.values()]
-        if stage not in ("find_dt",) and max(moved) == 0:
+        if stage not in ("find_dt", "energy") and max(moved) == 0:
             bad.append((stage, "nothing changed"))
         for name, e in arrays.items():
             if e["kind"] == "int":
