@@ -169,7 +169,9 @@ def sedimentation(n=(64, 64, 64), side=(16.0, 16.0, 16.0), npart=8, nu=0.1,
                     npart=npart, seed=seed, options=opts)
 
 
-# BASELINE configurations (seeded synthetic inputs with the stated shapes)
+# The benchmark configurations C1-C5: Taylor-Green 32^3, then sedimenting
+# sphere packs from 64^3 + 8 spheres to 256x256x512 + 8000 spheres (seeded
+# synthetic inputs of those shapes)
 def config_c1():
     return taylor_green(32)
 
