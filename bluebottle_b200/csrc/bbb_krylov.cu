@@ -1081,8 +1081,8 @@ static boxc retile(const boxc &B0, int per_sm, bool align, int gxw = 0, int gyw 
   return b;
 }
 
-/* cuTensorMapEncodeTiled through the runtime's driver entry point (no link
- * against the driver library); NULL when the driver does not offer it */
+/* cuTensorMapEncodeTiled through the CUDA runtime's driver entry point (no
+ * link against libcuda); NULL when the installed CUDA driver lacks it */
 typedef CUresult (*as_encode_fn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t,
   void *, const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,

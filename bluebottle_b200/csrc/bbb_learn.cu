@@ -437,8 +437,8 @@ __global__ void __launch_bounds__(LG_THREADS, 2) k_conv_z(lg_zbox Z,
 
 /* ------------------------------------------------ reference convolution
  * The same three modes on the CUDA cores in FP32 (one thread per cell and
- * output channel group); the checker of the tensor-core path and the
- * fallback-free path for boxes where a 128-cell tile does not fit. */
+ * output channel group): the FP32 result the tests hold the tensor-core
+ * path to, and the path for boxes where a 128-cell tile does not fit. */
 template <int MODE>
 __global__ void k_conv_ref(lg_box B, const bf16 *__restrict__ in,
   const float *__restrict__ w, const float *__restrict__ bias, float *pre,

@@ -2,7 +2,7 @@
  *
  * TEST INFRASTRUCTURE ONLY.  This is a plain C99 + OpenMP restatement of the
  * reference's algorithm, used by tests/, __graft_entry__.smoke() and
- * bench.py's CPU-baseline leg as the checker.  The product library
+ * bench.py's CPU-baseline leg as the result to check against.  The product library
  * (libbbb200.so) never links, loads or calls it.
  *
  * Every routine names the reference file:line it restates.  The arrays use

@@ -1,7 +1,7 @@
 """ctypes wrapper of the CPU FP64 oracle (liborc.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
-bench.py's CPU-baseline leg, as the checker.  Nothing in bluebottle_b200
+bench.py's CPU-baseline leg, as the result to check against.  Nothing in bluebottle_b200
 imports it.
 """
 import ctypes as C

@@ -59,8 +59,8 @@ $(OUT)/libref_dropin.so: $(OUT)/domain_d.o $(OUT)/particle_d.o $(OUT)/rng_d.o $(
 # CUSP, which the reference does not ship) and src/cuda_testing.cu --
 # compiled unmodified for sm_100a and linked with the host set-up above
 # into oracle/_ref/libref_gpu.so: the reference's GPU kernels behind its
-# own cuda_* entry points, the checker of this library's non-solver entry
-# points (tests/test_gpu_refkernels.py).  `make -f oracle/ref.mk gpu`.
+# own cuda_* entry points, which tests/test_gpu_refkernels.py compares this
+# library's non-solver entry points with.  `make -f oracle/ref.mk gpu`.
 NVCC = nvcc
 NVFLAGS = -gencode arch=compute_100a,code=sm_100a -O2 -DDOUBLE -w \
   -Xcompiler -fPIC,-fopenmp -I$(OUT) -I$(REF)

@@ -8,8 +8,9 @@
  * src/cuda_bicgstab.cu:1178-1202), the particle rewrite cuda_part_BC_p,
  * and the 13-diagonal matrix (src/cuda_bicgstab.cu:729-815) -- launching
  * the reference's own kernels from src/bicgstab_kernel.cu with the launch
- * shapes those lines use, and hands the system to the caller: the checker
- * that this library's solve satisfies the reference's own system.
+ * shapes those lines use, and hands the system to the caller, so a test
+ * can verify that this library's solve satisfies the reference's own
+ * system.
  *
  * The matrix is returned in the layout of CUSP's dia_matrix values: column
  * d of a pitched array, A[d * pitch + row], with the diagonal offsets of
