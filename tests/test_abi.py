@@ -98,3 +98,28 @@ def test_status_strings():
         s = lib.bbb_status_string(code)
         assert s and len(s) >= 2
     assert lib.bbb_device_count() >= 0
+
+
+@pytest.mark.parametrize("cname,cls", [("bbb_stats", abi.Stats),
+                                       ("bbb_options", abi.Options)])
+def test_library_struct_mirrors_match_header(cname, cls, tmp_path):
+    """The ctypes mirrors of the library's own structs (statistics, options)
+    against the header, compiled: every field's offset and the size."""
+    import json
+    import subprocess
+    lines = ['#include "bluebottle_b200.h"', "#include <stdio.h>",
+             "#include <stddef.h>", "int main(void) {",
+             '  printf("{\\"sizeof\\": %%zu", sizeof(%s));' % cname]
+    for fname, _ in cls._fields_:
+        lines.append('  printf(", \\"%s\\": %%zu", offsetof(%s, %s));'
+                     % (fname, cname, fname))
+    lines += ['  printf("}\\n");', "  return 0;", "}"]
+    src, exe = tmp_path / "probe.c", tmp_path / "probe"
+    src.write_text("\n".join(lines) + "\n")
+    subprocess.run(["gcc", "-std=gnu99", "-o", str(exe), str(src), "-I" + INCLUDE],
+                   check=True, capture_output=True)
+    got = json.loads(subprocess.run([str(exe)], check=True, capture_output=True,
+                                    text=True).stdout)
+    assert C.sizeof(cls) == got["sizeof"]
+    for fname, _ in cls._fields_:
+        assert getattr(cls, fname).offset == got[fname], fname
