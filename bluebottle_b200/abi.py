@@ -99,7 +99,9 @@ class Stats(C.Structure):
                 ("lamb_iters", C.c_int), ("lamb_err", C.c_double),
                 ("guess_used", C.c_int), ("guess_r0", C.c_double),
                 ("extrap_r0", C.c_double), ("guess_evaluated", C.c_int),
-                ("guess_cost_ms", C.c_double), ("guess_benefit_ms", C.c_double)]
+                ("guess_cost_ms", C.c_double), ("guess_benefit_ms", C.c_double),
+                ("step_dt", C.c_double), ("cfl_adv", C.c_double),
+                ("helm_solves", C.c_int), ("pp_iters_max", C.c_int)]
 
 
 PERIODIC, DIRICHLET, NEUMANN, PRECURSOR = 0, 1, 2, 3

@@ -129,12 +129,13 @@ class Workload:
     rsr: float = 1.2
     seed: int = 1
     taylor_green: float = 0.0
+    loa: float = 0.0
     options: dict = field(default_factory=dict)
 
     def write(self, dirpath):
         os.makedirs(dirpath, exist_ok=True)
         write_flow_config(os.path.join(dirpath, "flow.config"), **self.flow)
-        write_part_config(os.path.join(dirpath, "part.config"), [])
+        write_part_config(os.path.join(dirpath, "part.config"), [], loa=self.loa)
         return dirpath
 
 
@@ -155,23 +156,43 @@ def taylor_green(n=32, steps_dt=0.01, tol=1e-10):
 
 
 def sedimentation(n=(64, 64, 64), side=(16.0, 16.0, 16.0), npart=8, nu=0.1,
-                  tol=1e-8, lamb_max_iter=25, dt=None, seed=1, prec=0):
+                  tol=1e-8, lamb_max_iter=25, dt=None, seed=1, prec=0,
+                  gap=0.1, loa=0.0):
     """Periodic box of seeded spheres (radius 1, density ratio 2) settling
-    under gravity 1 along -z; the box's net weight is balanced by gradP.z."""
+    under gravity 1 along -z; the box's net weight is balanced by gradP.z.
+
+    The time step follows the reference's rule (cuda_find_dt,
+    src/cuda_bluebottle.cu:3500-3577, Crank-Nicolson form): CFL 0.5 over the
+    advective terms, growing at most 1.1x per step from the viscous start
+    value of domain_init.  `dt` fixes it instead.  `gap` is the pack's
+    minimum surface gap in radii; `loa` the lubrication range l/a of
+    part.config (the reference's collision_parts acts for gaps below
+    int(l/a) radii, src/bluebottle_kernel.cu:2597)."""
     f = _box(n[0], n[1], n[2], side)
-    f.update(nu=nu, pp_residual=tol, pp_max_iter=20000,
+    f.update(nu=nu, pp_residual=tol, pp_max_iter=20000, CFL=0.5,
              lamb_max_iter=lamb_max_iter, lamb_residual=1e-2, g=(0.0, 0.0, -1.0),
              lamb_cut=1e-4, lamb_relax=1.0)
-    dx = side[0] / n[0]
-    opts = dict(implicit=1, gravity_balance=1, precision=prec,
-                fixed_dt=dt if dt is not None else 0.5 * dx)
+    opts = dict(implicit=1, gravity_balance=1, precision=prec)
+    if dt is not None:
+        opts["fixed_dt"] = dt
     return Workload("sediment_%dx%dx%d_%dp" % (n[0], n[1], n[2], npart), f,
-                    npart=npart, seed=seed, options=opts)
+                    npart=npart, seed=seed, gap=gap, loa=loa, options=opts)
 
 
 # The benchmark configurations C1-C5: Taylor-Green 32^3, then sedimenting
 # sphere packs from 64^3 + 8 spheres to 256x256x512 + 8000 spheres (seeded
-# synthetic inputs of those shapes)
+# synthetic inputs of those shapes).  The 8-sphere pack keeps its 0.1-radius
+# minimum gap; the dense packs are seeded 0.5 radii apart (2 cells at 4
+# cells per radius) and carry the reference's default lubrication range
+# l/a = 1 (sim/input/part.config).  At 4 cells per radius a pair closer than
+# about 0.12 radii has quadrature nodes (rs = 1.2 a) inside its partner,
+# which the reference's check_nodes screens for walls only
+# (src/quadrature_kernel.cu:45-96), and the flow in that gap diverges
+# within a few steps, in either precision form.
+DENSE_GAP = 0.5
+DENSE_LOA = 1.0
+
+
 def config_c1():
     return taylor_green(32)
 
@@ -180,15 +201,17 @@ def config_c2():
     return sedimentation((64, 64, 64), (16.0, 16.0, 16.0), 8, nu=0.1)
 
 
-def config_c3():
+def config_c3(prec=1):
     return sedimentation((128, 128, 128), (32.0, 32.0, 32.0), 256, nu=0.1,
-                         prec=1)
+                         prec=prec, gap=DENSE_GAP, loa=DENSE_LOA)
 
 
-def config_c4():
-    return sedimentation((256, 256, 256), (64.0, 64.0, 64.0), 2000, nu=0.05)
+def config_c4(prec=0):
+    return sedimentation((256, 256, 256), (64.0, 64.0, 64.0), 2000, nu=0.05,
+                         prec=prec, gap=DENSE_GAP, loa=DENSE_LOA)
 
 
 def config_c5(prec=1, lamb_max_iter=25):
     return sedimentation((256, 256, 512), (64.0, 64.0, 128.0), 8000, nu=0.05,
-                         prec=prec, lamb_max_iter=lamb_max_iter)
+                         prec=prec, lamb_max_iter=lamb_max_iter, gap=DENSE_GAP,
+                         loa=DENSE_LOA)

@@ -786,6 +786,8 @@ extern "C" real cuda_find_dt(void)
   d2h(g_dev.red_host, g_dev.red_dev + 16, 3 * sizeof(double));
   BBB_CK(cudaStreamSynchronize(g_dev.stream));
   real umax = g_dev.red_host[0], vmax = g_dev.red_host[1], wmax = g_dev.red_host[2];
+  g_stats.cfl_adv = g_stats.step_dt
+    * (umax / d->dx + vmax / d->dy + wmax / d->dz);
   real tmp;
   if(!g_opt.implicit) {
     tmp = umax / d->dx + 2. * nu / d->dx / d->dx;

@@ -916,6 +916,7 @@ int bbb_step(void)
   int st0 = bbb_last_status();
   if(st0 != BBB_OK) return st0;
   memset(&g_stats, 0, sizeof(g_stats));
+  g_stats.step_dt = dt;
   bbb_advance_clock();
   cuda_compute_forcing(&pid_int, &pid_back, Kp, Ki, Kd);
   /* compute_vel_BC (src/domain.c:3144) */

@@ -143,6 +143,18 @@ void bbb_record_solver(const char *name, int niter, real resid);
   cudaError_t e_ = cudaPeekAtLastError(); if(e_ != cudaSuccess) \
     bbb_set_status_at(BBB_ERR_CUDA, cudaGetErrorString(e_), __FILE__, __LINE__); } while(0)
 
+/* per-launch CUDA-event timing of the solver and RHS kernels while
+ * bbb_profile_enable(1) is on (bbb_krylov.cu): the slots, as
+ * bbb_profile_get_pass numbers them */
+#define BBB_PROF_PASS_A 0         /* BiCGSTAB pass A                       */
+#define BBB_PROF_PASS_B 1         /* BiCGSTAB pass B                       */
+#define BBB_PROF_OUTER 2          /* FP64 outer residual (defect correction) */
+#define BBB_PROF_CG1 3            /* Helmholtz CG stencil pass             */
+#define BBB_PROF_CG2 4            /* Helmholtz CG pointwise pass           */
+#define BBB_PROF_RHS 5            /* momentum right-hand side              */
+void bbb_prof_begin(int slot, double bytes);
+void bbb_prof_end(void);
+
 /* entry points between the .cu files */
 void bbb_dev_require(void);
 void bbb_build_masks(void);

@@ -912,17 +912,20 @@ __global__ void k_pp_writeback(const double *x, real *ph, bbb_geom G,
  * only the passes the device really executed are summed, each with its
  * algorithmic bytes (compulsory reads and writes of the owned cells). */
 #define BBB_PROF_MAX 16384
+#define BBB_PROF_SLOTS 6
 static struct {
   int on, n;
   cudaEvent_t ev[2 * BBB_PROF_MAX];     /* start / end event of each launch */
-  int slot[BBB_PROF_MAX];               /* 0 pass A, 1 pass B              */
+  int slot[BBB_PROF_MAX];               /* BBB_PROF_* kind of the launch    */
+  unsigned char ran[BBB_PROF_MAX];      /* 0: returned at once (after the
+                                           solve had converged)            */
   double bytes[BBB_PROF_MAX];
-  double ms[2], kbytes[2];
-  long long launches[2];
+  double ms[BBB_PROF_SLOTS], kbytes[BBB_PROF_SLOTS];
+  long long launches[BBB_PROF_SLOTS];
   long long iters;
 } g_prof;
 
-/* before a pass launch: its slot and algorithmic bytes, start event */
+/* before a launch: its slot and algorithmic bytes, start event */
 static void prof_begin(int slot, double b)
 {
   if(!g_prof.on || g_prof.n >= BBB_PROF_MAX) return;
@@ -931,6 +934,7 @@ static void prof_begin(int slot, double b)
   if(!g_prof.ev[2 * i + 1]) cudaEventCreate(&g_prof.ev[2 * i + 1]);
   g_prof.slot[i] = slot;
   g_prof.bytes[i] = b;
+  g_prof.ran[i] = 1;
   cudaEventRecord(g_prof.ev[2 * i], g_dev.stream);
 }
 
@@ -942,12 +946,28 @@ static void prof_end(void)
   g_prof.n++;
 }
 
-/* the stream has been synchronised: the first `npass` recorded launches
- * really ran (later ones returned at once) */
-static void prof_collect(long long npass)
+/* for launches made in the other source files (the momentum RHS) */
+void bbb_prof_begin(int slot, double bytes) { prof_begin(slot, bytes); }
+void bbb_prof_end(void) { prof_end(); }
+
+/* index of the next record: the first launch of an iteration loop */
+static int prof_mark(void) { return g_prof.on ? g_prof.n : 0; }
+
+/* of the records from `from` on, only the first `nran` launches did work
+ * (the device had converged before the later ones ran) */
+static void prof_ran(int from, long long nran)
 {
   if(!g_prof.on) return;
-  for(int i = 0; i < g_prof.n && i < npass; i++) {
+  for(int i = from; i < g_prof.n; i++)
+    if(i - from >= nran) g_prof.ran[i] = 0;
+}
+
+/* the stream has been synchronised: sum the launches that did work */
+static void prof_collect(void)
+{
+  if(!g_prof.on) return;
+  for(int i = 0; i < g_prof.n; i++) {
+    if(!g_prof.ran[i]) continue;
     float t = 0.f;
     if(cudaEventElapsedTime(&t, g_prof.ev[2 * i], g_prof.ev[2 * i + 1]) == cudaSuccess) {
       int sl = g_prof.slot[i];
@@ -956,14 +976,13 @@ static void prof_collect(long long npass)
       g_prof.launches[sl]++;
     }
   }
-  g_prof.iters += npass / 2;
   g_prof.n = 0;
 }
 
 extern "C" void bbb_profile_enable(int on) { g_prof.on = on; g_prof.n = 0; }
 extern "C" void bbb_profile_reset(void)
 {
-  for(int a = 0; a < 2; a++) {
+  for(int a = 0; a < BBB_PROF_SLOTS; a++) {
     g_prof.ms[a] = 0.; g_prof.kbytes[a] = 0.; g_prof.launches[a] = 0;
   }
   g_prof.iters = 0; g_prof.n = 0;
@@ -977,7 +996,7 @@ extern "C" void bbb_profile_get(double *ms, long long *iters, double *bytes)
 extern "C" void bbb_profile_get_pass(int pass, double *ms, long long *launches,
   double *bytes)
 {
-  if(pass < 0 || pass >= 2) { *ms = 0.; *launches = 0; *bytes = 0.; return; }
+  if(pass < 0 || pass >= BBB_PROF_SLOTS) { *ms = 0.; *launches = 0; *bytes = 0.; return; }
   *ms = g_prof.ms[pass]; *launches = g_prof.launches[pass]; *bytes = g_prof.kbytes[pass];
 }
 
@@ -1184,7 +1203,7 @@ static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
      * x, rh; + mask */
     double a_bytes = (launched == 0 && !resume) ? (double)n * (5. * w + 1.)
                                                 : (double)n * (10. * w + 1.);
-    prof_begin(0, a_bytes);
+    prof_begin(BBB_PROF_PASS_A, a_bytes);
     if(staged) {
       as_args<T> A;
       A.mask = mask;
@@ -1204,7 +1223,7 @@ static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
   };
   /* pass B: reads r and the latest v (buffer cur) */
   auto pass_b = [&]() {
-    prof_begin(1, (double)n * (5. * w + 1.));
+    prof_begin(BBB_PROF_PASS_B, (double)n * (5. * w + 1.));
     if(staged) {
       as_args<T> A;
       A.mask = mask;
@@ -1220,6 +1239,7 @@ static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
     BBB_LAUNCHED();
     prof_end();
   };
+  const int pmark = prof_mark();
   if(resume) drive(s, [&]() { pass_b(); pass_a(); }, maxit, batch0);
   else drive(s, [&]() { pass_a(); pass_b(); }, maxit, batch0);
   /* passes executed -- fresh: the opening pass A, B and A of each counted
@@ -1230,7 +1250,9 @@ static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
   long long npass;
   if(resume) npass = 2LL * h->iter + (h->s_conv ? 2 : 0);
   else npass = h->first ? 0 : 2LL * h->iter + 1 + (h->s_conv ? 2 : 0);
-  prof_collect(npass);
+  prof_ran(pmark, npass);
+  if(g_prof.on) g_prof.iters += npass / 2;
+  prof_collect();
   /* launches after convergence return at once but still flip `cur`: the
    * latest p, v are where the passes A that really ran left them */
   if(curp) {
@@ -1291,6 +1313,7 @@ int bbb_poisson_solve(int record)
   g_stats.pp_solves++;
   g_stats.pp_iters_total += h->iter;
   g_stats.pp_iters_last = h->iter;
+  if(h->iter > g_stats.pp_iters_max) g_stats.pp_iters_max = h->iter;
   g_stats.pp_resid_last = resid;
   g_stats.pp_outer_last = 1;
   bbb_learn_solve_done(h->rnorm);
@@ -1531,17 +1554,57 @@ static void outer_resid(const boxc &BD, const opc &O, const uint8_t *mask,
       A.mask = mask; A.h[0] = x; A.s = s; A.partials = g_dev.partials;
       A.rf = rf; A.si = si; A.itol = itol; A.imaxit = imaxit;
       A.project = project; A.n = n;
+      prof_begin(BBB_PROF_OUTER, (double)n * (2. * 8. + 4. + 1.));
       k_bicg_async<double, 2><<<B2.nblk, AS_THREADS, as_layout<double, 2>::SMEM,
         g_dev.stream>>>(B2, O, A, M);
       BBB_LAUNCHED();
+      prof_end();
       return;
     }
   }
   dim3 grd = box_grid(BD), blk(TX, TY);
+  prof_begin(BBB_PROF_OUTER, (double)n * (2. * 8. + 4. + 1.));
   k_outer_resid<VD><<<grd, blk, 0, g_dev.stream>>>(BD, O, mask, b, x, rf, s, si,
     g_dev.partials, itol, imaxit, project, n);
   BBB_LAUNCHED();
+  prof_end();
 }
+
+/* Fail-fast rule of a defect-correction solve.  The inner iterations of all
+ * sweeps share one budget, pp_max_iter -- the cap of the whole FP64 solve,
+ * as CUSP's monitor caps the reference's (src/cuda_bicgstab.cu:996-1018) --
+ * and the FP64 residual must halve at least every two sweeps.  A solve that
+ * breaks either rule stops at once as not converged, so a diverging or
+ * stagnating solve reports after at most pp_max_iter inner iterations
+ * instead of running every sweep to its own cap. */
+struct dc_guard {
+  int budget, used, sweeps;
+  double hist[2];                 /* FP64 ||r|| of the two previous sweeps */
+  explicit dc_guard(int b) : budget(b), used(0), sweeps(0) { hist[0] = hist[1] = -1.; }
+  int remaining() const { return budget - used; }
+  /* rn: the FP64 residual the sweep started from; returns 1 when the solve
+   * must stop */
+  int after_sweep(int inner_iters, double rn, const char *what)
+  {
+    used += inner_iters;
+    int stop = 0;
+    if(sweeps >= 2 && hist[0] >= 0. && !(rn <= 0.5 * hist[0])) {
+      if(g_opt.verbose)
+        fprintf(stderr, "%s: FP64 residual %.3e not below half of %.3e two "
+          "sweeps earlier: stopping\n", what, rn, hist[0]);
+      stop = 1;
+    }
+    if(remaining() <= 0) {
+      if(g_opt.verbose)
+        fprintf(stderr, "%s: inner iteration budget %d spent\n", what, budget);
+      stop = 1;
+    }
+    hist[0] = hist[1];
+    hist[1] = rn;
+    sweeps++;
+    return stop;
+  }
+};
 
 /* runs after k_pp_rhs has filled b, x and s->bnorm */
 template <int VD, int VF>
@@ -1565,9 +1628,10 @@ static int poisson_mixed(const boxc &BD, const boxc &BF, const opc &O,
     && (bc.pB == bc.pT);
   double itol = g_opt.inner_tol > 0 ? g_opt.inner_tol : 1e-4;
   int inner_total = 0, cur = 0, fresh = 1, resume_failed = 0;
+  dc_guard guard(pp_max_iter);
   for(int outer = 0; outer <= init.maxit; outer++) {
     outer_resid<VD>(BD, O, g_dev.mask_p, g_dev.kb, g_dev.kx, g_dev.fb, s, si,
-      itol, pp_max_iter, project, n);
+      itol, guard.remaining(), project, n);
     /* a sweep starts the FP32 BiCGSTAB from e = 0; with reliable updates
      * later sweeps replace its residual by the FP64 one and carry on
      * (restarting only after an inner breakdown).  On the 256x256x512
@@ -1585,7 +1649,7 @@ static int poisson_mixed(const boxc &BD, const boxc &BF, const opc &O,
     BBB_LAUNCHED();
     bicgstab_iterations<float, VF>(BF, O, n, g_dev.mask_p, g_dev.fr, g_dev.frh,
       g_dev.fp[0], g_dev.fp[1], g_dev.fv[0], g_dev.fv[1], g_dev.fs, g_dev.ft,
-      g_dev.fx, si, pp_max_iter, 4, &cur, !fresh);
+      g_dev.fx, si, guard.remaining(), 4, &cur, !fresh);
     if(bbb_last_status() == BBB_ERR_CUDA) return -1;
     inner_total += g_dev.kry_host->iter;
     if(g_opt.verbose)
@@ -1616,12 +1680,16 @@ static int poisson_mixed(const boxc &BD, const boxc &BF, const opc &O,
       fprintf(stderr, "poisson mixed sweep %d: FP64 ||r|| %.3e (tol %.3e)\n",
         outer, g_dev.kry_host->rnorm, g_dev.kry_host->tol);
     if(g_dev.kry_host->done) break;
+    if(guard.after_sweep(inner_total - guard.used, g_dev.kry_host->rnorm,
+                         "pressure-Poisson (mixed)"))
+      break;
   }
   bbb_kry *h = g_dev.kry_host;
   real resid = h->bnorm > 0 ? h->rnorm / h->bnorm : h->rnorm;
   g_stats.pp_solves++;
   g_stats.pp_iters_total += inner_total;
   g_stats.pp_iters_last = inner_total;
+  if(inner_total > g_stats.pp_iters_max) g_stats.pp_iters_max = inner_total;
   g_stats.pp_resid_last = resid;
   g_stats.pp_outer_last = h->iter;
   if(record) bbb_record_solver("solver_expd.rec", inner_total, resid);
@@ -2065,23 +2133,31 @@ static int helmholtz_mixed(const boxc &BD, const boxc &BF, const opc &O,
   BBB_LAUNCHED();
   dim3 grdD = box_grid(BD), grdF = box_grid(BF), blk(TX, TY);
   int inner_total = 0;
+  dc_guard guard(pp_max_iter);
   for(int outer = 0; outer <= max_outer; outer++) {
     outer_resid<VD>(BD, O, mask, g_dev.kb, g_dev.kx, g_dev.fr, s, si, itol,
-      pp_max_iter, 0, n);
+      guard.remaining(), 0, n);
     k_cg_inner_setup<VF><<<NPW, 256, 0, g_dev.stream>>>(n, O, mask, g_dev.fr,
       g_dev.fx, g_dev.fp[0], si, g_dev.partials);
     BBB_LAUNCHED();
     int cur = 0;
+    const int pmark = prof_mark();
     drive(si, [&]() {
+      prof_begin(BBB_PROF_CG1, (double)n * (4. * 4. + 1.));
       k_cg1<float, VF><<<grdF, blk, 0, g_dev.stream>>>(BF, O, mask, g_dev.fr,
         g_dev.fp[cur], g_dev.fp[cur ^ 1], g_dev.fv[0], si, g_dev.partials);
       BBB_LAUNCHED();
+      prof_end();
+      prof_begin(BBB_PROF_CG2, (double)n * (6. * 4. + 1.));
       k_cg2<float><<<NPW, 256, 0, g_dev.stream>>>(n, O, mask, g_dev.fx,
         g_dev.fp[cur ^ 1], g_dev.fr, g_dev.fv[0], si, g_dev.partials);
       BBB_LAUNCHED();
+      prof_end();
       cur ^= 1;
-    }, pp_max_iter, 2);
+    }, guard.remaining(), 2);
     if(bbb_last_status() == BBB_ERR_CUDA) return -1;
+    prof_ran(pmark, 2LL * g_dev.kry_host->iter);
+    prof_collect();
     inner_total += g_dev.kry_host->iter;
     k_accumulate<VF><<<NPW, 256, 0, g_dev.stream>>>(n, g_dev.kx, g_dev.fx, s);
     BBB_LAUNCHED();
@@ -2089,6 +2165,9 @@ static int helmholtz_mixed(const boxc &BD, const boxc &BF, const opc &O,
       cudaMemcpyDeviceToHost, g_dev.stream));
     BBB_CK(cudaStreamSynchronize(g_dev.stream));
     if(g_dev.kry_host->done) break;
+    if(guard.after_sweep(inner_total - guard.used, g_dev.kry_host->rnorm,
+                         "Helmholtz (mixed)"))
+      break;
   }
   k_cg_writeback<<<NPW, 256, 0, g_dev.stream>>>(g_dev.kx, star, G, comp,
     nx, ny, nz, tr);
@@ -2128,6 +2207,7 @@ int bbb_helmholtz_solve(int comp)
     bbb_kry *h = g_dev.kry_host;
     real resid = h->bnorm > 0 ? h->rnorm / h->bnorm : h->rnorm;
     g_stats.helm_iters_total += it > 0 ? it : 0;
+    g_stats.helm_solves++;
     bbb_record_solver("solver_helmholtz_expd.rec", it, resid);
     if(h->status == BBB_ERR_NONFINITE) bbb_set_status(BBB_ERR_NONFINITE, "Helmholtz");
     if(!h->converged) {
@@ -2159,7 +2239,9 @@ int bbb_helmholtz_solve(int comp)
   BBB_LAUNCHED();
   dim3 grd = box_grid(B), blk(TX, TY);
   int cur = 0;
+  const int pmark = prof_mark();
   drive(s, [&]() {
+    prof_begin(BBB_PROF_CG1, (double)n * (4. * 8. + 1.));
     if(V == 2)
       k_cg1<double, 2><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, g_dev.kr,
         g_dev.kp[cur], g_dev.kp[cur ^ 1], g_dev.kv[0], s, g_dev.partials);
@@ -2167,17 +2249,23 @@ int bbb_helmholtz_solve(int comp)
       k_cg1<double, 1><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, g_dev.kr,
         g_dev.kp[cur], g_dev.kp[cur ^ 1], g_dev.kv[0], s, g_dev.partials);
     BBB_LAUNCHED();
+    prof_end();
+    prof_begin(BBB_PROF_CG2, (double)n * (6. * 8. + 1.));
     k_cg2<double><<<NPW, 256, 0, g_dev.stream>>>(n, O, mask, g_dev.kx,
       g_dev.kp[cur ^ 1], g_dev.kr, g_dev.kv[0], s, g_dev.partials);
     BBB_LAUNCHED();
+    prof_end();
     cur ^= 1;
   }, pp_max_iter, 1);
+  prof_ran(pmark, 2LL * g_dev.kry_host->iter);
+  prof_collect();
   k_cg_writeback<<<NPW, 256, 0, g_dev.stream>>>(g_dev.kx, star, G, comp,
     nx, ny, nz, tr);
   BBB_LAUNCHED();
   bbb_kry *h = g_dev.kry_host;
   real resid = h->bnorm > 0 ? h->rnorm / h->bnorm : h->rnorm;
   g_stats.helm_iters_total += h->iter;
+  g_stats.helm_solves++;
   bbb_record_solver("solver_helmholtz_expd.rec", h->iter, resid);
   if(!h->converged) {
     bbb_set_status(BBB_ERR_NOT_CONVERGED, "Helmholtz");

@@ -130,8 +130,15 @@ void bbb_star_rhs(int comp_mask, int explicit_ab2)
   A.comp_mask = comp_mask;
   A.explicit_ab2 = explicit_ab2;
   dim3 blk(32, 8), grd((A.G.nx + 1 + 31) / 32, (A.G.ny + 1 + 7) / 8, A.G.nz + 1);
+  /* algorithmic words per cell: u0, v0, w0 and p0, read by every
+   * component, once; per component conv0 read, star and conv written
+   * (+ diff0 read and diff written in the explicit form) */
+  int ncomp = (comp_mask & 1) + ((comp_mask >> 1) & 1) + ((comp_mask >> 2) & 1);
+  double words = ncomp * (explicit_ab2 ? 5. : 3.) + 4.;
+  bbb_prof_begin(BBB_PROF_RHS, (double)A.G.nx * A.G.ny * A.G.nz * words * sizeof(real));
   k_star_rhs<<<grd, blk, 0, g_dev.stream>>>(A);
   BBB_LAUNCHED();
+  bbb_prof_end();
 }
 
 /* src/cuda_bluebottle.cu:2930-3026 */

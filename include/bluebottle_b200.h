@@ -248,6 +248,12 @@ typedef struct bbb_stats {
   int guess_evaluated;     /* the guess was computed for this step (1/0)   */
   real guess_cost_ms;      /* device time of that evaluation               */
   real guess_benefit_ms;   /* estimated solve time it saved (cost gate)    */
+  real step_dt;            /* dt the step advanced by                      */
+  real cfl_adv;            /* step_dt * (max u / dx + max v / dy + max w /
+                              dz) of the velocity the step ended with: the
+                              advective CFL number cuda_find_dt bounds     */
+  int helm_solves;         /* Helmholtz (CG) solves in the step            */
+  int pp_iters_max;        /* most iterations of one Poisson solve         */
 } bbb_stats;
 void bbb_get_stats(bbb_stats *st);
 
@@ -266,13 +272,17 @@ void bbb_divergence(real *max_abs, real *l2);
 long long bbb_kernel_launches(void);
 void bbb_reset_kernel_launches(void);
 
-/* Live timing of the pressure solver's BiCGSTAB iterations, by CUDA
- * events on the solver stream around each of the two fused passes, over
- * the passes the device executed while enabled.  bbb_profile_get: total
- * milliseconds, iteration count and algorithmic bytes (15 vector words +
- * 2 mask bytes per unknown and iteration).  bbb_profile_get_pass: the same
- * for one pass (0: pass A, the p/v update and first stencil; 1: pass B,
- * the s/t update and second stencil), with its launch count. */
+/* Live timing of the solver and right-hand-side kernels, by CUDA events
+ * on the library's stream around each launch, over the launches that did
+ * work while enabled (launches that returned at once after a solve had
+ * converged are left out).  bbb_profile_get: the BiCGSTAB iterations'
+ * total milliseconds, iteration count and algorithmic bytes (15 vector
+ * words + 2 mask bytes per unknown and iteration).  bbb_profile_get_pass:
+ * milliseconds, launches and algorithmic bytes of one kernel kind --
+ * 0: BiCGSTAB pass A (the p/v update and first stencil), 1: pass B (the
+ * s/t update and second stencil), 2: the FP64 outer residual of the mixed
+ * form, 3: the Helmholtz CG stencil pass, 4: its pointwise pass, 5: the
+ * momentum right-hand side. */
 void bbb_profile_enable(int on);
 void bbb_profile_reset(void);
 void bbb_profile_get(double *ms, long long *iters, double *bytes);

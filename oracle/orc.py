@@ -87,6 +87,40 @@ def load():
 
 INT_FIELDS = ("phase", "phase_shell", "flag_u", "flag_v", "flag_w")
 
+REF_DIR = os.path.join(HERE, "_ref")
+
+
+def reference_host_lib(implicit=True):
+    """Path of the reference's own host set-up code built by oracle/ref.mk
+    (src/domain.c, src/particle.c, src/rng.c; the -DIMPLICIT build for the
+    Crank-Nicolson program), or None when it has not been built."""
+    p = os.path.join(REF_DIR, "libref_host_implicit.so" if implicit
+                     else "libref_host.so")
+    return p if os.path.exists(p) else None
+
+
+def reference_setup(run_dir, implicit=True):
+    """Run the reference's host set-up in run_dir (which holds
+    input/flow.config and input/part.config): domain_read_input,
+    parts_read_input, domain_init, parts_init (src/bluebottle.c:415-431).
+    Returns the loaded library, whose globals hold the state."""
+    path = reference_host_lib(implicit)
+    if path is None:
+        raise FileNotFoundError("oracle/_ref/libref_host*.so is not built")
+    ref = C.CDLL(path, mode=os.RTLD_LOCAL | getattr(os, "RTLD_DEEPBIND", 0))
+    ref.domain_init.restype = C.c_int
+    ref.parts_init.restype = C.c_int
+    cwd = os.getcwd()
+    os.chdir(run_dir)
+    try:
+        ref.domain_read_input()
+        ref.parts_read_input(0)
+        if ref.domain_init() != 0 or ref.parts_init() != 0:
+            raise RuntimeError("the reference's domain_init/parts_init failed")
+    finally:
+        os.chdir(cwd)
+    return ref
+
 
 class Oracle:
     """FP64 CPU state mirroring the reference's host arrays."""
@@ -123,43 +157,88 @@ class Oracle:
                     lamb_iters=iv[7], pp_resid=rv[0], lamb_err=rv[1],
                     cg_resid=list(rv[2:5]))
 
+    REAL_PARAMS = ("rho_f", "nu", "mu", "dt", "dt0", "ttime", "CFL",
+                   "pp_residual", "lamb_residual", "lamb_relax", "lamb_cut",
+                   "vel_tDelay", "p_tDelay", "g_tDelay", "Kp", "Ki", "Kd",
+                   "pid_int", "pid_back", "interactionLengthRatio")
+    INT_PARAMS = ("pp_max_iter", "lamb_max_iter", "out_plane", "stepnum")
+    FIELD_NAMES = ("p0", "p", "phi", "u", "v", "w", "u0", "v0", "w0",
+                   "u_star", "v_star", "w_star", "conv_u", "conv_v",
+                   "conv_w", "conv0_u", "conv0_v", "conv0_w", "diff_u",
+                   "diff_v", "diff_w", "diff0_u", "diff0_v", "diff0_w")
+
+    @classmethod
+    def _from_host(cls, dom, nparts, coeff_stride, scalar, array, bc, g, gradP,
+                   parts_addr, implicit, fixed_dt, lamb_override, prepare):
+        o = cls(dom, nparts, coeff_stride)
+        P = o.P
+        for k in cls.REAL_PARAMS + cls.INT_PARAMS:
+            setattr(P, k, scalar(k))
+        P.implicit = implicit
+        P.fixed_dt = fixed_dt
+        if lamb_override > 0:
+            P.lamb_max_iter = lamb_override
+        C.memmove(C.byref(P.bc), C.byref(bc), C.sizeof(abi.BCStruct))
+        C.memmove(C.byref(P.g), C.byref(g), C.sizeof(abi.GStruct))
+        C.memmove(C.byref(P.gradP), C.byref(gradP), C.sizeof(abi.GStruct))
+        for name in cls.FIELD_NAMES:
+            a = array(name, o.field(name).size)
+            if a is not None:
+                o.field(name)[:] = a
+        if nparts > 0:
+            dst = o.field("parts")
+            C.memmove(C.addressof(dst), parts_addr,
+                      C.sizeof(abi.PartStruct) * nparts)
+            from bluebottle_b200.sim import COEF_NAMES
+            for name in COEF_NAMES:
+                a = array(name, o.field(name).size)
+                if a is not None:
+                    o.field(name)[:] = a
+        if prepare:
+            o.prepare()
+        return o
+
     @classmethod
     def from_sim(cls, sim, prepare=True):
         """Copy a Sim's host state after its host initialisation (before or
         without its device set-up) and, optionally, run the reference's
         set-up sequence (src/bluebottle.c:528-543) on the CPU."""
-        o = cls(sim.dom, sim.nparts, sim.scalar("coeff_stride"))
-        P = o.P
-        for k in ("rho_f", "nu", "mu", "dt", "dt0", "ttime", "CFL",
-                  "pp_residual", "lamb_residual", "lamb_relax", "lamb_cut",
-                  "vel_tDelay", "p_tDelay", "g_tDelay", "Kp", "Ki", "Kd",
-                  "pid_int", "pid_back", "interactionLengthRatio"):
-            setattr(P, k, sim.scalar(k))
-        for k in ("pp_max_iter", "lamb_max_iter", "out_plane", "stepnum"):
-            setattr(P, k, sim.scalar(k))
-        P.implicit = sim.options.implicit
-        P.fixed_dt = sim.options.fixed_dt
-        if sim.options.lamb_max_iter_override > 0:
-            P.lamb_max_iter = sim.options.lamb_max_iter_override
-        C.memmove(C.byref(P.bc), C.byref(sim.bc), C.sizeof(abi.BCStruct))
-        C.memmove(C.byref(P.g), C.byref(sim.g), C.sizeof(abi.GStruct))
-        C.memmove(C.byref(P.gradP), C.byref(sim.gradP), C.sizeof(abi.GStruct))
-        for name in ("p0", "p", "phi", "u", "v", "w", "u0", "v0", "w0",
-                     "u_star", "v_star", "w_star", "conv_u", "conv_v",
-                     "conv_w", "conv0_u", "conv0_v", "conv0_w", "diff_u",
-                     "diff_v", "diff_w", "diff0_u", "diff0_v", "diff0_w"):
-            o.field(name)[:] = sim.array(name)
-        if sim.nparts > 0:
-            src = sim.parts()
-            dst = o.field("parts")
-            C.memmove(C.addressof(dst), C.addressof(src),
-                      C.sizeof(abi.PartStruct) * sim.nparts)
-            from bluebottle_b200.sim import COEF_NAMES
-            for name in COEF_NAMES:
-                o.field(name)[:] = sim.array(name)
-        if prepare:
-            o.prepare()
-        return o
+        n = sim.nparts
+        addr = C.addressof(sim.parts()) if n > 0 else 0
+        return cls._from_host(
+            sim.dom, n, sim.scalar("coeff_stride"), sim.scalar,
+            lambda name, size: sim.array(name), sim.bc, sim.g, sim.gradP,
+            addr, sim.options.implicit, sim.options.fixed_dt,
+            sim.options.lamb_max_iter_override, prepare)
+
+    @classmethod
+    def from_reference(cls, ref, implicit=1, fixed_dt=0.0, lamb_override=0,
+                       prepare=True):
+        """Copy the host state the reference's own set-up left in `ref`
+        (a library from reference_setup): its Dom, boundary conditions,
+        scalars, initial fields, particle records and Lamb coefficients."""
+        real_names = set(cls.REAL_PARAMS)
+
+        def scalar(name):
+            t = C.c_double if name in real_names else C.c_int
+            return t.in_dll(ref, name).value
+
+        def array(name, size):
+            ptr = C.POINTER(C.c_double).in_dll(ref, name)
+            if not ptr:
+                return None       # not allocated by this build (-DIMPLICIT)
+            return np.ctypeslib.as_array(ptr, shape=(size,))
+
+        n = C.c_int.in_dll(ref, "nparts").value
+        addr = 0
+        if n > 0:
+            addr = C.addressof(C.POINTER(abi.PartStruct).in_dll(ref, "parts").contents)
+        return cls._from_host(
+            abi.DomStruct.in_dll(ref, "Dom"), n,
+            C.c_int.in_dll(ref, "coeff_stride").value, scalar, array,
+            abi.BCStruct.in_dll(ref, "bc"), abi.GStruct.in_dll(ref, "g"),
+            abi.GStruct.in_dll(ref, "gradP"), addr, implicit, fixed_dt,
+            lamb_override, prepare)
 
     def prepare(self):
         lib, st = self.lib, self.st

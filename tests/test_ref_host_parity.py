@@ -125,3 +125,44 @@ def test_host_setup_matches_reference(tmp_path, case):
                 assert d == [], d
     finally:
         sim.close()
+
+
+def test_reference_arm_setup_matches_library(tmp_path):
+    """The benchmark's reference arm sets up through the reference's own
+    readers and initialisation (oracle/_ref/libref_host_implicit.so) from
+    the seeded inputs oracle/seed.py writes; that state, copied into the
+    oracle, equals the state the library's own set-up gives the oracle."""
+    from oracle.orc import Oracle, reference_host_lib, reference_setup
+    from oracle.seed import write_workload_inputs
+    if os.path.isdir(REFSRC):
+        subprocess.run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "ref.mk"),
+                        "REF=" + REFSRC], check=True, cwd=ROOT)
+    if reference_host_lib(True) is None:
+        pytest.skip("the reference tree is not available to build oracle/_ref")
+    wl = configs.sedimentation((32, 32, 32), (8.0, 8.0, 8.0), 6, nu=0.05,
+                               gap=0.5, loa=1.0, seed=5)
+    run = tmp_path / "run"
+    write_workload_inputs(wl, str(run / "input"))
+    ref = reference_setup(str(run), implicit=True)
+    a = Oracle.from_reference(ref, implicit=1, lamb_override=3, prepare=False)
+    sim = Sim(wl, options=dict(lamb_max_iter_override=3))
+    try:
+        b = Oracle.from_sim(sim, prepare=False)
+    finally:
+        sim.close()
+    try:
+        assert _diff(a.dom, b.dom, "dom") == []
+        pa, pb = a.P, b.P
+        d = [x for x in _diff(pa, pb, "P")]
+        assert d == [], d
+        for name in Oracle.FIELD_NAMES:
+            assert np.array_equal(a.field(name), b.field(name)), name
+        ra, rb = a.field("parts"), b.field("parts")
+        assert len(ra) == len(rb) == 6
+        for q in range(6):
+            d = [x for x in _diff(ra[q], rb[q], "parts[%d]" % q)
+                 if not x[0].endswith(".bin")]
+            assert d == [], d
+    finally:
+        a.close()
+        b.close()
