@@ -75,6 +75,7 @@ void bbb_default_options(bbb_options *opt)
   opt->lamb_max_iter_override = 0;
   opt->verbose = 0;
   opt->reliable = 0;
+  opt->contact_overrun = 0;
 }
 
 static void opt_init(void)

@@ -41,6 +41,7 @@
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
+#include <mutex>
 #include "bbb_internal.h"
 #include "bbb_reduce.cuh"
 
@@ -2313,8 +2314,10 @@ static __device__ __align__(256) unsigned char
   g_static_scratch[BBB_STATIC_SCRATCH_BYTES];
 
 /* device address of g_static_scratch per device, looked up once with that
- * device current */
+ * device current; the lock makes host threads that make their first call
+ * on a device at the same time take one look-up */
 static unsigned char *g_static_addr[64];
+static std::mutex g_static_lock;
 
 template <int V>
 static int static_iterations(const boxc &B, const opc &O, const uint8_t *mask,
@@ -2357,15 +2360,19 @@ extern "C" int bbb_PP_bicgstab_static(int nx, int ny, int nz, double dx,
   if(n > BBB_STATIC_MAX_CELLS) return BBB_ERR_TOO_LARGE;
   int dev = 0;
   if(cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return BBB_ERR_CUDA;
-  if(!g_static_addr[dev]) {
-    unsigned char *p = NULL;
-    if(cudaGetSymbolAddress((void **)&p, g_static_scratch) != cudaSuccess || !p)
-      return BBB_ERR_CUDA;
-    g_static_addr[dev] = p;
+  unsigned char *base;
+  {
+    std::lock_guard<std::mutex> hold(g_static_lock);
+    if(!g_static_addr[dev]) {
+      unsigned char *p = NULL;
+      if(cudaGetSymbolAddress((void **)&p, g_static_scratch) != cudaSuccess || !p)
+        return BBB_ERR_CUDA;
+      g_static_addr[dev] = p;
+    }
+    base = g_static_addr[dev];
   }
   cudaStream_t st = (cudaStream_t)stream;
   /* carve the scratch */
-  unsigned char *base = g_static_addr[dev];
   long long off = 0;
 #define CARVE(T, ptr, bytes) do { ptr = (T *)(base + off); \
   off += 256LL * (((long long)(bytes) + 255LL) / 256LL); } while(0)

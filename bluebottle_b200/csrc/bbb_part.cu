@@ -1431,6 +1431,7 @@ struct bin_geom {
 struct coll_args {
   double mu, rho_f, nu, dt;
   int ilr;                        /* (int) interactionLengthRatio */
+  int overrun;                    /* option contact_overrun */
   double xs, xe, xl, ys, ye, yl, zs, ze, zl;
   BC bc;
 };
@@ -1458,24 +1459,54 @@ __device__ __forceinline__ double d_st_get(const part_struct *q, int k)
 __device__ __forceinline__ void d_st_set(part_struct *q, int k, double v)
 { memcpy((char *)q->St + sizeof(double) * k, &v, sizeof(double)); }
 
-__device__ void d_contact_forget(part_struct *q, int key)
+/* The contact list of a sphere: partner keys iSt[0..11] with the impact
+ * Stokes numbers St[0..11].  With `overrun` the searches test the slot
+ * before the bound, as the reference's collision kernels do, and so reach
+ * slot 12: the bytes that follow iSt and St in part_struct (the low word
+ * of e_dry; iSt[0..1]) -- read, and written when all 12 slots are taken.
+ * Without it they stop at the list's end: a partner not found is not
+ * removed, and a new contact with no free slot is not stored (slot -1, its
+ * current Stokes number is used). */
+__device__ void d_contact_forget(part_struct *q, int key, int overrun)
 {
   int k = 0;
-  while(d_ist_get(q, k) != key && k < D_MAXN) k++;
-  if(d_ist_get(q, k) == key) { d_ist_set(q, k, -1); d_st_set(q, k, 0.); }
+  if(overrun) {
+    while(d_ist_get(q, k) != key && k < D_MAXN) k++;
+    if(d_ist_get(q, k) == key) { d_ist_set(q, k, -1); d_st_set(q, k, 0.); }
+    return;
+  }
+  while(k < D_MAXN && d_ist_get(q, k) != key) k++;
+  if(k < D_MAXN) { d_ist_set(q, k, -1); d_st_set(q, k, 0.); }
 }
 
-__device__ int d_contact_slot(part_struct *q, int key, double St)
+__device__ int d_contact_slot(part_struct *q, int key, double St, int overrun)
 {
   int k = 0;
-  while(d_ist_get(q, k) != key && k < D_MAXN) k++;
-  if(k == D_MAXN) {
-    k = 0;
-    while(d_ist_get(q, k) != -1 && k < D_MAXN) k++;
-    d_ist_set(q, k, key);
-    d_st_set(q, k, St);
+  if(overrun) {
+    while(d_ist_get(q, k) != key && k < D_MAXN) k++;
+    if(k == D_MAXN) {
+      k = 0;
+      while(d_ist_get(q, k) != -1 && k < D_MAXN) k++;
+      d_ist_set(q, k, key);
+      d_st_set(q, k, St);
+    }
+    return k;
   }
+  while(k < D_MAXN && d_ist_get(q, k) != key) k++;
+  if(k < D_MAXN) return k;
+  k = 0;
+  while(k < D_MAXN && d_ist_get(q, k) != -1) k++;
+  if(k == D_MAXN) return -1;
+  d_ist_set(q, k, key);
+  d_st_set(q, k, St);
   return k;
+}
+
+/* the stored Stokes number of contact slot q, or St when it has none */
+__device__ __forceinline__ double d_contact_st(const part_struct *q, int slot,
+  double St)
+{
+  return slot >= 0 ? d_st_get(q, slot) : St;
 }
 
 __device__ __forceinline__ double d_min_image(double a, double b, double L,
@@ -1513,7 +1544,7 @@ __device__ void d_pair_force(part_struct *pi, const part_struct *pj, int j,
   double ucnx = uty * nz - utz * ny, ucny = -utx * nz + utz * nx, ucnz = utx * ny - uty * nx;
   double Fnx, Fny, Fnz, Ftx, Fty, Ftz, Lox, Loy, Loz;
   if(h < hN && h > 0) {
-    d_contact_forget(pi, j);
+    d_contact_forget(pi, j, A.overrun);
     if(h < eps * pi->r) h = eps * pi->r;
     double ah = ai / h - ai / hN, lnah = log(hN / h);
     Fnx = -1. * B * B / (opB * opB) * ah - B * (1. + 7. * B + B * B) / (5. * opB * opB * opB) * lnah;
@@ -1537,7 +1568,8 @@ __device__ void d_pair_force(part_struct *pi, const part_struct *pj, int j,
     Fnx = 0; Fny = 0; Fnz = 0; Ftx = 0; Fty = 0; Ftz = 0; Lox = 0; Loy = 0; Loz = 0;
   }
   if(h < 0) {
-    int q = d_contact_slot(pi, j, 1. / 9. * pi->rho / rhof * 2. * pi->r * fabs(udotn) / nu);
+    double St_now = 1. / 9. * pi->rho / rhof * 2. * pi->r * fabs(udotn) / nu;
+    int q = d_contact_slot(pi, j, St_now, A.overrun);
     double Vx = -utx + 0.5 * (ai + aj + h) * ocnx;
     double Vy = -uty + 0.5 * (ai + aj + h) * ocny;
     double Vz = -utz + 0.5 * (ai + aj + h) * ocnz;
@@ -1549,7 +1581,7 @@ __device__ void d_pair_force(part_struct *pi, const part_struct *pj, int j,
     double k = 4. / 3. / ((1. - pi->sigma * pi->sigma) / pi->E
       + (1. - pj->sigma * pj->sigma) / pj->E) / sqrt(1. / ai + 1. / aj);
     double xcx0 = 1.e-4;
-    double e = pi->e_dry + (1. + pi->e_dry) / d_st_get(pi, q) * log(xcx0);
+    double e = pi->e_dry + (1. + pi->e_dry) / d_contact_st(pi, q, St_now) * log(xcx0);
     if(e < 0) e = 0;
     double alpha = -2.263 * pow(e, 0.3948) + 2.22;
     double eta = alpha * sqrt(4. / 3. * PI * ai * ai * ai * pi->rho * k * sqrt(-h));
@@ -1608,7 +1640,7 @@ __device__ void d_wall_force(part_struct *p, int ax, int hi, const coll_args &A,
   int t1 = ax == 0 ? 1 : 0, t2 = ax == 2 ? 1 : 2;
   double sg = hi ? -1. : 1.;
   if(h < hN && h > 0) {
-    d_contact_forget(p, key);
+    d_contact_forget(p, key, A.overrun);
     if(h < eps * p->r) h = eps * p->r;
     double ah = ai / h - ai / hN, lnah = log(hN / h);
     double Un = vel[ax] - wv[ax];
@@ -1637,7 +1669,8 @@ __device__ void d_wall_force(part_struct *p, int ax, int hi, const coll_args &A,
     double Un = sg * (vel[ax] - wv[ax]);
     double Ut1 = 0.5 * (vel[t1] + vel0[t1]) - sd[t1];
     double Ut2 = 0.5 * (vel[t2] + vel0[t2]) - sd[t2];
-    int q = d_contact_slot(p, key, 1. / 9. * p->rho / rhof * 2. * p->r * fabs(Un) / nu);
+    double St_now = 1. / 9. * p->rho / rhof * 2. * p->r * fabs(Un) / nu;
+    int q = d_contact_slot(p, key, St_now, A.overrun);
     double o[3] = {0.5 * (om[0] + om0[0]), 0.5 * (om[1] + om0[1]), 0.5 * (om[2] + om0[2])};
     double so = (ax == 1) ? -1. : 1.;
     double o2 = ax == 0 ? o[0] : o[t1];
@@ -1650,7 +1683,7 @@ __device__ void d_wall_force(part_struct *p, int ax, int hi, const coll_args &A,
     double k = 4. / 3. / ((1. - p->sigma * p->sigma) / p->E + (1. - p->sigma * p->sigma) / p->E)
       / sqrt(1. / ai);
     double xcx0 = 1.e-4;
-    double e = p->e_dry + (1. + p->e_dry) / d_st_get(p, q) * log(xcx0);
+    double e = p->e_dry + (1. + p->e_dry) / d_contact_st(p, q, St_now) * log(xcx0);
     if(e < 0) e = 0;
     double alpha = -2.263 * pow(e, 0.3948) + 2.22;
     double eta = alpha * sqrt(4. / 3. * PI * ai * ai * ai * p->rho * k * sqrt(-h));
@@ -1855,6 +1888,7 @@ static coll_args make_coll_args(void)
   coll_args A;
   A.mu = mu; A.rho_f = rho_f; A.nu = nu; A.dt = dt;
   A.ilr = (int)interactionLengthRatio;
+  A.overrun = g_opt.contact_overrun;
   A.xs = Dom.xs; A.xe = Dom.xe; A.xl = Dom.xl;
   A.ys = Dom.ys; A.ye = Dom.ye; A.yl = Dom.yl;
   A.zs = Dom.zs; A.ze = Dom.ze; A.zl = Dom.zl;

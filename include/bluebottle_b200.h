@@ -172,6 +172,15 @@ typedef struct bbb_options {
                               replacements (reliable updates, falling back
                               to a restart on breakdown); 0 restarts it at
                               every sweep                                  */
+  int contact_overrun;     /* 1: the sphere/wall contact-list searches run
+                              one slot past iSt / St as the reference's
+                              collision kernels do (reading and writing the
+                              part_struct bytes after those arrays: the low
+                              word of e_dry, iSt[0..1]), for byte-for-byte
+                              comparison with them; 0 (default): the
+                              searches stop at the list's end and a contact
+                              that finds no free slot uses its current
+                              Stokes number unstored                       */
 } bbb_options;
 
 void bbb_default_options(bbb_options *opt);
@@ -360,7 +369,8 @@ void bbb_learn_use_reference_conv(int on);
  *     the grid to nx*ny*nz <= 64^3 cells, and larger requests return
  *     BBB_ERR_TOO_LARGE.
  *   - The first call on a device looks up that array's device address
- *     (with that device current); make that first call before any stream
+ *     (with that device current; host threads calling for the first time
+ *     together take one look-up); make that first call before any stream
  *     capture.
  *   - Every call shares the array and it keeps the last call's contents:
  *     calls that overlap on the GPU (other streams, other host threads)

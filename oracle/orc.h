@@ -42,6 +42,9 @@ typedef struct orc_params {
   g_struct g;
   gradP_struct gradP;
   int stepnum;
+  int contact_overrun;        /* 1: contact-list searches reach slot 12 as
+                                 the reference's kernels do (option
+                                 contact_overrun of the library)          */
 } orc_params;
 
 typedef struct orc_state {

@@ -30,7 +30,8 @@ class OrcParams(C.Structure):
                 ("pid_int", C.c_double), ("pid_back", C.c_double),
                 ("interactionLengthRatio", C.c_double),
                 ("bc", abi.BCStruct), ("g", abi.GStruct),
-                ("gradP", abi.GStruct), ("stepnum", C.c_int)]
+                ("gradP", abi.GStruct), ("stepnum", C.c_int),
+                ("contact_overrun", C.c_int)]
 
 
 _lib = None
@@ -169,13 +170,15 @@ class Oracle:
 
     @classmethod
     def _from_host(cls, dom, nparts, coeff_stride, scalar, array, bc, g, gradP,
-                   parts_addr, implicit, fixed_dt, lamb_override, prepare):
+                   parts_addr, implicit, fixed_dt, lamb_override, prepare,
+                   contact_overrun=0):
         o = cls(dom, nparts, coeff_stride)
         P = o.P
         for k in cls.REAL_PARAMS + cls.INT_PARAMS:
             setattr(P, k, scalar(k))
         P.implicit = implicit
         P.fixed_dt = fixed_dt
+        P.contact_overrun = contact_overrun
         if lamb_override > 0:
             P.lamb_max_iter = lamb_override
         C.memmove(C.byref(P.bc), C.byref(bc), C.sizeof(abi.BCStruct))
@@ -209,7 +212,8 @@ class Oracle:
             sim.dom, n, sim.scalar("coeff_stride"), sim.scalar,
             lambda name, size: sim.array(name), sim.bc, sim.g, sim.gradP,
             addr, sim.options.implicit, sim.options.fixed_dt,
-            sim.options.lamb_max_iter_override, prepare)
+            sim.options.lamb_max_iter_override, prepare,
+            sim.options.contact_overrun)
 
     @classmethod
     def from_reference(cls, ref, implicit=1, fixed_dt=0.0, lamb_override=0,

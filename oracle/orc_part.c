@@ -898,26 +898,53 @@ static void st_set(part_struct *q, int k, real v)
   memcpy((char *)q->St + sizeof(real) * (size_t)k, &v, sizeof(real));
 }
 
+/* 1 while the current interaction pass emulates the reference's slot-12
+ * accesses (orc_params.contact_overrun); 0 keeps the searches inside the
+ * 12 slots, as the library does by default */
+static int g_overrun;
+
 /* lubrication range entered: drop `key` from the contact list */
 static void contact_forget(part_struct *q, int key)
 {
   int k = 0;
-  while(ist_get(q, k) != key && k < ORC_MAXN) k++;
-  if(ist_get(q, k) == key) { ist_set(q, k, -1); st_set(q, k, 0.); }
+  if(g_overrun) {
+    while(ist_get(q, k) != key && k < ORC_MAXN) k++;
+    if(ist_get(q, k) == key) { ist_set(q, k, -1); st_set(q, k, 0.); }
+    return;
+  }
+  while(k < ORC_MAXN && ist_get(q, k) != key) k++;
+  if(k < ORC_MAXN) { ist_set(q, k, -1); st_set(q, k, 0.); }
 }
 
-/* contact: slot of `key`, adding it with Stokes number `St` when new */
+/* contact: slot of `key`, adding it with Stokes number `St` when new;
+ * without the emulation -1 when the list is full (nothing stored) */
 static int contact_slot(part_struct *q, int key, real St)
 {
   int k = 0;
-  while(ist_get(q, k) != key && k < ORC_MAXN) k++;
-  if(k == ORC_MAXN) {
-    k = 0;
-    while(ist_get(q, k) != -1 && k < ORC_MAXN) k++;
-    ist_set(q, k, key);
-    st_set(q, k, St);
+  if(g_overrun) {
+    while(ist_get(q, k) != key && k < ORC_MAXN) k++;
+    if(k == ORC_MAXN) {
+      k = 0;
+      while(ist_get(q, k) != -1 && k < ORC_MAXN) k++;
+      ist_set(q, k, key);
+      st_set(q, k, St);
+    }
+    return k;
   }
+  while(k < ORC_MAXN && ist_get(q, k) != key) k++;
+  if(k < ORC_MAXN) return k;
+  k = 0;
+  while(k < ORC_MAXN && ist_get(q, k) != -1) k++;
+  if(k == ORC_MAXN) return -1;
+  ist_set(q, k, key);
+  st_set(q, k, St);
   return k;
+}
+
+/* stored Stokes number of a contact slot, or St when it has none */
+static real contact_st(const part_struct *q, int slot, real St)
+{
+  return slot >= 0 ? st_get(q, slot) : St;
 }
 
 typedef struct orc_bins {
@@ -1091,7 +1118,8 @@ static void pair_force(orc_state *st, int i, int j)
     Fnx = 0; Fny = 0; Fnz = 0; Ftx = 0; Fty = 0; Ftz = 0; Lox = 0; Loy = 0; Loz = 0;
   }
   if(h < 0) {
-    int q = contact_slot(pi, j, 1. / 9. * pi->rho / rhof * 2. * pi->r * fabs(udotn) / nu);
+    real St_now = 1. / 9. * pi->rho / rhof * 2. * pi->r * fabs(udotn) / nu;
+    int q = contact_slot(pi, j, St_now);
     real Vx = -utx + 0.5 * (ai + aj + h) * ocnx;
     real Vy = -uty + 0.5 * (ai + aj + h) * ocny;
     real Vz = -utz + 0.5 * (ai + aj + h) * ocnz;
@@ -1103,7 +1131,7 @@ static void pair_force(orc_state *st, int i, int j)
     real k = 4. / 3. / ((1. - pi->sigma * pi->sigma) / pi->E
       + (1. - pj->sigma * pj->sigma) / pj->E) / sqrt(1. / ai + 1. / aj);
     real xcx0 = 1.e-4;
-    real e = pi->e_dry + (1. + pi->e_dry) / st_get(pi, q) * log(xcx0);
+    real e = pi->e_dry + (1. + pi->e_dry) / contact_st(pi, q, St_now) * log(xcx0);
     if(e < 0) e = 0;
     real alpha = -2.263 * pow(e, 0.3948) + 2.22;
     real eta = alpha * sqrt(4. / 3. * PI * ai * ai * ai * pi->rho * k * sqrt(-h));
@@ -1254,7 +1282,8 @@ static void wall_force(orc_state *st, part_struct *p, int ax, int hi, real *Ftx_
     real Un = sg * (vel[ax] - wv[ax]);
     real Ut1 = 0.5 * (vel[t1] + vel0[t1]) - sd[t1];
     real Ut2 = 0.5 * (vel[t2] + vel0[t2]) - sd[t2];
-    int q = contact_slot(p, key, 1. / 9. * p->rho / rhof * 2. * p->r * fabs(Un) / nu);
+    real St_now = 1. / 9. * p->rho / rhof * 2. * p->r * fabs(Un) / nu;
+    int q = contact_slot(p, key, St_now);
     real o[3] = {0.5 * (om[0] + om0[0]), 0.5 * (om[1] + om0[1]), 0.5 * (om[2] + om0[2])};
     /* slip velocity at the contact point; the x walls take omega_x where
      * omega_y belongs (src/bluebottle_kernel.cu:2977, :3091) */
@@ -1269,7 +1298,7 @@ static void wall_force(orc_state *st, part_struct *p, int ax, int hi, real *Ftx_
     real k = 4. / 3. / ((1. - p->sigma * p->sigma) / p->E + (1. - p->sigma * p->sigma) / p->E)
       / sqrt(1. / ai);
     real xcx0 = 1.e-4;
-    real e = p->e_dry + (1. + p->e_dry) / st_get(p, q) * log(xcx0);
+    real e = p->e_dry + (1. + p->e_dry) / contact_st(p, q, St_now) * log(xcx0);
     if(e < 0) e = 0;
     real alpha = -2.263 * pow(e, 0.3948) + 2.22;
     real eta = alpha * sqrt(4. / 3. * PI * ai * ai * ai * p->rho * k * sqrt(-h));
@@ -1390,7 +1419,6 @@ static void move_parts(orc_state *st, int final)
   }
 }
 
-/* src/cuda_bluebottle.cu:4317-4433 */
 /* src/cuda_bluebottle.cu:4317-4433: interaction forces, the first
  * Newton-Euler half step, interaction forces again; the final call adds
  * the position update (move_parts_b) */
@@ -1398,6 +1426,7 @@ static void interactions(orc_state *st, int final)
 {
   int n = st->nparts;
   if(n <= 0) return;
+  g_overrun = st->P.contact_overrun;
   orc_bins B;
   memset(&B, 0, sizeof(B));
   if(n > 1) {

@@ -7,7 +7,9 @@
 # by an empty stub header.  Test infrastructure only.
 #
 #   make -f oracle/ref.mk REF=/path/to/reference/src
-REF ?= /root/reference/src
+# (default: $BLUEBOTTLE_REF/src, the checkout at /root/reference otherwise)
+BLUEBOTTLE_REF ?= /root/reference
+REF ?= $(BLUEBOTTLE_REF)/src
 HERE := $(dir $(lastword $(MAKEFILE_LIST)))
 OUT := $(HERE)_ref
 CC = gcc

@@ -1,6 +1,13 @@
+import os
+
 import numpy as np
 
 from bluebottle_b200 import interior
+
+# the reference checkout the reference-built checkers compile from (only
+# where it exists; the tests that need it skip otherwise)
+REF_ROOT = os.environ.get("BLUEBOTTLE_REF", "/root/reference")
+REF_SRC = os.path.join(REF_ROOT, "src")
 
 
 def rel_err(a, b):

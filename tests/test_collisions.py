@@ -19,7 +19,7 @@ PART_FIELDS = ("x", "y", "z", "u", "v", "w", "ox", "oy", "oz", "iFx", "iFy",
                "iFz", "iLx", "iLy", "iLz", "udot", "wdot", "oxdot", "ozdot")
 
 
-def _scene(tmp_path, dt=None, vel=True):
+def _scene(tmp_path, dt=None, vel=True, overrun=0):
     d = str(tmp_path)
     configs.write_flow_config(os.path.join(d, "flow.config"), n=(32, 32, 32),
                               lo=(0., 0., 0.), hi=(8., 8., 8.),
@@ -29,6 +29,7 @@ def _scene(tmp_path, dt=None, vel=True):
              dict(r=1.0, x=3.0, y=1.5, z=0.98), dict(r=1.0, x=6.5, y=6.6, z=6.5)]
     configs.write_part_config(os.path.join(d, "part.config"), parts, loa=1.0)
     opts = {"fixed_dt": dt} if dt else {}
+    opts["contact_overrun"] = overrun
     sim = Sim(input_dir=d, options=opts)
     if dt:
         sim.set_scalar("dt", dt)
@@ -76,6 +77,80 @@ def test_contact_laws_on_the_oracle(tmp_path):
     lub = -6 * math.pi * mu * 1.0 * 0.05 * (1.0 / hl - 1.0 / 1.0)
     assert math.isclose(q[3].iFz, lub, rel_tol=1e-6)
     o.close()
+
+
+def _fill_contact_list(P):
+    """Sphere 0 keeps 12 stored contacts with other keys, so its new contact
+    with sphere 1 finds no free slot."""
+    for k in range(12):
+        P[0].iSt[k] = 100 + k
+        P[0].St[k] = 5.0 + k
+
+
+@pytest.mark.parametrize("overrun", [0, 1])
+def test_full_contact_list_on_the_oracle(tmp_path, overrun):
+    """A new contact on a full list: with the reference's slot-12 accesses
+    (contact_overrun = 1) the key lands in the bytes after iSt, the low word
+    of e_dry; without them (the default) nothing outside the list changes
+    and the contact uses its current Stokes number."""
+    import ctypes as C
+    sim = _scene(tmp_path, dt=1e-12, vel=False, overrun=overrun)
+    _fill_contact_list(sim.parts())
+    o = Oracle.from_sim(sim, prepare=False)
+    sim.close()
+    o.P.dt = 1e-12
+    o.lib.orc_move_parts_sub(o.st)
+    q = o.field("parts")[0]
+    low = C.c_int.from_address(C.addressof(q) + type(q).e_dry.offset).value
+    if overrun:
+        # iSt[12] is the low word of e_dry (the partner's key lands there)
+        # and St[12] the 8 bytes of iSt[0..1] (the stored Stokes number)
+        assert low == 1
+        assert q.e_dry != 1.0
+        assert list(q.iSt)[2:] == [100 + k for k in range(2, 12)]
+        st12 = C.c_double.from_address(C.addressof(q.iSt)).value
+        assert st12 > 0 and math.isfinite(st12)
+    else:
+        assert q.e_dry == 1.0
+        assert list(q.iSt) == [100 + k for k in range(12)]
+    assert math.isfinite(q.iFx) and q.iFx < 0
+    o.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("overrun", [0, 1])
+def test_gpu_full_contact_list_matches_oracle(gpu, tmp_path, overrun):
+    sim = _scene(tmp_path, dt=0.01, overrun=overrun)
+    _fill_contact_list(sim.parts())
+    orc = Oracle.from_sim(sim, prepare=False)
+    try:
+        sim.prepare()
+        lib = sim.lib
+        lib.cuda_part_push()
+        for _ in range(2):
+            lib.cuda_move_parts_sub()
+            orc.lib.orc_move_parts_sub(orc.st)
+        lib.cuda_part_pull()
+        g, c = sim.parts(), orc.field("parts")
+        for q in range(4):
+            for f in PART_FIELDS + ("e_dry",):
+                a, b = getattr(g[q], f), getattr(c[q], f)
+                assert abs(a - b) <= 1e-11 * max(1.0, abs(b)), (q, f, a, b)
+            if overrun and q == 0:
+                # iSt[0..1] hold the bytes of the stored Stokes number
+                # (St[12]), which GPU and CPU round differently in the
+                # last bits: compared as that double
+                import ctypes as C
+                sa = C.c_double.from_address(C.addressof(g[q].iSt)).value
+                sb = C.c_double.from_address(C.addressof(c[q].iSt)).value
+                assert abs(sa - sb) <= 1e-11 * abs(sb)
+                assert list(g[q].iSt)[2:] == list(c[q].iSt)[2:], q
+            else:
+                assert list(g[q].iSt) == list(c[q].iSt), q
+        assert (g[0].e_dry == 1.0) == (overrun == 0)
+    finally:
+        sim.close()
+        orc.close()
 
 
 @pytest.mark.gpu

@@ -16,7 +16,7 @@ import pytest
 from bluebottle_b200 import configs
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REFSRC = "/root/reference/src"
+from tests.helpers import REF_SRC as REFSRC  # noqa: E402
 DROPIN = os.path.join(ROOT, "oracle", "_ref", "libref_dropin.so")
 
 

@@ -31,7 +31,7 @@ from bluebottle_b200 import configs
 pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REFSRC = "/root/reference/src"
+from tests.helpers import REF_SRC as REFSRC  # noqa: E402
 REFGPU = {"explicit": os.path.join(ROOT, "oracle", "_ref", "libref_gpu.so"),
           "implicit": os.path.join(ROOT, "oracle", "_ref", "libref_gpu_implicit.so")}
 

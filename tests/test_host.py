@@ -225,10 +225,11 @@ def test_written_part_config_reads_back(tmp_path):
     finally:
         back.close()
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    if os.path.isdir("/root/reference/src"):
+    from tests.helpers import REF_SRC
+    if os.path.isdir(REF_SRC):
         import subprocess
         subprocess.run(["make", "-s", "-f", os.path.join(root, "oracle", "ref.mk"),
-                        "REF=/root/reference/src"], check=True, cwd=root)
+                        "REF=" + REF_SRC], check=True, cwd=root)
     ref = os.path.join(root, "oracle", "_ref", "libref_host.so")
     if not os.path.exists(ref):
         return

@@ -18,7 +18,7 @@ from bluebottle_b200 import Sim, abi, configs
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REFLIB = os.path.join(ROOT, "oracle", "_ref", "libref_host.so")
-REFSRC = "/root/reference/src"
+from tests.helpers import REF_SRC as REFSRC  # noqa: E402
 
 
 def _reflib():

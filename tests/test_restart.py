@@ -14,7 +14,7 @@ import pytest
 from bluebottle_b200 import Sim, abi, configs
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REFSRC = "/root/reference/src"
+from tests.helpers import REF_SRC as REFSRC  # noqa: E402
 
 FACE = {"u": "Gfx", "u0": "Gfx", "diff0_u": "Gfx", "conv0_u": "Gfx",
         "diff_u": "Gfx", "conv_u": "Gfx", "u_star": "Gfx",
