@@ -8,7 +8,7 @@
  * array one box of 10 rows x (128 + two 16-byte x-halo chunks), the mask
  * likewise, the block's own 8 rows of the arrays only it reads -- into a
  * shared-memory stage whose mbarrier completes when all bytes have landed.
- * AS_NS stages rotate, so the next plane is in flight while the block
+ * NS stages rotate, so the next plane is in flight while the block
  * computes this one (two stages measured faster than three, four or five
  * on 256x256x512: pass A 2%, pass B 5%, the FP64 pass B 7%); the warps
  * synchronise only through the stages' barriers and release counts, never
@@ -36,8 +36,21 @@
 #include <cuda.h>
 
 #define AS_W 128
-#define AS_NS 2
 #define AS_THREADS 256
+/* pipeline stages and resident blocks per SM of the FP32 passes (the FP64
+ * ones keep 2 stages); build-time switches for measurement */
+#ifndef BBB_AS_NS_A
+#define BBB_AS_NS_A 2
+#endif
+#ifndef BBB_AS_NS_B
+#define BBB_AS_NS_B 2
+#endif
+#ifndef BBB_AS_MINB_A
+#define BBB_AS_MINB_A 2
+#endif
+#ifndef BBB_AS_MINB_B
+#define BBB_AS_MINB_B 3
+#endif
 
 __host__ __device__ constexpr int as_rup(int v, int a) { return (v + a - 1) / a * a; }
 
@@ -69,14 +82,19 @@ struct as_layout {
   static constexpr int OWN_OFF = MASK_OFF + MREG;
   static constexpr int XW_OFF = OWN_OFF + NO * 8 * OWNB;
   static constexpr int STAGE = as_rup(XW_OFF + (NA + 1) * 256, 128);
-  static constexpr int TAB_OFF = AS_NS * STAGE;
+  /* stages in the ring */
+  static constexpr int NS = ESZ == 4 ? (PASS == 1 ? BBB_AS_NS_B
+                                        : (PASS == 0 ? BBB_AS_NS_A : 2)) : 2;
+  static constexpr int TAB_OFF = NS * STAGE;
   static constexpr int BAR_OFF = TAB_OFF + 2 * 128 * ESZ;
-  static constexpr int CNT_OFF = BAR_OFF + AS_NS * 8;   /* release counts */
-  static constexpr int SH_OFF = as_rup(CNT_OFF + AS_NS * 4, 16);
+  static constexpr int CNT_OFF = BAR_OFF + NS * 8;      /* release counts */
+  static constexpr int SH_OFF = as_rup(CNT_OFF + NS * 4, 16);
   /* + 128: the dynamic window is aligned up to 128 bytes at run time */
   static constexpr int SMEM = SH_OFF + 32 * 5 * 8 + 128;
   /* resident blocks per SM the register budget targets */
-  static constexpr int MINB = ESZ == 4 ? (PASS == 1 ? 3 : 2) : (PASS == 0 ? 1 : 2);
+  static constexpr int MINB = ESZ == 4 ? (PASS == 1 ? BBB_AS_MINB_B
+                                          : (PASS == 0 ? BBB_AS_MINB_A : 2))
+                                       : (PASS == 0 ? 1 : 2);
   /* plane-aligned group runs (retile): off -- grouping neighbouring tiles
    * gets the same L2 reuse without idle slots */
   static constexpr bool ALIGN = false;
@@ -429,7 +447,7 @@ __device__ __forceinline__ T as_q1(const uint8_t *h, int stride, unsigned m,
  * Per plane: wait for the stage; each warp forms q of its row (with the
  * pointwise work where the plane is the block's) and of its south / north
  * rows and x-halo cells; releases the stage (the last warp to release it
- * refills it with the plane AS_NS ahead); then the stencil and epilogue of
+ * refills it with the plane NS ahead); then the stencil and epilogue of
  * the plane below, from registers. */
 template <typename T, int PASS>
 __global__ void __launch_bounds__(AS_THREADS, as_layout<T, PASS>::MINB)
@@ -449,7 +467,7 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
   const int tid = threadIdx.x, tx = tid & 31, w = tid >> 5;
   uint32_t *rel = reinterpret_cast<uint32_t *>(sm + L::CNT_OFF);
   if(tid == 0) {
-    for(int b = 0; b < AS_NS; b++) { as_bar_init(as_saddr(&bars[b])); rel[b] = 0u; }
+    for(int b = 0; b < L::NS; b++) { as_bar_init(as_saddr(&bars[b])); rel[b] = 0u; }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   optab_fill<T>(tab, O);                  /* ends with a barrier */
@@ -483,8 +501,8 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
     const int cnt = k1 - k0 + 2;
     const long long L0 = nload;
     if(tid == 0)
-      for(int a = 0; a < AS_NS && a < cnt; a++) {
-        int b = (int)((L0 + a) % AS_NS);
+      for(int a = 0; a < L::NS && a < cnt; a++) {
+        int b = (int)((L0 + a) % L::NS);
         as_issue<T, PASS>(B, A, M, sbase + b * L::STAGE, as_saddr(&bars[b]), i0, j0,
           mapz(B, k0 - 1 + a), E);
       }
@@ -536,8 +554,8 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
     for(int a = 0; a < cnt; a++) {
       const int pl = k0 - 1 + a;
       const long long Ld = L0 + a;
-      const int buf = (int)(Ld % AS_NS);
-      const uint32_t par = (uint32_t)((Ld / AS_NS) & 1);
+      const int buf = (int)(Ld % L::NS);
+      const uint32_t par = (uint32_t)((Ld / L::NS) & 1);
       const uint8_t *st = sm + buf * L::STAGE;
       if(!as_wait(as_saddr(&bars[buf]), par)) bad = 1;
       const bool full = pl >= k0 && pl < k1;
@@ -557,14 +575,14 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
         }
       }
       /* release the stage: the last of the 8 warps to finish reading it
-       * refills it with the plane AS_NS ahead (no block-wide barrier, so
+       * refills it with the plane NS ahead (no block-wide barrier, so
        * warps drift apart by up to the stage depth) */
       __syncwarp();
       if(tx == 0) {
         uint32_t old = as_release(as_saddr(&rel[buf]));
-        if(old % 8u == 7u && a + AS_NS < cnt)
+        if(old % 8u == 7u && a + L::NS < cnt)
           as_issue<T, PASS>(B, A, M, sbase + buf * L::STAGE, as_saddr(&bars[buf]),
-            i0, j0, mapz(B, pl + AS_NS), E);
+            i0, j0, mapz(B, pl + L::NS), E);
       }
       if(a >= 2 && valid) {
         const int k = pl - 1;
@@ -618,9 +636,9 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
     /* a stage never completed: let whatever is still landing finish
      * before the block's shared memory is released */
     if(nload > 0)
-      for(int b = 0; b < AS_NS; b++) {
-        long long last = nload - 1 - ((nload - 1 - b) % AS_NS + AS_NS) % AS_NS;
-        if(last >= 0) as_wait(as_saddr(&bars[b]), (uint32_t)((last / AS_NS) & 1));
+      for(int b = 0; b < L::NS; b++) {
+        long long last = nload - 1 - ((nload - 1 - b) % L::NS + L::NS) % L::NS;
+        if(last >= 0) as_wait(as_saddr(&bars[b]), (uint32_t)((last / L::NS) & 1));
       }
     if(tid == 0) atomicOr(&s->pad, 1);
   }
