@@ -39,14 +39,16 @@ REF_STEPS = 2           # whole CPU steps the reference arm times at most
 
 # kernel kinds timed live (bbb_profile_get_pass numbering) and their names
 # in the FP32-inner form
-KERNELS = ((0, "k_bicg_async<float,0>", "BiCGSTAB pass A (FP32): reads s, t, "
-            "p, v, x, rh, mask; writes r, x, p, v: 10 words + 1 mask byte"),
+KERNELS = ((0, "k_bicg_async<float,0>", "BiCGSTAB pass A (FP32): reads r, t, "
+            "p, v, x, rh, mask (s = r - alpha v formed in registers); writes "
+            "r, x, p, v: 10 words + 1 mask byte"),
            (1, "k_bicg_async<float,1>", "BiCGSTAB pass B (FP32): reads r, v, "
-            "rh, mask; writes s, t: 5 words + 1 mask byte"),
+            "rh, mask; writes t: 4 words + 1 mask byte"),
            (2, "k_bicg_async<double,2>", "FP64 outer residual: reads x, b "
             "(FP64), mask; writes r (FP32): 21 bytes"),
-           (3, "k_cg1<float,4>", "Helmholtz CG stencil pass (FP32): reads r, "
-            "p, mask; writes p, Ap: 4 words + 1 byte"),
+           (3, "k_bicg_async<float,3>", "Helmholtz CG stencil pass (FP32, "
+            "staged like the BiCGSTAB passes): reads r, p, mask; writes p, Ap: "
+            "4 words + 1 byte"),
            (4, "k_cg2<float>", "Helmholtz CG pointwise pass (FP32): reads p, "
             "x, Ap, r, mask; writes x, r: 6 words + 1 byte"),
            (5, "k_star_rhs", "Crank-Nicolson momentum RHS (FP64), one "
@@ -391,7 +393,7 @@ def kernel_table(form, peak, fp64=False):
         if pn <= 0 or pms <= 0:
             continue
         if fp64 and k in (0, 1, 3, 4):
-            name = name.replace("float", "double").replace("<double,4>", "<double,2>")
+            name = name.replace("float", "double")
             what = what.replace("FP32", "FP64")
         gbs = pby / (pms / 1000.0) / 1e9
         rows[name] = {"launches": pn, "ms_per_launch": pms / pn,

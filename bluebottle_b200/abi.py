@@ -101,7 +101,8 @@ class Stats(C.Structure):
                 ("extrap_r0", C.c_double), ("guess_evaluated", C.c_int),
                 ("guess_cost_ms", C.c_double), ("guess_benefit_ms", C.c_double),
                 ("step_dt", C.c_double), ("cfl_adv", C.c_double),
-                ("helm_solves", C.c_int), ("pp_iters_max", C.c_int)]
+                ("helm_solves", C.c_int), ("pp_iters_max", C.c_int),
+                ("pp_iters_first", C.c_int)]
 
 
 PERIODIC, DIRICHLET, NEUMANN, PRECURSOR = 0, 1, 2, 3

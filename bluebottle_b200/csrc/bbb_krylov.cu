@@ -1186,33 +1186,43 @@ static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
   bool staged = BBB_ASYNC_ON && B.nx % AS_W == 0 && as_per_sm<T, 0>() > 0
     && as_per_sm<T, 1>() > 0;
   boxc BA = B, BB = B;
-  as_maps MA[2], MB[2];   /* pass A maps reading p, v of buffer c; pass B
-                             maps reading v of buffer c */
+  /* The staged passes keep r in two buffers, rr[0] = sv and rr[1] = r:
+   * pass A reads r from rr[rc] and writes the new r to rr[rc ^ 1], and
+   * pass B, which stores no s, reads r from rr[rc].  A fresh solve's
+   * set-up leaves s = r0 in sv, which the opening pass A reads as its r
+   * (rc = 0); a resumed run starts with pass B on the replaced residual
+   * the set-up wrote to r (rc = 1). */
+  T *rr[2] = {sv, r};
+  int rc = resume ? 1 : 0;
+  as_maps MA[2][2], MB[2][2];   /* [r buffer][p, v buffer] */
   if(staged) {
     BA = retile(B, as_per_sm<T, 0>(), as_layout<T, 0>::ALIGN);
     BB = retile(B, as_per_sm<T, 1>(), as_layout<T, 1>::ALIGN);
-    for(int c = 0; c < 2 && staged; c++) {
-      const T *ha[4] = {sv, tv, pp[c], vv[c]}, *oa[2] = {x, rh};
-      const T *hb[4] = {r, vv[c], NULL, NULL}, *ob[2] = {rh, NULL};
-      staged = as_pass_maps<T, 0>(&MA[c], BA, mask, ha, oa)
-            && as_pass_maps<T, 1>(&MB[c], BB, mask, hb, ob);
-    }
+    for(int q = 0; q < 2 && staged; q++)
+      for(int c = 0; c < 2 && staged; c++) {
+        const T *ha[4] = {rr[q], tv, pp[c], vv[c]}, *oa[2] = {x, rh};
+        const T *hb[4] = {rr[q], vv[c], NULL, NULL}, *ob[2] = {rh, NULL};
+        staged = as_pass_maps<T, 0>(&MA[q][c], BA, mask, ha, oa)
+              && as_pass_maps<T, 1>(&MB[q][c], BB, mask, hb, ob);
+      }
   }
-  /* pass A: reads p, v of buffer cur, writes buffer cur ^ 1, then cur flips */
+  /* pass A: reads p, v of buffer cur, writes buffer cur ^ 1, then cur flips
+   * (and, staged, the r buffer with it) */
   auto pass_a = [&]() {
-    /* the opening pass of a fresh solve reads s, rh; later ones s, t, p, v,
-     * x, rh; + mask */
+    /* the opening pass of a fresh solve reads s, rh; later ones s (staged:
+     * r), t, p, v, x, rh; + mask */
     double a_bytes = (launched == 0 && !resume) ? (double)n * (5. * w + 1.)
                                                 : (double)n * (10. * w + 1.);
     prof_begin(BBB_PROF_PASS_A, a_bytes);
     if(staged) {
-      as_args<T> A;
+      as_args<T> A = {};
       A.mask = mask;
-      A.h[0] = sv; A.h[1] = tv; A.h[2] = pp[cur]; A.h[3] = vv[cur];
-      A.w0 = r; A.w1 = pp[cur ^ 1]; A.w2 = vv[cur ^ 1]; A.x = x;
+      A.h[0] = rr[rc]; A.h[1] = tv; A.h[2] = pp[cur]; A.h[3] = vv[cur];
+      A.w0 = rr[rc ^ 1]; A.w1 = pp[cur ^ 1]; A.w2 = vv[cur ^ 1]; A.x = x;
       A.s = s; A.partials = g_dev.partials;
       k_bicg_async<T, 0><<<BA.nblk, AS_THREADS, as_layout<T, 0>::SMEM,
-        g_dev.stream>>>(BA, O, A, MA[cur]);
+        g_dev.stream>>>(BA, O, A, MA[rc][cur]);
+      rc ^= 1;
     } else {
       k_bicgA<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, sv, tv, pp[cur],
         vv[cur], rh, r, pp[cur ^ 1], vv[cur ^ 1], x, s, g_dev.partials);
@@ -1222,17 +1232,18 @@ static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
     cur ^= 1;
     launched++;
   };
-  /* pass B: reads r and the latest v (buffer cur) */
+  /* pass B: reads r and the latest v (buffer cur); staged, it writes t
+   * only (4 words + mask per unknown), else s and t */
   auto pass_b = [&]() {
-    prof_begin(BBB_PROF_PASS_B, (double)n * (5. * w + 1.));
+    prof_begin(BBB_PROF_PASS_B, (double)n * ((staged ? 4. : 5.) * w + 1.));
     if(staged) {
-      as_args<T> A;
+      as_args<T> A = {};
       A.mask = mask;
-      A.h[0] = r; A.h[1] = vv[cur]; A.h[2] = NULL; A.h[3] = NULL;
-      A.w0 = sv; A.w1 = tv; A.w2 = NULL; A.x = NULL;
+      A.h[0] = rr[rc]; A.h[1] = vv[cur]; A.h[2] = NULL; A.h[3] = NULL;
+      A.w0 = NULL; A.w1 = tv; A.w2 = NULL; A.x = NULL;
       A.s = s; A.partials = g_dev.partials;
       k_bicg_async<T, 1><<<BB.nblk, AS_THREADS, as_layout<T, 1>::SMEM,
-        g_dev.stream>>>(BB, O, A, MB[cur]);
+        g_dev.stream>>>(BB, O, A, MB[rc][cur]);
     } else {
       k_bicgB<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, r, vv[cur],
         rh, sv, tv, s, g_dev.partials);
@@ -1311,6 +1322,7 @@ int bbb_poisson_solve(int record)
   BBB_CK(cudaStreamSynchronize(g_dev.stream));
   bbb_kry *h = g_dev.kry_host;
   real resid = h->bnorm > 0 ? h->rnorm / h->bnorm : h->rnorm;
+  if(g_stats.pp_solves == 0) g_stats.pp_iters_first = h->iter;
   g_stats.pp_solves++;
   g_stats.pp_iters_total += h->iter;
   g_stats.pp_iters_last = h->iter;
@@ -1687,6 +1699,7 @@ static int poisson_mixed(const boxc &BD, const boxc &BF, const opc &O,
   }
   bbb_kry *h = g_dev.kry_host;
   real resid = h->bnorm > 0 ? h->rnorm / h->bnorm : h->rnorm;
+  if(g_stats.pp_solves == 0) g_stats.pp_iters_first = inner_total;
   g_stats.pp_solves++;
   g_stats.pp_iters_total += inner_total;
   g_stats.pp_iters_last = inner_total;
@@ -2120,6 +2133,41 @@ __global__ void __launch_bounds__(256) k_cg_inner_setup(long long n, opc O,
   }
 }
 
+/* The Helmholtz CG stencil pass (p = M r + beta p_old, y = A p, (p, y))
+ * staged by tensor-map copies where the rows are a multiple of 128 cells
+ * (the v and w systems of a 256-wide box; the u system carries the
+ * duplicated periodic face and stays on the register-tiled k_cg1).  Maps
+ * for both direction buffers are made once per solve. */
+template <typename T>
+struct cg_staged {
+  bool on = false;
+  boxc B;
+  as_maps M[2];
+  cg_staged(const boxc &B0, const uint8_t *mask, const T *r, T *const *p)
+  {
+    B = B0;
+    on = BBB_ASYNC_ON && B0.nx % AS_W == 0 && as_per_sm<T, 3>() > 0;
+    if(!on) return;
+    B = retile(B0, as_per_sm<T, 3>(), as_layout<T, 3>::ALIGN);
+    for(int c = 0; c < 2 && on; c++) {
+      const T *h[4] = {r, p[c], NULL, NULL};
+      on = as_pass_maps<T, 3>(&M[c], B, mask, h, NULL);
+    }
+  }
+  /* reads r and p[cur], writes p[cur ^ 1] and y */
+  void launch(const opc &O, const uint8_t *mask, const T *r, T *const *p,
+    int cur, T *y, bbb_kry *s) const
+  {
+    as_args<T> A = {};
+    A.mask = mask;
+    A.h[0] = r; A.h[1] = p[cur];
+    A.w0 = p[cur ^ 1]; A.w1 = y;
+    A.s = s; A.partials = g_dev.partials;
+    k_bicg_async<T, 3><<<B.nblk, AS_THREADS, as_layout<T, 3>::SMEM,
+      g_dev.stream>>>(B, O, A, M[cur]);
+  }
+};
+
 template <int VD, int VF>
 static int helmholtz_mixed(const boxc &BD, const boxc &BF, const opc &O,
   const uint8_t *mask, long long n, bbb_geom G, int comp, int tr, real *star)
@@ -2135,6 +2183,7 @@ static int helmholtz_mixed(const boxc &BD, const boxc &BF, const opc &O,
   dim3 grdD = box_grid(BD), grdF = box_grid(BF), blk(TX, TY);
   int inner_total = 0;
   dc_guard guard(pp_max_iter);
+  const cg_staged<float> CS(BF, mask, g_dev.fr, g_dev.fp);
   for(int outer = 0; outer <= max_outer; outer++) {
     outer_resid<VD>(BD, O, mask, g_dev.kb, g_dev.kx, g_dev.fr, s, si, itol,
       guard.remaining(), 0, n);
@@ -2145,8 +2194,11 @@ static int helmholtz_mixed(const boxc &BD, const boxc &BF, const opc &O,
     const int pmark = prof_mark();
     drive(si, [&]() {
       prof_begin(BBB_PROF_CG1, (double)n * (4. * 4. + 1.));
-      k_cg1<float, VF><<<grdF, blk, 0, g_dev.stream>>>(BF, O, mask, g_dev.fr,
-        g_dev.fp[cur], g_dev.fp[cur ^ 1], g_dev.fv[0], si, g_dev.partials);
+      if(CS.on)
+        CS.launch(O, mask, g_dev.fr, g_dev.fp, cur, g_dev.fv[0], si);
+      else
+        k_cg1<float, VF><<<grdF, blk, 0, g_dev.stream>>>(BF, O, mask, g_dev.fr,
+          g_dev.fp[cur], g_dev.fp[cur ^ 1], g_dev.fv[0], si, g_dev.partials);
       BBB_LAUNCHED();
       prof_end();
       prof_begin(BBB_PROF_CG2, (double)n * (6. * 4. + 1.));
@@ -2241,9 +2293,12 @@ int bbb_helmholtz_solve(int comp)
   dim3 grd = box_grid(B), blk(TX, TY);
   int cur = 0;
   const int pmark = prof_mark();
+  const cg_staged<double> CS(B, mask, g_dev.kr, g_dev.kp);
   drive(s, [&]() {
     prof_begin(BBB_PROF_CG1, (double)n * (4. * 8. + 1.));
-    if(V == 2)
+    if(CS.on)
+      CS.launch(O, mask, g_dev.kr, g_dev.kp, cur, g_dev.kv[0], s);
+    else if(V == 2)
       k_cg1<double, 2><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, g_dev.kr,
         g_dev.kp[cur], g_dev.kp[cur ^ 1], g_dev.kv[0], s, g_dev.partials);
     else
@@ -2268,6 +2323,7 @@ int bbb_helmholtz_solve(int comp)
   g_stats.helm_iters_total += h->iter;
   g_stats.helm_solves++;
   bbb_record_solver("solver_helmholtz_expd.rec", h->iter, resid);
+  if(h->status == BBB_ERR_NONFINITE) bbb_set_status(BBB_ERR_NONFINITE, "Helmholtz");
   if(!h->converged) {
     bbb_set_status(BBB_ERR_NOT_CONVERGED, "Helmholtz");
     if(bbb_fail_exit()) {

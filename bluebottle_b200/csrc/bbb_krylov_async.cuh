@@ -1,9 +1,16 @@
-/* bbb_krylov_async.cuh -- the two BiCGSTAB passes with their inputs staged
- * by the tensor memory accelerator (included by bbb_krylov.cu, which
- * defines boxc, opc, optab, op_apply, mapx/y/z, lin and the reductions).
+/* bbb_krylov_async.cuh -- the two BiCGSTAB passes, the FP64 outer residual
+ * of the defect correction and the Helmholtz CG stencil pass with their
+ * inputs staged by the tensor memory accelerator (included by
+ * bbb_krylov.cu, which defines boxc, opc, optab, op_apply, mapx/y/z, lin
+ * and the reductions).
  *
- * Same arithmetic as k_bicgA / k_bicgB, for rows of a multiple of 128
- * cells.  A block owns a 128 x 8 tile and marches along z.  For every plane
+ * Same arithmetic as k_bicgA / k_bicgB / k_outer_resid / k_cg1, for rows
+ * of a multiple of 128 cells, with one difference in where a value lives:
+ * pass B does not store s = r - alpha v; pass A forms it again from the r
+ * and v it reads anyway (the same FP32 or FP64 expression, so the same
+ * bits), which takes one vector write out of every iteration.  Pass A
+ * reads r and writes the new r, so r alternates between two buffers (the
+ * second is the one s would have used).  A block owns a 128 x 8 tile and marches along z.  For every plane
  * it needs, one thread issues a handful of 3-D tensor copies -- per input
  * array one box of 10 rows x (128 + two 16-byte x-halo chunks), the mask
  * likewise, the block's own 8 rows of the arrays only it reads -- into a
@@ -37,37 +44,70 @@
 
 #define AS_W 128
 #define AS_THREADS 256
-/* pipeline stages and resident blocks per SM of the FP32 passes (the FP64
- * ones keep 2 stages); build-time switches for measurement */
-#ifndef BBB_AS_NS_A
-#define BBB_AS_NS_A 2
+/* pipeline stages and resident blocks per SM of each pass (F: FP32, D:
+ * FP64; 0 pass A, 1 pass B, 2 the FP64 outer residual, 3 the Helmholtz
+ * CG stencil pass); build-time switches for measurement */
+#ifndef BBB_AS_NS_F0
+#define BBB_AS_NS_F0 2
 #endif
-#ifndef BBB_AS_NS_B
-#define BBB_AS_NS_B 2
+#ifndef BBB_AS_NS_F1
+#define BBB_AS_NS_F1 2
 #endif
-#ifndef BBB_AS_MINB_A
-#define BBB_AS_MINB_A 2
+#ifndef BBB_AS_NS_D0
+#define BBB_AS_NS_D0 2
 #endif
-#ifndef BBB_AS_MINB_B
-#define BBB_AS_MINB_B 3
+#ifndef BBB_AS_NS_D1
+#define BBB_AS_NS_D1 2
+#endif
+#ifndef BBB_AS_NS_D2
+#define BBB_AS_NS_D2 2
+#endif
+#ifndef BBB_AS_NS_F3
+#define BBB_AS_NS_F3 2
+#endif
+#ifndef BBB_AS_NS_D3
+#define BBB_AS_NS_D3 2
+#endif
+#ifndef BBB_AS_MINB_F3
+#define BBB_AS_MINB_F3 3
+#endif
+#ifndef BBB_AS_MINB_D3
+#define BBB_AS_MINB_D3 2
+#endif
+#ifndef BBB_AS_MINB_F0
+#define BBB_AS_MINB_F0 2
+#endif
+#ifndef BBB_AS_MINB_F1
+#define BBB_AS_MINB_F1 3
+#endif
+#ifndef BBB_AS_MINB_D0
+#define BBB_AS_MINB_D0 1
+#endif
+#ifndef BBB_AS_MINB_D1
+#define BBB_AS_MINB_D1 2
+#endif
+#ifndef BBB_AS_MINB_D2
+#define BBB_AS_MINB_D2 2
 #endif
 
 __host__ __device__ constexpr int as_rup(int v, int a) { return (v + a - 1) / a * a; }
 
 /* Stage layout in bytes (T the element type, CH = 16 / sizeof(T)):
- *   per halo array (pass A: s, t, p, v; pass B: r, v) a region of
+ *   per halo array (pass A: r, t, p, v; pass B: r, v; outer residual: x;
+ *   CG: r, p) a region of
  *     10 box rows of [CH | 128 | CH] cells (tile rows j0-1 .. j0+8),
  *     2 extra rows of 128 cells (y = -1, y = ny);
  *   mask: 10 rows of [16 | 128 | 16] bytes, 2 extra rows of 128;
- *   own arrays (pass A: x, rh; pass B: rh): 8 rows of 128 cells;
+ *   own arrays (pass A: x, rh; pass B: rh; outer residual: b; CG: none):
+ *   8 rows of 128 cells;
  *   x-wrap chunks: per halo array and the mask [2 sides][8 rows][16 B].
  * Regions start on 128-byte boundaries (tensor-copy destinations). */
 template <typename T, int PASS>
 struct as_layout {
   static constexpr int ESZ = (int)sizeof(T);
   static constexpr int CH = 16 / ESZ;
-  static constexpr int NA = PASS == 0 ? 4 : (PASS == 1 ? 2 : 1);
-  static constexpr int NO = PASS == 0 ? 2 : 1;
+  static constexpr int NA = PASS == 0 ? 4 : (PASS == 1 || PASS == 3 ? 2 : 1);
+  static constexpr int NO = PASS == 0 ? 2 : (PASS == 3 ? 0 : 1);
   static constexpr int BOXW = AS_W + 2 * CH;        /* halo-array box  */
   static constexpr int BOXH = 10;
   static constexpr int MBOXW = AS_W + 32;            /* mask box        */
@@ -83,8 +123,10 @@ struct as_layout {
   static constexpr int XW_OFF = OWN_OFF + NO * 8 * OWNB;
   static constexpr int STAGE = as_rup(XW_OFF + (NA + 1) * 256, 128);
   /* stages in the ring */
-  static constexpr int NS = ESZ == 4 ? (PASS == 1 ? BBB_AS_NS_B
-                                        : (PASS == 0 ? BBB_AS_NS_A : 2)) : 2;
+  static constexpr int NS = ESZ == 4
+    ? (PASS == 0 ? BBB_AS_NS_F0 : (PASS == 3 ? BBB_AS_NS_F3 : BBB_AS_NS_F1))
+    : (PASS == 0 ? BBB_AS_NS_D0 : (PASS == 1 ? BBB_AS_NS_D1
+       : (PASS == 3 ? BBB_AS_NS_D3 : BBB_AS_NS_D2)));
   static constexpr int TAB_OFF = NS * STAGE;
   static constexpr int BAR_OFF = TAB_OFF + 2 * 128 * ESZ;
   static constexpr int CNT_OFF = BAR_OFF + NS * 8;      /* release counts */
@@ -92,9 +134,10 @@ struct as_layout {
   /* + 128: the dynamic window is aligned up to 128 bytes at run time */
   static constexpr int SMEM = SH_OFF + 32 * 5 * 8 + 128;
   /* resident blocks per SM the register budget targets */
-  static constexpr int MINB = ESZ == 4 ? (PASS == 1 ? BBB_AS_MINB_B
-                                          : (PASS == 0 ? BBB_AS_MINB_A : 2))
-                                       : (PASS == 0 ? 1 : 2);
+  static constexpr int MINB = ESZ == 4
+    ? (PASS == 0 ? BBB_AS_MINB_F0 : (PASS == 3 ? BBB_AS_MINB_F3 : BBB_AS_MINB_F1))
+    : (PASS == 0 ? BBB_AS_MINB_D0 : (PASS == 1 ? BBB_AS_MINB_D1
+       : (PASS == 3 ? BBB_AS_MINB_D3 : BBB_AS_MINB_D2)));
   /* plane-aligned group runs (retile): off -- grouping neighbouring tiles
    * gets the same L2 reuse without idle slots */
   static constexpr bool ALIGN = false;
@@ -117,7 +160,8 @@ template <typename T>
 struct as_args {
   const uint8_t *mask;
   const T *h[4];          /* halo arrays                                 */
-  T *w0, *w1, *w2;        /* pass A: r, p_new, v_new; pass B: s, t       */
+  T *w0, *w1, *w2;        /* pass A: r_new, p_new, v_new; pass B: -, t;
+                             CG: p_new, y = A p_new                     */
   T *x;                   /* pass A: x, updated in place                 */
   bbb_kry *s;
   double *partials;
@@ -313,6 +357,23 @@ struct as_scal {
   int first;
 };
 
+/* The Helmholtz CG direction at 4 cells (pass 3): p = M r + beta p_old
+ * (r array 0, p_old array 1 at h + stride), or p_old itself in the first
+ * iteration, where the set-up left p = M r -- the expression of prod_c1 */
+template <typename T>
+__device__ __forceinline__ void as_cg_q4(const uint8_t *h, int stride,
+  unsigned mw, const T *dinv, const as_scal &S, T (&q)[4])
+{
+  as_ld4<T>(h + stride, q);
+  if(!S.first) {
+    T rr[4];
+    const T be = (T)S.beta;
+    as_ld4<T>(h, rr);
+#pragma unroll
+    for(int a = 0; a < 4; a++) q[a] = (T)1. * (dinv[mbyte(mw, a)] * rr[a]) + be * q[a];
+  }
+}
+
 /* q at 4 consecutive cells of a staged row: h the first cell of array 0
  * (array a at h + a * AREG), mw the 4 mask bytes */
 template <typename T, int PASS>
@@ -328,12 +389,13 @@ __device__ __forceinline__ void as_q4(const uint8_t *h, unsigned mw,
       for(int a = 0; a < 4; a++) q[a] = dinv[mbyte(mw, a)] * ss[a];
     } else {
       T tt[4], pp[4], vv[4];
-      T om = (T)S.omega, be = (T)S.beta, bo = (T)S.bo;
+      T al = (T)S.alpha, om = (T)S.omega, be = (T)S.beta, bo = (T)S.bo;
       as_ld4<T>(h + 1 * L::AREG, tt);
       as_ld4<T>(h + 2 * L::AREG, pp);
       as_ld4<T>(h + 3 * L::AREG, vv);
 #pragma unroll
       for(int a = 0; a < 4; a++) {
+        ss[a] = ss[a] - al * vv[a];        /* s = r - alpha v, as pass B */
         T rr = ss[a] - om * tt[a];
         T pn = rr + be * pp[a] + bo * vv[a];
         q[a] = dinv[mbyte(mw, a)] * pn;
@@ -346,6 +408,8 @@ __device__ __forceinline__ void as_q4(const uint8_t *h, unsigned mw,
     as_ld4<T>(h + 1 * L::AREG, vv);
 #pragma unroll
     for(int a = 0; a < 4; a++) q[a] = dinv[mbyte(mw, a)] * (rr[a] - al * vv[a]);
+  } else if constexpr(PASS == 3) {
+    as_cg_q4<T>(h, L::AREG, mw, dinv, S, q);
   } else {
     as_ld4<T>(h, q);                   /* outer residual: q = x */
     (void)mw; (void)dinv; (void)S;
@@ -377,6 +441,7 @@ __device__ __forceinline__ void as_own4(const uint8_t *h, unsigned mw,
       as_ld4<T>(o, xx);
 #pragma unroll
       for(int a = 0; a < 4; a++) {
+        ss[a] = ss[a] - al * vv[a];        /* s = r - alpha v, as pass B */
         rr[a] = ss[a] - om * tt[a];
         pn[a] = rr[a] + be * pp[a] + bo * vv[a];
         T di = dinv[mbyte(mw, a)];
@@ -404,7 +469,14 @@ __device__ __forceinline__ void as_own4(const uint8_t *h, unsigned mw,
     }
     as_ld4<T>(o, raw1);
     as_dot4<T>(red[2], raw0, raw0);
-    as_st4<T>(A.w0 + gc, raw0);
+  } else if constexpr(PASS == 3) {
+    /* Helmholtz CG: the new direction p is stored (w0) and kept for the
+     * epilogue's (p, A p) */
+    as_cg_q4<T>(h, L::AREG, mw, dinv, S, q);
+#pragma unroll
+    for(int a = 0; a < 4; a++) raw0[a] = q[a];
+    as_st4<T>(A.w0 + gc, q);
+    (void)o; (void)raw1; (void)red;
   } else {
     /* outer residual: q = x (sum x over the owned cells), raw0 = b */
     as_ld4<T>(h, q);
@@ -428,6 +500,7 @@ __device__ __forceinline__ T as_q1(const uint8_t *h, int stride, unsigned m,
       T tt = *reinterpret_cast<const T *>(h + 1 * stride);
       T pp = *reinterpret_cast<const T *>(h + 2 * stride);
       T vv = *reinterpret_cast<const T *>(h + 3 * stride);
+      ss = ss - (T)S.alpha * vv;            /* s = r - alpha v, as pass B */
       T rr = ss - (T)S.omega * tt;
       pn = rr + (T)S.beta * pp + (T)S.bo * vv;
     }
@@ -436,13 +509,20 @@ __device__ __forceinline__ T as_q1(const uint8_t *h, int stride, unsigned m,
     T rr = *reinterpret_cast<const T *>(h);
     T vv = *reinterpret_cast<const T *>(h + stride);
     return dinv[m] * (rr - (T)S.alpha * vv);
+  } else if constexpr(PASS == 3) {
+    T pp = *reinterpret_cast<const T *>(h + stride);
+    if(S.first) return pp;
+    T rr = *reinterpret_cast<const T *>(h);
+    return (T)1. * (dinv[m] * rr) + (T)S.beta * pp;
   } else {
     (void)stride; (void)m; (void)dinv; (void)S;
     return *reinterpret_cast<const T *>(h);
   }
 }
 
-/* One BiCGSTAB pass (PASS 0: pass A, 1: pass B) over this block's units,
+/* One staged pass (PASS 0: BiCGSTAB pass A, 1: pass B, 2: the FP64 outer
+ * residual of the defect correction, 3: the Helmholtz CG stencil pass) over
+ * this block's units,
  * 256 threads = 8 warps, warp w owning tile row w, lane l cells 4l..4l+3.
  * Per plane: wait for the stage; each warp forms q of its row (with the
  * pointwise work where the plane is the block's) and of its south / north
@@ -609,6 +689,10 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
           as_dot4<T>(red[1], Aq, Aq);
           as_dot4<T>(red[3], r1c, r0c);
           as_dot4<T>(red[4], r1c, Aq);
+        } else if constexpr(PASS == 3) {
+          /* y = A p and (A p, p), as epi_c1 */
+          as_st4<T>(A.w1 + ge, Aq);
+          as_dot4<T>(red[0], Aq, r0c);
         } else {
           /* outer residual r = b - A x in FP64, stored rounded to FP32 */
           T rr[4];
@@ -643,8 +727,18 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
     if(tid == 0) atomicOr(&s->pad, 1);
   }
   /* the pass's reductions and scalar updates, as k_bicgA / k_bicgB /
-   * k_outer_resid */
-  if constexpr(PASS == 2) {
+   * k_outer_resid / k_cg1 */
+  if constexpr(PASS == 3) {
+    double r1[1] = {red[0]};
+    if(bbb_grid_partial<1>(r1, A.partials, &s->ticket, sh)) {
+      bbb_grid_finish_sum<1>(r1, A.partials, &s->ticket, sh);
+      if(tid == 0) {
+        s->alpha = s->rho / r1[0];
+        s->first = 0;
+        if(((volatile bbb_kry *)s)->pad) { s->status = BBB_ERR_CUDA; s->done = 1; }
+      }
+    }
+  } else if constexpr(PASS == 2) {
     double r3[3] = {red[0], red[1], red[2]};
     if(bbb_grid_partial<3>(r3, A.partials, &s->ticket, sh)) {
       bbb_grid_finish_sum<3>(r3, A.partials, &s->ticket, sh);

@@ -98,16 +98,25 @@ __device__ __forceinline__ void rhs_component(const rhs_args &A, int i, int j,
 #undef OFF
 }
 
+/* A block owns a 32 x 8 tile of (i, j) and marches through RHS_KZ planes
+ * along k, so the k - 1 and k + 1 neighbours a thread reads were read by
+ * the same block one plane earlier and come from L1, not L2. */
+#define RHS_KZ 8
+
 __global__ void __launch_bounds__(256) k_star_rhs(rhs_args A)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  int k = blockIdx.z + 1;
   const bbb_geom &G = A.G;
   if(i > G.nx + 1 || j > G.ny + 1) return;
-  if((A.comp_mask & 1) && j <= G.ny && k <= G.nz) rhs_component<0>(A, i, j, k);
-  if((A.comp_mask & 2) && i <= G.nx && k <= G.nz) rhs_component<1>(A, i, j, k);
-  if((A.comp_mask & 4) && i <= G.nx && j <= G.ny) rhs_component<2>(A, i, j, k);
+  const int k0 = blockIdx.z * RHS_KZ + 1;
+  const int k1 = min(k0 + RHS_KZ, G.nz + 2);
+#pragma unroll 1
+  for(int k = k0; k < k1; k++) {
+    if((A.comp_mask & 1) && j <= G.ny && k <= G.nz) rhs_component<0>(A, i, j, k);
+    if((A.comp_mask & 2) && i <= G.nx && k <= G.nz) rhs_component<1>(A, i, j, k);
+    if((A.comp_mask & 4) && i <= G.nx && j <= G.ny) rhs_component<2>(A, i, j, k);
+  }
 }
 
 void bbb_star_rhs(int comp_mask, int explicit_ab2)
@@ -129,7 +138,8 @@ void bbb_star_rhs(int comp_mask, int explicit_ab2)
   A.f[0] = -gradP.x / rho_f; A.f[1] = -gradP.y / rho_f; A.f[2] = -gradP.z / rho_f;
   A.comp_mask = comp_mask;
   A.explicit_ab2 = explicit_ab2;
-  dim3 blk(32, 8), grd((A.G.nx + 1 + 31) / 32, (A.G.ny + 1 + 7) / 8, A.G.nz + 1);
+  dim3 blk(32, 8), grd((A.G.nx + 1 + 31) / 32, (A.G.ny + 1 + 7) / 8,
+    (A.G.nz + 1 + RHS_KZ - 1) / RHS_KZ);
   /* algorithmic words per cell: u0, v0, w0 and p0, read by every
    * component, once; per component conv0 read, star and conv written
    * (+ diff0 read and diff written in the explicit form) */

@@ -263,6 +263,8 @@ typedef struct bbb_stats {
                               advective CFL number cuda_find_dt bounds     */
   int helm_solves;         /* Helmholtz (CG) solves in the step            */
   int pp_iters_max;        /* most iterations of one Poisson solve         */
+  int pp_iters_first;      /* iterations of the step's first Poisson solve
+                              (the one the learned guess may start)        */
 } bbb_stats;
 void bbb_get_stats(bbb_stats *st);
 
@@ -286,7 +288,8 @@ void bbb_reset_kernel_launches(void);
  * work while enabled (launches that returned at once after a solve had
  * converged are left out).  bbb_profile_get: the BiCGSTAB iterations'
  * total milliseconds, iteration count and algorithmic bytes (15 vector
- * words + 2 mask bytes per unknown and iteration).  bbb_profile_get_pass:
+ * words + 2 mask bytes per unknown and iteration; 14 words in the passes
+ * staged by tensor-map copies, whose pass B stores no s).  bbb_profile_get_pass:
  * milliseconds, launches and algorithmic bytes of one kernel kind --
  * 0: BiCGSTAB pass A (the p/v update and first stencil), 1: pass B (the
  * s/t update and second stencil), 2: the FP64 outer residual of the mixed

@@ -44,13 +44,16 @@ def test_c1_taylor_green_100_steps(gpu, prec):
     than that later (vortex stretching adds dissipation: 3.4e-3 below it at
     t = 1 in the oracle).  The pressure correction phi of a nearly steady
     pressure is small: relative to its own size the FP32-inner form's phi
-    differs by up to 6e-6 (measured) while the fields agree to 1e-8."""
+    differs by up to 6e-6 (measured) while the fields agree to 1e-8, and
+    the energy, quadratic in the fields, to 2e-9 (FP64 form: 1e-10)."""
     rows = oracle_run("c1", prec, 100, 10)
     _check_rows(rows, 1e-8, phi_tol=1e-9 if prec == 0 else 2e-5)
     dx = 2 * math.pi / 32
     lam = 3.0 * (2.0 / dx * math.sin(dx / 2)) ** 2
+    e_tol = 1e-10 if prec == 0 else 2e-9
     for r in rows:
-        assert abs(r["energy"] - r["energy_ref"]) <= 1e-10 * r["energy_ref"]
+        assert abs(r["energy"] - r["energy_ref"]) <= e_tol * r["energy_ref"], (
+            r["step"], r["energy"], r["energy_ref"])
         ratio = r["energy"] / r["energy0"] / math.exp(-2 * 0.01 * lam * r["time"])
         if r["step"] <= 10:
             assert abs(ratio - 1) < 2e-5, (r["step"], ratio)
