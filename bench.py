@@ -31,7 +31,11 @@ sys.path.insert(0, ROOT)
 METRIC = ("timesteps/s at 256x256x512+8000 spheres, learned/FP32 vs plain "
           "FP64, same tol")
 LAMB_ITERS = 3          # Lamb sub-iterations per step, fixed for the bench
-LEARN_ITERS = 200       # Adam steps of the learned guess before timing
+LEARN_ONLINE = 100      # Adam steps of the learned guess after each
+                        # warm-up step (on the crops recorded so far)
+LEARN_ITERS = 1000      # Adam steps after the warm-up, before timing
+LEARN_CROPS = 32        # training crops (128 x 32 x 32) recorded per
+                        # warm-up step, 12.5% of the 256x256x512 box
 PROBE_STEPS = 1         # untimed steps after the warm-up (the learned
                         # guess's cost probe); both forms take them, so both
                         # time the same step numbers
@@ -195,7 +199,8 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
     `warmup` untimed steps, PROBE_STEPS untimed steps, `steps` timed steps
     and `e2e_steps` end-to-end steps.  With `learned`, the warm-up steps
     record training crops of the first Poisson solve of each step, the net
-    is trained on them (outside the timed region), and the probe and timed
+    is trained on them after each warm-up step and once more after the
+    last (all outside the timed region), and the probe and timed
     steps start that solve from the gated learned guess.  The evaluation
     itself is cost-gated (bbb_learn_enable bit 4): the probe step measures
     the guess's cost and its estimated saving, and while the saving stays
@@ -208,12 +213,17 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
                                learned_guess=1 if learned else 0))
     lib = sim.lib
     sim.prepare()
-    for _ in range(warmup):
-        sim.step()
-    out = {}
     if learned:
         lib.bbb_learn_train.restype = C.c_double
         lib.bbb_learn_train.argtypes = [C.c_int, C.c_double]
+        if lib.bbb_learn_set_crops_per_step(LEARN_CROPS) != 0:
+            raise RuntimeError("bbb_learn_set_crops_per_step(%d)" % LEARN_CROPS)
+    for _ in range(warmup):
+        sim.step()
+        if learned:
+            lib.bbb_learn_train(LEARN_ONLINE, 1e-3)
+    out = {}
+    if learned:
         out["learn_crops"] = lib.bbb_learn_crops()
         out["learn_loss"] = lib.bbb_learn_train(LEARN_ITERS, 1e-3)
         lib.bbb_learn_enable(2 | 4)
@@ -493,7 +503,8 @@ def main():
                            "cfl_max": mixed["cfl_max"],
                            "learned_guess": None if args.no_learned else {
                                "train_crops": mixed.get("learn_crops"),
-                               "adam_steps": LEARN_ITERS,
+                               "crops_per_warmup_step": LEARN_CROPS,
+                               "adam_steps": LEARN_ITERS + LEARN_ONLINE * warmup,
                                "last_batch_rel_mse": mixed.get("learn_loss"),
                                "timed_steps_guess_evaluated":
                                    mixed.get("guess_evaluated_steps"),

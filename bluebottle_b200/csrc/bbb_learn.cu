@@ -155,13 +155,32 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
   for(int a = 0; a < 16; a++) v[a] = __uint_as_float(r[a]);
 }
 
+/* GELU in its tanh form (Hendrycks and Gimpel, "Gaussian Error Linear
+ * Units", 2016): gelu(z) = z/2 (1 + tanh(k (z + c z^3))), k = sqrt(2/pi),
+ * c = 0.044715, with the tanh of the hardware's special-function unit
+ * (PTX tanh.approx.f32, relative error about 2^-11, below the BF16
+ * rounding of the activations it feeds).  gelu_d is its derivative. */
+__device__ __forceinline__ float lg_tanh(float x)
+{
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+#define LG_GELU_K 0.7978845608028654f
+#define LG_GELU_C 0.044715f
+
 __device__ __forceinline__ float gelu(float z)
-{ return 0.5f * z * (1.f + erff(z * 0.70710678118654752f)); }
+{
+  float t = lg_tanh(LG_GELU_K * (z + LG_GELU_C * z * z * z));
+  return 0.5f * z * (1.f + t);
+}
 
 __device__ __forceinline__ float gelu_d(float z)
 {
-  return 0.5f * (1.f + erff(z * 0.70710678118654752f))
-    + z * 0.39894228040143268f * expf(-0.5f * z * z);
+  float t = lg_tanh(LG_GELU_K * (z + LG_GELU_C * z * z * z));
+  return 0.5f * (1.f + t)
+    + 0.5f * z * (1.f - t * t) * LG_GELU_K * (1.f + 3.f * LG_GELU_C * z * z);
 }
 
 __device__ __forceinline__ int wrap_or(int g, int n, int per)
@@ -922,6 +941,8 @@ static void lg_crop_store(void)
 /* one convolution layer on box B (tensor cores, or the FP32 reference
  * when `ref`) */
 static int g_lg_ref = 0;
+/* crops recorded per recorded step (bbb_learn_set_crops_per_step) */
+static int g_lg_per_step = 8;
 static void lg_conv(int mode, const lg_box &B, const bf16 *in, int layer,
   int transposed, float *pre, bf16 *act, float *out32)
 {
@@ -980,6 +1001,13 @@ extern "C" int bbb_learn_enable(int mode)
 }
 
 extern "C" void bbb_learn_use_reference_conv(int on) { g_lg_ref = on; }
+
+extern "C" int bbb_learn_set_crops_per_step(int n)
+{
+  if(n < 1 || n > 64) return BBB_ERR_CONFIG;
+  g_lg_per_step = n;
+  return BBB_OK;
+}
 
 /* the solve that follows is the first of a time step (called by
  * cuda_store_u, the last call of the reference's step) */
@@ -1104,8 +1132,7 @@ void bbb_learn_post_solve(void)
   lg_crop_store();
   bbb_geom G = bbb_make_geom();
   long long cc = (long long)L.cx * L.cy * L.cz;
-  int per_solve = 8;
-  for(int q = 0; q < per_solve; q++) {
+  for(int q = 0; q < g_lg_per_step; q++) {
     int slot = L.next;
     L.next = (L.next + 1) % L.cap;
     if(L.ncrop < L.cap) L.ncrop++;

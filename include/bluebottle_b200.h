@@ -355,6 +355,9 @@ int bbb_learn_forward(int nx, int ny, int nz, int px, int py, int pz,
 double bbb_learn_grad(int cx, int cy, int cz, int nb, int margin,
   const void *feat_d, const float *tgt_d, float *grad_host);
 void bbb_learn_use_reference_conv(int on);
+/* crops (128 x 32 x 32 cells, or the box where smaller) recorded at each
+ * recorded solve, 1..64 (8 by default); BBB_ERR_CONFIG outside that */
+int bbb_learn_set_crops_per_step(int n);
 
 /* Allocation-free pressure-Poisson solve.  No counterpart in the
  * reference: it is the FP64 solve of cuda_PP_bicgstab for callers that

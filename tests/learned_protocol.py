@@ -24,9 +24,14 @@ both initial residuals.
 Spheres are given Young's modulus `--E` (1e4 by default instead of the
 reference's 1e6): with the contact forces integrated explicitly at the
 flow's CFL time step, as the reference does, E = 1e6 throws a touching pair
-apart within one step (its contact time is far below dt), and a run of
-3000 steps at this volume fraction meets such pairs.  The Poisson problem
-the guess acts on does not depend on E.
+apart within one step (its contact time is far below dt).  The Poisson
+problem the guess acts on does not depend on E.  Even so the 256^3 run
+does not reach 3000 steps: at step 434 (seed 1) the advective CFL number
+jumps from 0.4 to 125 and the step fails on its time-step bound -- a pair
+closer than the quadrature shell (rs = 1.2 a), whose nodes then lie inside
+the partner, the failure the seeding gap of 0.5 a avoids at the start
+(the 128^3 configuration meets it at step 276).  The phases are therefore
+run shortened, `--gen-steps 250 --infer-steps 120`, inside that window.
 
 One JSON object per step, then a summary object.
 """

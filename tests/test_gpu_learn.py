@@ -70,7 +70,7 @@ def _torch_net(feat, W, b, dims, periodic, emulate_bf16=True):
             xp = torch.cat([lo, xp, hi], dim=dim)
         z = F.conv3d(xp, w) + torch.from_numpy(b[l]).reshape(1, NC, 1, 1, 1)
         if l < NL - 1:
-            x = F.gelu(z)
+            x = F.gelu(z, approximate="tanh")
             if emulate_bf16:
                 x = _bf16(x)
         else:
@@ -159,7 +159,7 @@ def test_parameter_gradient_matches_autograd(gpu):
         for l in range(NL):
             w = Wt[l].reshape(3, 3, 3, NC, NC).permute(3, 4, 0, 1, 2)
             z = F.conv3d(x, w, padding=1) + bt[l].reshape(1, NC, 1, 1, 1)
-            x = F.gelu(z) if l < NL - 1 else z
+            x = F.gelu(z, approximate="tanh") if l < NL - 1 else z
         out = x[0, 0]
         m = torch.zeros(cz * nb, cy, cx, dtype=torch.bool)
         for q in range(nb):
