@@ -142,6 +142,20 @@ def test_learned_guess_cost_gate():
     assert decide(0.0, 0.0, 1.0, 0.1, 1e-8) == 16
 
 
+def test_learned_guess_crops_per_step_range():
+    """bbb_learn_set_crops_per_step takes 1..64 crops per recorded solve and
+    refuses anything else with BBB_ERR_CONFIG, keeping the setting it had
+    (no device is touched)."""
+    lib = abi.load()
+    ERR_CONFIG = 3
+    for bad in (0, -1, 65, 1000):
+        assert lib.bbb_learn_set_crops_per_step(bad) == ERR_CONFIG
+    for good in (1, 32, 64):
+        assert lib.bbb_learn_set_crops_per_step(good) == 0
+    assert lib.bbb_learn_set_crops_per_step(8) == 0
+    assert lib.bbb_last_status() == 0
+
+
 def _walled_sim(tmp_path, periodic, screens=(0.0, 0.0)):
     """a 16 x 16 x 12 box without particles; non-periodic axes are walls,
     the bottom/top screens (bc.dsB, bc.dsT) as given"""
