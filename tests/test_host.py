@@ -148,6 +148,7 @@ def test_learned_guess_crops_per_step_range():
     (no device is touched)."""
     lib = abi.load()
     ERR_CONFIG = 3
+    lib.bbb_clear_status()
     for bad in (0, -1, 65, 1000):
         assert lib.bbb_learn_set_crops_per_step(bad) == ERR_CONFIG
     for good in (1, 32, 64):
