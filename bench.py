@@ -55,7 +55,7 @@ KERNELS = ((0, "k_bicg_async<float,0>", "BiCGSTAB pass A (FP32): reads r, t, "
             "4 words + 1 byte"),
            (4, "k_cg2<float>", "Helmholtz CG pointwise pass (FP32): reads p, "
             "x, Ap, r, mask; writes x, r: 6 words + 1 byte"),
-           (5, "k_star_rhs", "Crank-Nicolson momentum RHS (FP64), one "
+           (5, "k_star_rhs_z<C>", "Crank-Nicolson momentum RHS (FP64), one "
             "component per launch: u0, v0, w0, p0, conv0 read, u*, conv "
             "written: 7 words"))
 
