@@ -168,7 +168,8 @@ __global__ void __launch_bounds__(256) k_star_rhs(rhs_args A)
  * the neighbouring lanes by shuffles (lanes 0 and 31 read their outer
  * neighbour themselves), the rest are plain coalesced loads: 8 loads per
  * face of u and w, 10 of v, instead of 18.  The arithmetic is rhs_eval's,
- * so the results are the same bits as rhs_component's. */
+ * as in rhs_component (the compiler may fuse a multiply-add differently in
+ * the two kernels: a last-bit difference at most). */
 #define RHS_KZC 16
 /* resident blocks per SM the register budget targets: 3 (80 registers, a
  * few values spilled) measured 0.495 ms per component at 256x256x512
