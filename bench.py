@@ -194,7 +194,7 @@ def profiler_range(on):
 
 
 def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
-             learned=False, prof_range=False, keep=False):
+             learned=False, prof_range=False, keep=False, lamb_pp_tol=0.0):
     """One fresh simulation of the workload in precision form `prec`:
     `warmup` untimed steps, PROBE_STEPS untimed steps, `steps` timed steps
     and `e2e_steps` end-to-end steps.  With `learned`, the warm-up steps
@@ -210,7 +210,8 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
     import ctypes as C
     wl = workload(wl_name, prec)
     sim = Sim(wl, options=dict(lamb_max_iter_override=LAMB_ITERS,
-                               learned_guess=1 if learned else 0))
+                               learned_guess=1 if learned else 0,
+                               lamb_pp_tol=lamb_pp_tol))
     lib = sim.lib
     sim.prepare()
     if learned:
@@ -425,6 +426,10 @@ def main():
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the timed steps of the FP32 form with "
                     "cuProfilerStart/Stop (for ncu --profile-from-start off)")
+    ap.add_argument("--lamb-pp-tol", type=float, default=0.0,
+                    help="relative tolerance of the pressure solves of the "
+                    "Lamb sub-iterations before the last (0: every solve to "
+                    "1e-8, as the reference); applied to both forms")
     ap.add_argument("--workload", default="c5", choices=sorted(WORKLOADS),
                     help="c5: the headline 256x256x512 + 8000 spheres; small: "
                     "128x128x256 + 1000 spheres for profiler captures; tiny: "
@@ -449,7 +454,8 @@ def main():
     want_cpu = world == 1 and not args.no_cpu
     mixed = run_form(1, steps, warmup, e2e_steps=steps, wl_name=args.workload,
                      prof_range=args.profile_range,
-                     learned=not args.no_learned, keep=want_cpu)
+                     learned=not args.no_learned, keep=want_cpu,
+                     lamb_pp_tol=args.lamb_pp_tol)
     clocks = sampler.stop()
     ms = dist.max(mixed["ms"])
     e2e_ms = dist.max(mixed["e2e_ms"])
@@ -464,7 +470,8 @@ def main():
             sim.close()
     fp64 = None
     if not args.no_fp64:
-        fp64 = run_form(0, steps, warmup, e2e_steps=0, wl_name=args.workload)
+        fp64 = run_form(0, steps, warmup, e2e_steps=0, wl_name=args.workload,
+                        lamb_pp_tol=args.lamb_pp_tol)
         fp64["ms"] = dist.max(fp64["ms"])
     dist.barrier()
     if rank == 0:
@@ -499,6 +506,7 @@ def main():
                                warmup + PROBE_STEPS + 1,
                                warmup + PROBE_STEPS + steps, warmup, PROBE_STEPS),
                            "lamb_iters_per_step": LAMB_ITERS,
+                           "lamb_pp_tol": args.lamb_pp_tol or None,
                            "dt_range": mixed["dt_range"],
                            "cfl_max": mixed["cfl_max"],
                            "learned_guess": None if args.no_learned else {

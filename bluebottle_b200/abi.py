@@ -89,7 +89,8 @@ class Options(C.Structure):
                 ("max_outer", C.c_int), ("learned_guess", C.c_int),
                 ("record", C.c_int), ("gravity_balance", C.c_int),
                 ("lamb_max_iter_override", C.c_int), ("verbose", C.c_int),
-                ("reliable", C.c_int), ("contact_overrun", C.c_int)]
+                ("reliable", C.c_int), ("contact_overrun", C.c_int),
+                ("lamb_pp_tol", C.c_double)]
 
 
 class Stats(C.Structure):

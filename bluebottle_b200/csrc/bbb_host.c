@@ -33,6 +33,7 @@ WEAK real duration, ttime, vel_tDelay, p_tDelay, g_tDelay;
 WEAK real dt, dt0, CFL;
 WEAK int pp_max_iter;
 WEAK real pp_residual;
+real g_pp_tol_now = 0.;
 WEAK int lamb_max_iter;
 WEAK real lamb_residual, lamb_relax, lamb_cut;
 WEAK int out_plane, stepnum, init_cond;
@@ -76,6 +77,7 @@ void bbb_default_options(bbb_options *opt)
   opt->verbose = 0;
   opt->reliable = 0;
   opt->contact_overrun = 0;
+  opt->lamb_pp_tol = 0.;
 }
 
 static void opt_init(void)
@@ -941,7 +943,13 @@ int bbb_step(void)
                                                : lamb_max_iter;
   int iter = 0;
   real iter_err = FLT_MAX;
-  while(iter_err > lamb_residual) {
+  /* with options.lamb_pp_tol the pressure solves of all but the last
+   * sub-iteration stop at that looser tolerance; the step still ends on a
+   * solve to pp_residual (force_full: one more sub-iteration after a
+   * loosened one that met the coefficient criterion) */
+  const real loose = g_opt.lamb_pp_tol;
+  int force_full = 0;
+  while(iter_err > lamb_residual || force_full) {
     if(g_opt.implicit) {
       cuda_ustar_helmholtz(0);
       cuda_vstar_helmholtz(0);
@@ -954,7 +962,10 @@ int bbb_step(void)
     cuda_solvability();
     if(nparts > 0) cuda_part_BC_star();
     cuda_dom_BC_star();
+    const int loose_now = loose > 0 && !force_full && iter + 1 < lmax;
+    g_pp_tol_now = loose_now ? loose : 0.;
     cuda_PP_bicgstab(0);
+    g_pp_tol_now = 0.;
     cuda_dom_BC_phi();
     cuda_project();
     if(nparts > 0) cuda_part_BC();
@@ -970,7 +981,8 @@ int bbb_step(void)
     iter_err = cuda_lamb_err();
     iter++;
     if(bbb_last_status() != BBB_OK) return bbb_last_status();
-    if(iter == lmax) break;
+    if(force_full || iter == lmax) break;
+    if(loose_now && iter_err <= lamb_residual) force_full = 1;
   }
   g_stats.lamb_iters = iter;
   g_stats.lamb_err = iter_err;

@@ -131,11 +131,17 @@ void bbb_set_status(int status, const char *where);
 void bbb_set_status_at(int status, const char *what, const char *file, int line);
 int bbb_fail_exit(void);
 extern bbb_options g_opt;
+/* >0 while bbb_step runs a Lamb sub-iteration whose pressure solve takes
+ * the loosened tolerance g_opt.lamb_pp_tol (bbb_pp_tol) */
+extern real g_pp_tol_now;
 extern bbb_stats g_stats;
 void bbb_record_solver(const char *name, int niter, real resid);
 #ifdef __cplusplus
 }
 #endif
+
+/* relative tolerance of the pressure solve about to run */
+static inline real bbb_pp_tol(void) { return g_pp_tol_now > 0 ? g_pp_tol_now : pp_residual; }
 
 #define BBB_CK(call) do { cudaError_t e_ = (call); if(e_ != cudaSuccess) { \
   bbb_set_status_at(BBB_ERR_CUDA, cudaGetErrorString(e_), __FILE__, __LINE__); } } while(0)

@@ -1287,7 +1287,7 @@ static void poisson_fp64(const boxc &B, const opc &O, long long n, bbb_kry *s)
 {
   dim3 grd = box_grid(B), blk(TX, TY);
   k_bicg_setup<double, V><<<grd, blk, 0, g_dev.stream>>>(B, O, g_dev.mask_p,
-    g_dev.kb, g_dev.kx, g_dev.ks, g_dev.krh, s, g_dev.partials, pp_residual,
+    g_dev.kb, g_dev.kx, g_dev.ks, g_dev.krh, s, g_dev.partials, bbb_pp_tol(),
     pp_max_iter);
   BBB_LAUNCHED();
   bicgstab_iterations<double, V>(B, O, n, g_dev.mask_p, g_dev.kr, g_dev.krh,
@@ -1633,7 +1633,7 @@ static int poisson_mixed(const boxc &BD, const boxc &BF, const opc &O,
     cudaMemcpyDeviceToHost, g_dev.stream));
   BBB_CK(cudaStreamSynchronize(g_dev.stream));
   init.bnorm = g_dev.kry_host->bnorm;
-  init.tol = pp_residual * init.bnorm;
+  init.tol = bbb_pp_tol() * init.bnorm;
   init.maxit = g_opt.max_outer > 0 ? g_opt.max_outer : 40;
   BBB_CK(cudaMemcpyAsync(s, &init, sizeof(bbb_kry), cudaMemcpyHostToDevice,
     g_dev.stream));

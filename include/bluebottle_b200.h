@@ -181,6 +181,13 @@ typedef struct bbb_options {
                               searches stop at the list's end and a contact
                               that finds no free slot uses its current
                               Stokes number unstored                       */
+  real lamb_pp_tol;        /* >0: relative tolerance of the pressure solves
+                              of every Lamb sub-iteration but the last
+                              (0, the default: pp_residual, as the
+                              reference).  A loosened sub-iteration whose
+                              coefficient error meets lamb_residual is
+                              followed by one more at pp_residual, so a
+                              step always ends on a solve to pp_residual  */
 } bbb_options;
 
 void bbb_default_options(bbb_options *opt);
