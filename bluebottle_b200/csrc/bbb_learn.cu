@@ -245,24 +245,51 @@ __device__ __forceinline__ void lg_cp16(uint32_t dst, const void *src, int bytes
                :: "r"(dst), "l"(src), "r"(bytes) : "memory");
 }
 
-/* stage plane kk's LG_TY + 2 rows of tile (i0, j0) into the ring slot */
-__device__ __forceinline__ void lg_stage_plane(const lg_box &B, const bf16 *in,
-  uint32_t slot, int i0, int j0, int kk)
+/* The 16-byte copies that stage one plane of a tile: (LG_TY + 2) rows x
+ * LG_RC cells x 2 channel halves, copy q = ry * 2 LG_RC + 2 c + h going
+ * to row ry, cell c, half h of the slot.  Thread t issues copies t, t +
+ * LG_EPI, ..: LG_NQ of them. */
+#define LG_NCOPY ((LG_TY + 2) * LG_RC * 2)
+#define LG_NQ ((LG_NCOPY + LG_EPI - 1) / LG_EPI)
+
+/* this thread's copies of tile (i0, j0): the source of each inside a
+ * plane in 16-byte units (cell (gi, gj) wrapped on periodic axes, x
+ * fastest), -1 where the cell lies outside a non-periodic box (zero
+ * fill); plane-independent, so computed once per run of planes */
+__device__ __forceinline__ void lg_stage_map(const lg_box &B, int i0, int j0,
+  int (&src)[LG_NQ])
 {
-  int gk = wrap_or(kk, B.nz, B.pz);
-  for(int q = threadIdx.x; q < (LG_TY + 2) * LG_RC * 2; q += LG_EPI) {
-    int ry = q / (LG_RC * 2), rem = q - ry * (LG_RC * 2);
-    int c = rem >> 1, h = rem & 1;
-    int gi = wrap_or(i0 - 1 + c, B.nx, B.px);
-    int gj = wrap_or(j0 - 1 + ry, B.ny, B.py);
-    const uint4 *src = reinterpret_cast<const uint4 *>(in);
-    int bytes = 0;
-    if(gi >= 0 && gj >= 0 && gk >= 0) {
-      long long cell = gi + (long long)B.nx * (gj + (long long)B.ny * gk);
-      src += cell * 2 + h;
-      bytes = 16;
+#pragma unroll
+  for(int n = 0; n < LG_NQ; n++) {
+    const int q = threadIdx.x + n * LG_EPI;
+    src[n] = -1;
+    if(q < LG_NCOPY) {
+      const int ry = q / (LG_RC * 2), rem = q - ry * (LG_RC * 2);
+      const int c = rem >> 1, h = rem & 1;
+      const int gi = wrap_or(i0 - 1 + c, B.nx, B.px);
+      const int gj = wrap_or(j0 - 1 + ry, B.ny, B.py);
+      if(gi >= 0 && gj >= 0) src[n] = (gi + B.nx * gj) * 2 + h;
     }
-    lg_cp16(slot + ry * LG_ROWB + h * LG_HALF + c * 16, src, bytes);
+  }
+}
+
+/* stage plane kk of the tile whose copies lg_stage_map listed into the
+ * ring slot */
+__device__ __forceinline__ void lg_stage_plane(const lg_box &B, const bf16 *in,
+  uint32_t slot, const int (&src)[LG_NQ], int kk)
+{
+  const int gk = wrap_or(kk, B.nz, B.pz);
+  const uint4 *base = reinterpret_cast<const uint4 *>(in)
+    + (gk >= 0 ? (long long)gk * B.nx * B.ny * 2 : 0LL);
+#pragma unroll
+  for(int n = 0; n < LG_NQ; n++) {
+    const int q = threadIdx.x + n * LG_EPI;
+    if(q < LG_NCOPY) {
+      const int ry = q / (LG_RC * 2), rem = q - ry * (LG_RC * 2);
+      const bool live = src[n] >= 0 && gk >= 0;
+      lg_cp16(slot + ry * LG_ROWB + (rem & 1) * LG_HALF + (rem >> 1) * 16,
+        live ? base + src[n] : reinterpret_cast<const uint4 *>(in), live ? 16 : 0);
+    }
   }
 }
 
@@ -390,9 +417,11 @@ __global__ void __launch_bounds__(LG_THREADS, 2) k_conv_z(lg_zbox Z,
     int k1 = left_ < (long long)(B.nz - k0) ? k0 + (int)left_ : B.nz;
     int i0 = (int)(tile % B.ntx) * LG_M;
     int j0 = (int)(tile / B.ntx) * LG_TY;
+    int srcm[LG_NQ];
+    lg_stage_map(B, i0, j0, srcm);
     if(tid < LG_EPI) {
       for(int kk = k0 - 1; kk <= k0 + 1; kk++)
-        lg_stage_plane(B, in, rbase + ((kk + 4) & 3) * LG_SLOTB, i0, j0, kk);
+        lg_stage_plane(B, in, rbase + ((kk + 4) & 3) * LG_SLOTB, srcm, kk);
       asm volatile("cp.async.wait_all;" ::: "memory");
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
@@ -415,7 +444,7 @@ __global__ void __launch_bounds__(LG_THREADS, 2) k_conv_z(lg_zbox Z,
          * reader, plane k - 1's MMAs, completed), plane k - 1's epilogue
          * from the other accumulator set */
         if(k + 1 < k1)
-          lg_stage_plane(B, in, rbase + ((k + 2 + 4) & 3) * LG_SLOTB, i0, j0, k + 2);
+          lg_stage_plane(B, in, rbase + ((k + 2 + 4) & 3) * LG_SLOTB, srcm, k + 2);
         if(k > k0)
           lg_epilogue<MODE>(B, tmem + (uint32_t)((buf ^ 1) * LG_ACC), i0, j0,
             k - 1, bv, pre, act, out32);
