@@ -194,7 +194,8 @@ def profiler_range(on):
 
 
 def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
-             learned=False, prof_range=False, keep=False, lamb_pp_tol=0.0):
+             learned=False, prof_range=False, keep=False, lamb_pp_tol=0.0,
+             gate=True):
     """One fresh simulation of the workload in precision form `prec`:
     `warmup` untimed steps, PROBE_STEPS untimed steps, `steps` timed steps
     and `e2e_steps` end-to-end steps.  With `learned`, the warm-up steps
@@ -227,7 +228,7 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
     if learned:
         out["learn_crops"] = lib.bbb_learn_crops()
         out["learn_loss"] = lib.bbb_learn_train(LEARN_ITERS, 1e-3)
-        lib.bbb_learn_enable(2 | 4)
+        lib.bbb_learn_enable(2 | 4 if gate else 2)
     for q in range(PROBE_STEPS):
         sim.step()
         if learned and q == 0:
@@ -426,6 +427,9 @@ def main():
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the timed steps of the FP32 form with "
                     "cuProfilerStart/Stop (for ncu --profile-from-start off)")
+    ap.add_argument("--no-gate", action="store_true",
+                    help="evaluate the learned guess in every step (no cost "
+                    "gate)")
     ap.add_argument("--lamb-pp-tol", type=float, default=0.0,
                     help="relative tolerance of the pressure solves of the "
                     "Lamb sub-iterations before the last (0: every solve to "
@@ -455,7 +459,7 @@ def main():
     mixed = run_form(1, steps, warmup, e2e_steps=steps, wl_name=args.workload,
                      prof_range=args.profile_range,
                      learned=not args.no_learned, keep=want_cpu,
-                     lamb_pp_tol=args.lamb_pp_tol)
+                     lamb_pp_tol=args.lamb_pp_tol, gate=not args.no_gate)
     clocks = sampler.stop()
     ms = dist.max(mixed["ms"])
     e2e_ms = dist.max(mixed["e2e_ms"])
@@ -514,6 +518,7 @@ def main():
                                "crops_per_warmup_step": LEARN_CROPS,
                                "adam_steps": LEARN_ITERS + LEARN_ONLINE * warmup,
                                "last_batch_rel_mse": mixed.get("learn_loss"),
+                               "cost_gate": not args.no_gate,
                                "timed_steps_guess_evaluated":
                                    mixed.get("guess_evaluated_steps"),
                                "timed_steps_guess_used": mixed.get("guess_used_steps"),
