@@ -137,7 +137,8 @@ bbb_part_state_pull bbb_mark bbb_mark_elapsed bbb_PP_bicgstab_static
 bbb_learn_enable bbb_learn_train bbb_learn_crops bbb_learn_param_count
 bbb_learn_get_params bbb_learn_set_params bbb_learn_forward
 bbb_learn_use_reference_conv bbb_learn_grad bbb_learn_gate_decide
-bbb_learn_set_crops_per_step""".split()
+bbb_learn_set_crops_per_step bbb_snapshot_start bbb_snapshot_finish
+bbb_snapshot_busy""".split()
 
 _lib = None
 
@@ -163,7 +164,8 @@ def load():
                  "bbb_learn_crops", "bbb_learn_param_count",
                  "bbb_learn_get_params", "bbb_learn_set_params",
                  "bbb_learn_forward", "bbb_PP_bicgstab_static",
-                 "bbb_learn_set_crops_per_step",
+                 "bbb_learn_set_crops_per_step", "bbb_snapshot_start",
+                 "bbb_snapshot_finish", "bbb_snapshot_busy",
                  "bbb_out_restart", "bbb_in_restart"):
         getattr(lib, name).restype = C.c_int
     lib.bbb_out_restart.argtypes = [C.c_char_p]

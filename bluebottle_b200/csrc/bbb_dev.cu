@@ -289,6 +289,7 @@ extern "C" void cuda_dom_free(void)
   if(!g_dev.ready) return;
   cudaStreamSynchronize(g_dev.stream);
   bbb_learn_release();
+  bbb_snapshot_release();
   real **rs[] = {&g_dev.p0, &g_dev.p, &g_dev.phi, &g_dev.u, &g_dev.v, &g_dev.w,
     &g_dev.u0, &g_dev.v0, &g_dev.w0, &g_dev.us, &g_dev.vs, &g_dev.ws,
     &g_dev.conv_u, &g_dev.conv_v, &g_dev.conv_w, &g_dev.conv0_u,

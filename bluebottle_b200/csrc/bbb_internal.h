@@ -178,6 +178,7 @@ void bbb_learn_post_solve(void);
 void bbb_learn_solve_done(double r_final);
 void bbb_learn_step_boundary(void);
 void bbb_learn_release(void);
+void bbb_snapshot_release(void);
 void bbb_bins_free(void);
 
 #endif

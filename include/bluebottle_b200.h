@@ -315,6 +315,23 @@ void bbb_profile_get_pass(int pass, double *ms, long long *launches,
 void bbb_part_state_push(void);
 void bbb_part_state_pull(void);
 
+/* Asynchronous output snapshot of the fields the reference's writers read
+ * (out_VTK, src/vtk.c:48; cgns_flow_field / cgns_particles,
+ * src/recorder.c:487-1890): u, v, w, p, phase and parts.  The reference
+ * pulls them with a blocking cuda_dom_pull / cuda_part_pull before every
+ * output (src/bluebottle.c:717-760).  bbb_snapshot_start copies them on the
+ * device after the step and moves the copy to pinned host staging on a
+ * stream of its own while the following steps run; bbb_snapshot_finish
+ * waits for that transfer and writes the snapshot into the host arrays
+ * (the state at the start call, whatever steps ran since).  One snapshot
+ * at a time: a second start before the finish, or a finish without a
+ * start, returns BBB_ERR_STATE.  The first start allocates the device copy
+ * and the pinned staging (about twice the six fields); cuda_dom_free
+ * releases them.  bbb_snapshot_busy: 1 between start and finish. */
+int bbb_snapshot_start(void);
+int bbb_snapshot_finish(void);
+int bbb_snapshot_busy(void);
+
 /* CUDA-event time marks (0..7) on the library's stream; elapsed waits for
  * mark b and returns milliseconds between marks a and b (-1 on error) */
 void bbb_mark(int i);
