@@ -207,3 +207,51 @@ def test_u_system_stored_y_fastest(gpu, precision):
     finally:
         sim.close()
         orc.close()
+
+
+def test_pid_controller_parity(gpu):
+    """The reference's PID control of the driving pressure gradient
+    (src/cuda_bluebottle.cu:3781-3805: gradP.z follows the spheres' mean
+    vertical acceleration with gains Kp, Ki, Kd, computed on the host from
+    the pulled particle records).  With nonzero gains the library and the
+    FP64 oracle step together and agree on gradP.z, the controller's
+    integral and last input, the fields and the spheres."""
+    import ctypes as C
+    wl = configs.sedimentation((32, 32, 64), (8.0, 8.0, 16.0), 4, nu=0.1,
+                               tol=1e-10, lamb_max_iter=2, seed=6)
+    sim = Sim(wl, options=dict(lamb_max_iter_override=2))
+    gains = (("Kp", 0.5), ("Ki", 0.1), ("Kd", 0.05))
+    for nm, v in gains:
+        C.c_double.in_dll(sim.lib, nm).value = v
+    try:
+        orc = Oracle.from_sim(sim)
+    except BaseException:
+        sim.close()
+        raise
+    try:
+        assert orc.P.Kp == 0.5 and orc.P.Ki == 0.1 and orc.P.Kd == 0.05
+        sim.prepare()
+        gz0 = sim.gradP.z
+        for _ in range(3):
+            sim.step()
+            orc.step()
+            a, b = sim.gradP.z, orc.P.gradP.z
+            assert abs(a - b) <= 1e-9 * max(abs(b), 1e-12), (a, b)
+            for nm in ("pid_int", "pid_back"):
+                x = C.c_double.in_dll(sim.lib, nm).value
+                y = getattr(orc.P, nm)
+                assert abs(x - y) <= 1e-9 * max(abs(y), 1e-12), (nm, x, y)
+        assert sim.gradP.z != gz0          # the controller acted
+        sim.pull()
+        d = sim.dom
+        for name in ("u", "v", "w", "p"):
+            e = rel_err(field_interior(d, name, sim.array(name)),
+                        field_interior(d, name, orc.field(name)))
+            assert e < 1e-8, (name, e)
+        for pg, po in zip(sim.parts(), orc.field("parts")):
+            for k in ("z", "w", "wdot"):
+                a, b = getattr(pg, k), getattr(po, k)
+                assert abs(a - b) <= 1e-8 * max(1.0, abs(b)), (k, a, b)
+    finally:
+        sim.close()
+        orc.close()
