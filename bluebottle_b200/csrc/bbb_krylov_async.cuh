@@ -24,8 +24,10 @@
  * Every warp owns one tile row and computes the Jacobi-scaled stencil input
  * q for its row and for the rows just south and north of it straight from
  * the stage (no shared ring, so the stages of two blocks fit per SM); the
- * row's x-halo q comes from the stage's halo chunks.  q of the plane below
- * and of the plane being stencilled stay in registers.
+ * row's x-halo q comes from the stage's halo chunks.  A plane's stencil
+ * sum is formed up to its top term as soon as its stage is read, so its
+ * south / north q die at once; the plane's q, that partial sum and its
+ * epilogue inputs stay in registers until the plane above completes it.
  *
  * Wrap-around neighbours that a tiled box cannot express land in slots of
  * their own, never under a box (two asynchronous writes to one byte would
@@ -336,10 +338,13 @@ __device__ __forceinline__ void as_sum4(double &r, const T (&a)[4])
 
 /* (A q) at one cell, as op_apply (same terms in the same order), with the
  * face terms of clear mask bits skipped rather than multiplied by zero --
- * the same value for finite q; w* already carry the operator's sign */
+ * the same value for finite q; w* already carry the operator's sign.  Split
+ * in two so a plane's sum is formed while its own neighbour rows are at
+ * hand: as_apply_lo sums the terms B, S, W, C, E, N; as_apply_hi adds T
+ * once the plane above is staged, then applies the inside-particle rule. */
 template <typename T>
-__device__ __forceinline__ T as_apply(unsigned m, T d, T wx, T wy, T wz, T qB,
-  T qS, T qW, T qC, T qE, T qN, T qT)
+__device__ __forceinline__ T as_apply_lo(unsigned m, T d, T wx, T wy, T qB,
+  T qS, T qW, T qC, T qE, T qN, T wz)
 {
   T acc = (T)0.;
   if(m & BBB_MB) acc += wz * qB;
@@ -348,6 +353,12 @@ __device__ __forceinline__ T as_apply(unsigned m, T d, T wx, T wy, T wz, T qB,
   acc += d * qC;
   if(m & BBB_ME) acc += wx * qE;
   if(m & BBB_MN) acc += wy * qN;
+  return acc;
+}
+
+template <typename T>
+__device__ __forceinline__ T as_apply_hi(unsigned m, T wz, T acc, T qC, T qT)
+{
   if(m & BBB_MT) acc += wz * qT;
   return (m & BBB_MID) ? qC : acc;
 }
@@ -623,36 +634,37 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
       }
     }
     const int o_own = L::OWN_OFF + w * L::OWNB + col * L::ESZ;
-    T qm[4], qc[4], qn[4], qSc[4], qNc[4], qSn[4], qNn[4];
-    T r0c[4], r1c[4], r0n[4], r1n[4];
-    T xqc = (T)0., xqn = (T)0.;
-    unsigned mc = 0, mn = 0;
+    /* carried from plane to plane: the previous plane's q, its stencil
+     * sum without the top term, its mask word and its epilogue inputs */
+    T qp[4], Pp[4], r0p[4], r1p[4];
+    unsigned mp = 0;
 #pragma unroll
-    for(int v = 0; v < 4; v++) {
-      qm[v] = qc[v] = qn[v] = qSc[v] = qNc[v] = qSn[v] = qNn[v] = (T)0.;
-      r0c[v] = r1c[v] = r0n[v] = r1n[v] = (T)0.;
-    }
+    for(int v = 0; v < 4; v++) qp[v] = Pp[v] = r0p[v] = r1p[v] = (T)0.;
+    /* the stage of load L0 + a and its barrier phase, advanced per plane
+     * (no 64-bit division in the loop) */
+    int buf = (int)(L0 % L::NS);
+    uint32_t par = (uint32_t)((L0 / L::NS) & 1);
     for(int a = 0; a < cnt; a++) {
       const int pl = k0 - 1 + a;
-      const long long Ld = L0 + a;
-      const int buf = (int)(Ld % L::NS);
-      const uint32_t par = (uint32_t)((Ld / L::NS) & 1);
       const uint8_t *st = sm + buf * L::STAGE;
       if(!as_wait(as_saddr(&bars[buf]), par)) bad = 1;
       const bool full = pl >= k0 && pl < k1;
+      T qk[4], qS[4], qN[4], Pk[4], r0k[4], r1k[4];
+      T xq = (T)0.;
+      unsigned mk = 0;
       if(valid) {
-        mn = *reinterpret_cast<const unsigned *>(st + m_own);
+        mk = *reinterpret_cast<const unsigned *>(st + m_own);
         if(full) {
-          as_own4<T, PASS>(st + h_own, mn, st + o_own, tab.dinv, S,
-            lin(B, i0 + col, j, pl), A, qn, r0n, r1n, red);
+          as_own4<T, PASS>(st + h_own, mk, st + o_own, tab.dinv, S,
+            lin(B, i0 + col, j, pl), A, qk, r0k, r1k, red);
           as_q4<T, PASS>(st + h_s, *reinterpret_cast<const unsigned *>(st + m_s),
-            tab.dinv, S, qSn);
+            tab.dinv, S, qS);
           as_q4<T, PASS>(st + h_n, *reinterpret_cast<const unsigned *>(st + m_n),
-            tab.dinv, S, qNn);
+            tab.dinv, S, qN);
           if(tx == 0 || tx == 31)
-            xqn = as_q1<T, PASS>(st + h_x, x_stride, st[m_x], tab.dinv, S);
+            xq = as_q1<T, PASS>(st + h_x, x_stride, st[m_x], tab.dinv, S);
         } else {
-          as_q4<T, PASS>(st + h_own, mn, tab.dinv, S, qn);
+          as_q4<T, PASS>(st + h_own, mk, tab.dinv, S, qk);
         }
       }
       /* release the stage: the last of the 8 warps to finish reading it
@@ -665,53 +677,62 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
           as_issue<T, PASS>(B, A, M, sbase + buf * L::STAGE, as_saddr(&bars[buf]),
             i0, j0, mapz(B, pl + L::NS), E);
       }
-      if(a >= 2 && valid) {
-        const int k = pl - 1;
-        T lft = __shfl_up_sync(0xffffffffu, qc[3], 1);
-        T rgt = __shfl_down_sync(0xffffffffu, qc[0], 1);
-        if(tx == 0) lft = xqc;
-        if(tx == 31) rgt = xqc;
-        T Aq[4];
+      if(valid) {
+        if(full) {
+          /* this plane's stencil up to its top term, while its south,
+           * north and x-halo q are at hand */
+          T lft = __shfl_up_sync(0xffffffffu, qk[3], 1);
+          T rgt = __shfl_down_sync(0xffffffffu, qk[0], 1);
+          if(tx == 0) lft = xq;
+          if(tx == 31) rgt = xq;
 #pragma unroll
-        for(int v = 0; v < 4; v++) {
-          unsigned mv = mbyte(mc, v);
-          T qW = v > 0 ? qc[v - 1] : lft;
-          T qE = v < 3 ? qc[v + 1] : rgt;
-          Aq[v] = as_apply<T>(mv, tab.diag[mv], wx, wy, wz, qm[v], qSc[v], qW,
-            qc[v], qE, qNc[v], qn[v]);
+          for(int v = 0; v < 4; v++) {
+            unsigned mv = mbyte(mk, v);
+            T qW = v > 0 ? qk[v - 1] : lft;
+            T qE = v < 3 ? qk[v + 1] : rgt;
+            Pk[v] = as_apply_lo<T>(mv, tab.diag[mv], wx, wy, qp[v], qS[v], qW,
+              qk[v], qE, qN[v], wz);
+          }
         }
-        const long long ge = lin(B, i0 + col, j, k);
-        if constexpr(PASS == 0) {
-          as_st4<T>(A.w2 + ge, Aq);
-          as_dot4<T>(red[0], r0c, Aq);
-        } else if constexpr(PASS == 1) {
-          as_st4<T>(A.w1 + ge, Aq);
-          as_dot4<T>(red[0], Aq, r0c);
-          as_dot4<T>(red[1], Aq, Aq);
-          as_dot4<T>(red[3], r1c, r0c);
-          as_dot4<T>(red[4], r1c, Aq);
-        } else if constexpr(PASS == 3) {
-          /* y = A p and (A p, p), as epi_c1 */
-          as_st4<T>(A.w1 + ge, Aq);
-          as_dot4<T>(red[0], Aq, r0c);
-        } else {
-          /* outer residual r = b - A x in FP64, stored rounded to FP32 */
-          T rr[4];
+        if(a >= 2) {
+          /* the previous plane completed by its top term */
+          const int k = pl - 1;
+          T Aq[4];
 #pragma unroll
-          for(int v = 0; v < 4; v++) rr[v] = r0c[v] - Aq[v];
-          *reinterpret_cast<float4 *>(A.rf + ge) =
-            make_float4((float)rr[0], (float)rr[1], (float)rr[2], (float)rr[3]);
-          as_dot4<T>(red[0], rr, rr);
-          as_sum4<T>(red[2], rr);
+          for(int v = 0; v < 4; v++)
+            Aq[v] = as_apply_hi<T>(mbyte(mp, v), wz, Pp[v], qp[v], qk[v]);
+          const long long ge = lin(B, i0 + col, j, k);
+          if constexpr(PASS == 0) {
+            as_st4<T>(A.w2 + ge, Aq);
+            as_dot4<T>(red[0], r0p, Aq);
+          } else if constexpr(PASS == 1) {
+            as_st4<T>(A.w1 + ge, Aq);
+            as_dot4<T>(red[0], Aq, r0p);
+            as_dot4<T>(red[1], Aq, Aq);
+            as_dot4<T>(red[3], r1p, r0p);
+            as_dot4<T>(red[4], r1p, Aq);
+          } else if constexpr(PASS == 3) {
+            /* y = A p and (A p, p), as epi_c1 */
+            as_st4<T>(A.w1 + ge, Aq);
+            as_dot4<T>(red[0], Aq, r0p);
+          } else {
+            /* outer residual r = b - A x in FP64, stored rounded to FP32 */
+            T rr[4];
+#pragma unroll
+            for(int v = 0; v < 4; v++) rr[v] = r0p[v] - Aq[v];
+            *reinterpret_cast<float4 *>(A.rf + ge) =
+              make_float4((float)rr[0], (float)rr[1], (float)rr[2], (float)rr[3]);
+            as_dot4<T>(red[0], rr, rr);
+            as_sum4<T>(red[2], rr);
+          }
         }
       }
 #pragma unroll
       for(int v = 0; v < 4; v++) {
-        qm[v] = qc[v]; qc[v] = qn[v]; qSc[v] = qSn[v]; qNc[v] = qNn[v];
-        r0c[v] = r0n[v]; r1c[v] = r1n[v];
+        qp[v] = qk[v]; Pp[v] = Pk[v]; r0p[v] = r0k[v]; r1p[v] = r1k[v];
       }
-      xqc = xqn;
-      mc = mn;
+      mp = mk;
+      if(++buf == L::NS) { buf = 0; par ^= 1u; }
     }
     nload = L0 + cnt;
     u0 += k1 - k0;
