@@ -1046,7 +1046,7 @@ static int as_per_sm(void)
          cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM) == cudaSuccess) {
       int v = 0;
       if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_bicg_async<T, PASS>,
-           AS_THREADS, L::SMEM) == cudaSuccess) nb = v;
+           L::THREADS, L::SMEM) == cudaSuccess) nb = v;
     }
     cudaGetLastError();
   }
@@ -1065,12 +1065,13 @@ static int as_per_sm(void)
  * from 0.36 to 0.26 ms.  `align` additionally cuts every group's planes
  * into equal runs so that all groups start at the same planes, where at
  * least 80% of the slots stay busy (slower than grouping alone there). */
-static boxc retile(const boxc &B0, int per_sm, bool align, int gxw = 0, int gyw = 0)
+static boxc retile(const boxc &B0, int per_sm, bool align, int th = 8, int gxw = 0,
+  int gyw = 0)
 {
   boxc b = B0;
   b.vec = AS_W / TX;
   b.tiles_x = b.nx / AS_W;
-  int tiles_y = (b.ny + TY - 1) / TY;
+  int tiles_y = (b.ny + th - 1) / th;
   long long all = (long long)sm_count() * (per_sm > 0 ? per_sm : 1);
   int gx = gxw > 0 ? gxw : (b.tiles_x <= 2 ? b.tiles_x : 1);
   if(b.tiles_x % gx) gx = 1;
@@ -1151,12 +1152,12 @@ static bool as_pass_maps(as_maps *M, const boxc &B, const uint8_t *mask,
   typedef as_layout<T, PASS> L;
   memset(M, 0, sizeof(*M));
   bool ok = as_map(&M->m, mask, 1, B, L::MBOXW, L::BOXH)
-    && as_map(&M->mx, mask, 1, B, 16, 8);
+    && as_map(&M->mx, mask, 1, B, 16, L::TH);
   for(int a = 0; a < L::NA && ok; a++)
     ok = as_map(&M->h[a], h[a], L::ESZ, B, L::BOXW, L::BOXH)
-      && as_map(&M->hx[a], h[a], L::ESZ, B, L::CH, 8);
+      && as_map(&M->hx[a], h[a], L::ESZ, B, L::CH, L::TH);
   for(int b = 0; b < L::NO && ok; b++)
-    ok = as_map(&M->o[b], o[b], L::ESZ, B, AS_W, 8);
+    ok = as_map(&M->o[b], o[b], L::ESZ, B, AS_W, L::TH);
   return ok;
 }
 
@@ -1196,8 +1197,8 @@ static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
   int rc = resume ? 1 : 0;
   as_maps MA[2][2], MB[2][2];   /* [r buffer][p, v buffer] */
   if(staged) {
-    BA = retile(B, as_per_sm<T, 0>(), as_layout<T, 0>::ALIGN);
-    BB = retile(B, as_per_sm<T, 1>(), as_layout<T, 1>::ALIGN);
+    BA = retile(B, as_per_sm<T, 0>(), as_layout<T, 0>::ALIGN, as_layout<T, 0>::TH);
+    BB = retile(B, as_per_sm<T, 1>(), as_layout<T, 1>::ALIGN, as_layout<T, 1>::TH);
     for(int q = 0; q < 2 && staged; q++)
       for(int c = 0; c < 2 && staged; c++) {
         const T *ha[4] = {rr[q], tv, pp[c], vv[c]}, *oa[2] = {x, rh};
@@ -1220,7 +1221,7 @@ static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
       A.h[0] = rr[rc]; A.h[1] = tv; A.h[2] = pp[cur]; A.h[3] = vv[cur];
       A.w0 = rr[rc ^ 1]; A.w1 = pp[cur ^ 1]; A.w2 = vv[cur ^ 1]; A.x = x;
       A.s = s; A.partials = g_dev.partials;
-      k_bicg_async<T, 0><<<BA.nblk, AS_THREADS, as_layout<T, 0>::SMEM,
+      k_bicg_async<T, 0><<<BA.nblk, as_layout<T, 0>::THREADS, as_layout<T, 0>::SMEM,
         g_dev.stream>>>(BA, O, A, MA[rc][cur]);
       rc ^= 1;
     } else {
@@ -1242,7 +1243,7 @@ static void bicgstab_iterations(const boxc &B, const opc &O, long long n,
       A.h[0] = rr[rc]; A.h[1] = vv[cur]; A.h[2] = NULL; A.h[3] = NULL;
       A.w0 = NULL; A.w1 = tv; A.w2 = NULL; A.x = NULL;
       A.s = s; A.partials = g_dev.partials;
-      k_bicg_async<T, 1><<<BB.nblk, AS_THREADS, as_layout<T, 1>::SMEM,
+      k_bicg_async<T, 1><<<BB.nblk, as_layout<T, 1>::THREADS, as_layout<T, 1>::SMEM,
         g_dev.stream>>>(BB, O, A, MB[rc][cur]);
     } else {
       k_bicgB<T, V><<<grd, blk, 0, g_dev.stream>>>(B, O, mask, r, vv[cur],
@@ -1558,7 +1559,7 @@ static void outer_resid(const boxc &BD, const opc &O, const uint8_t *mask,
   double itol, int imaxit, int project, long long n)
 {
   if(BBB_ASYNC_ON && BD.nx % AS_W == 0 && as_per_sm<double, 2>() > 0) {
-    boxc B2 = retile(BD, as_per_sm<double, 2>(), false);
+    boxc B2 = retile(BD, as_per_sm<double, 2>(), false, as_layout<double, 2>::TH);
     as_maps M;
     const double *h[4] = {x, NULL, NULL, NULL}, *o[2] = {b, NULL};
     if(as_pass_maps<double, 2>(&M, B2, mask, h, o)) {
@@ -1568,7 +1569,8 @@ static void outer_resid(const boxc &BD, const opc &O, const uint8_t *mask,
       A.rf = rf; A.si = si; A.itol = itol; A.imaxit = imaxit;
       A.project = project; A.n = n;
       prof_begin(BBB_PROF_OUTER, (double)n * (2. * 8. + 4. + 1.));
-      k_bicg_async<double, 2><<<B2.nblk, AS_THREADS, as_layout<double, 2>::SMEM,
+      k_bicg_async<double, 2><<<B2.nblk, as_layout<double, 2>::THREADS,
+        as_layout<double, 2>::SMEM,
         g_dev.stream>>>(B2, O, A, M);
       BBB_LAUNCHED();
       prof_end();
@@ -2148,7 +2150,7 @@ struct cg_staged {
     B = B0;
     on = BBB_ASYNC_ON && B0.nx % AS_W == 0 && as_per_sm<T, 3>() > 0;
     if(!on) return;
-    B = retile(B0, as_per_sm<T, 3>(), as_layout<T, 3>::ALIGN);
+    B = retile(B0, as_per_sm<T, 3>(), as_layout<T, 3>::ALIGN, as_layout<T, 3>::TH);
     for(int c = 0; c < 2 && on; c++) {
       const T *h[4] = {r, p[c], NULL, NULL};
       on = as_pass_maps<T, 3>(&M[c], B, mask, h, NULL);
@@ -2163,7 +2165,7 @@ struct cg_staged {
     A.h[0] = r; A.h[1] = p[cur];
     A.w0 = p[cur ^ 1]; A.w1 = y;
     A.s = s; A.partials = g_dev.partials;
-    k_bicg_async<T, 3><<<B.nblk, AS_THREADS, as_layout<T, 3>::SMEM,
+    k_bicg_async<T, 3><<<B.nblk, as_layout<T, 3>::THREADS, as_layout<T, 3>::SMEM,
       g_dev.stream>>>(B, O, A, M[cur]);
   }
 };

@@ -71,7 +71,7 @@
 #define BBB_AS_NS_D3 2
 #endif
 #ifndef BBB_AS_MINB_F3
-#define BBB_AS_MINB_F3 3
+#define BBB_AS_MINB_F3 2
 #endif
 #ifndef BBB_AS_MINB_D3
 #define BBB_AS_MINB_D3 2
@@ -80,7 +80,7 @@
 #define BBB_AS_MINB_F0 2
 #endif
 #ifndef BBB_AS_MINB_F1
-#define BBB_AS_MINB_F1 3
+#define BBB_AS_MINB_F1 2
 #endif
 #ifndef BBB_AS_MINB_D0
 #define BBB_AS_MINB_D0 1
@@ -91,18 +91,55 @@
 #ifndef BBB_AS_MINB_D2
 #define BBB_AS_MINB_D2 2
 #endif
+/* rows per warp (R) and tile height (TH, a multiple of R: the block has
+ * TH / R warps) of pass B, the CG stencil pass and the outer residual;
+ * pass A keeps one row per warp and 8-row tiles.  FP32 pass B and CG run
+ * two rows per warp in 16-row tiles (128 registers, 2 blocks per SM): on
+ * 256x256x512 pass B 0.178 -> 0.150 ms, CG 0.149 -> 0.146 ms against one
+ * row per warp in 8-row tiles (80 registers, 3 blocks per SM) */
+#ifndef BBB_AS_R_F1
+#define BBB_AS_R_F1 2
+#endif
+#ifndef BBB_AS_TH_F1
+#define BBB_AS_TH_F1 16
+#endif
+#ifndef BBB_AS_R_D1
+#define BBB_AS_R_D1 1
+#endif
+#ifndef BBB_AS_TH_D1
+#define BBB_AS_TH_D1 8
+#endif
+#ifndef BBB_AS_R_F3
+#define BBB_AS_R_F3 2
+#endif
+#ifndef BBB_AS_TH_F3
+#define BBB_AS_TH_F3 16
+#endif
+#ifndef BBB_AS_R_D2
+#define BBB_AS_R_D2 1
+#endif
+#ifndef BBB_AS_TH_D2
+#define BBB_AS_TH_D2 8
+#endif
+#ifndef BBB_AS_R_D3
+#define BBB_AS_R_D3 1
+#endif
+#ifndef BBB_AS_TH_D3
+#define BBB_AS_TH_D3 8
+#endif
 
 __host__ __device__ constexpr int as_rup(int v, int a) { return (v + a - 1) / a * a; }
 
-/* Stage layout in bytes (T the element type, CH = 16 / sizeof(T)):
+/* Stage layout in bytes (T the element type, CH = 16 / sizeof(T), TH the
+ * tile height in rows):
  *   per halo array (pass A: r, t, p, v; pass B: r, v; outer residual: x;
  *   CG: r, p) a region of
- *     10 box rows of [CH | 128 | CH] cells (tile rows j0-1 .. j0+8),
+ *     TH + 2 box rows of [CH | 128 | CH] cells (tile rows j0-1 .. j0+TH),
  *     2 extra rows of 128 cells (y = -1, y = ny);
- *   mask: 10 rows of [16 | 128 | 16] bytes, 2 extra rows of 128;
+ *   mask: TH + 2 rows of [16 | 128 | 16] bytes, 2 extra rows of 128;
  *   own arrays (pass A: x, rh; pass B: rh; outer residual: b; CG: none):
- *   8 rows of 128 cells;
- *   x-wrap chunks: per halo array and the mask [2 sides][8 rows][16 B].
+ *   TH rows of 128 cells;
+ *   x-wrap chunks: per halo array and the mask [2 sides][TH rows][16 B].
  * Regions start on 128-byte boundaries (tensor-copy destinations). */
 template <typename T, int PASS>
 struct as_layout {
@@ -110,20 +147,35 @@ struct as_layout {
   static constexpr int CH = 16 / ESZ;
   static constexpr int NA = PASS == 0 ? 4 : (PASS == 1 || PASS == 3 ? 2 : 1);
   static constexpr int NO = PASS == 0 ? 2 : (PASS == 3 ? 0 : 1);
+  /* rows per warp, tile rows, warps and threads per block */
+  static constexpr int R = ESZ == 4
+    ? (PASS == 1 ? BBB_AS_R_F1 : (PASS == 3 ? BBB_AS_R_F3 : 1))
+    : (PASS == 1 ? BBB_AS_R_D1 : (PASS == 3 ? BBB_AS_R_D3
+       : (PASS == 2 ? BBB_AS_R_D2 : 1)));
+  static constexpr int TH = ESZ == 4
+    ? (PASS == 1 ? BBB_AS_TH_F1 : (PASS == 3 ? BBB_AS_TH_F3 : 8))
+    : (PASS == 1 ? BBB_AS_TH_D1 : (PASS == 3 ? BBB_AS_TH_D3
+       : (PASS == 2 ? BBB_AS_TH_D2 : 8)));
+  static constexpr int WARPS = TH / R;
+  static constexpr int THREADS = 32 * WARPS;
+  static_assert(TH % R == 0 && WARPS >= 1 && WARPS <= 32 && TH + 2 <= 256,
+                "tile height: a multiple of the rows per warp, 1..32 warps");
   static constexpr int BOXW = AS_W + 2 * CH;        /* halo-array box  */
-  static constexpr int BOXH = 10;
+  static constexpr int BOXH = TH + 2;
   static constexpr int MBOXW = AS_W + 32;            /* mask box        */
   static constexpr int ROWP = BOXW * ESZ;
   static constexpr int OWNB = AS_W * ESZ;
-  static constexpr int EXT_OFF = 10 * ROWP;
+  static constexpr int EXT_OFF = BOXH * ROWP;
   static constexpr int AREG = as_rup(EXT_OFF + 2 * OWNB, 128);
   static constexpr int MROWP = MBOXW;
-  static constexpr int MEXT_OFF = 10 * MROWP;
+  static constexpr int MEXT_OFF = BOXH * MROWP;
   static constexpr int MREG = as_rup(MEXT_OFF + 2 * 128, 128);
   static constexpr int MASK_OFF = NA * AREG;
   static constexpr int OWN_OFF = MASK_OFF + MREG;
-  static constexpr int XW_OFF = OWN_OFF + NO * 8 * OWNB;
-  static constexpr int STAGE = as_rup(XW_OFF + (NA + 1) * 256, 128);
+  static constexpr int XW_OFF = OWN_OFF + NO * TH * OWNB;
+  /* x-wrap chunks of one array: 2 sides x TH rows x 16 bytes */
+  static constexpr int XWA = 2 * TH * 16;
+  static constexpr int STAGE = as_rup(XW_OFF + (NA + 1) * XWA, 128);
   /* stages in the ring */
   static constexpr int NS = ESZ == 4
     ? (PASS == 0 ? BBB_AS_NS_F0 : (PASS == 3 ? BBB_AS_NS_F3 : BBB_AS_NS_F1))
@@ -144,17 +196,17 @@ struct as_layout {
    * gets the same L2 reuse without idle slots */
   static constexpr bool ALIGN = false;
   /* bytes a stage receives: the boxes always, the wrap slots at edges */
-  static constexpr int TX_BASE = NA * BOXH * ROWP + BOXH * MROWP + NO * 8 * OWNB;
-  static constexpr int TX_XSIDE = (NA + 1) * 8 * 16;
+  static constexpr int TX_BASE = NA * BOXH * ROWP + BOXH * MROWP + NO * TH * OWNB;
+  static constexpr int TX_XSIDE = (NA + 1) * TH * 16;
   static constexpr int TX_YSIDE = NA * OWNB + 128;
 };
 
 /* the tensor maps of one pass, passed by value as a grid constant */
 struct as_maps {
-  CUtensorMap h[4];     /* halo arrays, box {128 + 2 CH, 10, 1}    */
-  CUtensorMap hx[4];    /* halo arrays, box {CH, 8, 1}             */
-  CUtensorMap m, mx;    /* mask, boxes {160, 10, 1} and {16, 8, 1} */
-  CUtensorMap o[2];     /* own arrays, box {128, 8, 1}             */
+  CUtensorMap h[4];     /* halo arrays, box {128 + 2 CH, TH + 2, 1}    */
+  CUtensorMap hx[4];    /* halo arrays, box {CH, TH, 1}                */
+  CUtensorMap m, mx;    /* mask, boxes {160, TH + 2, 1} and {16, TH, 1} */
+  CUtensorMap o[2];     /* own arrays, box {128, TH, 1}                */
 };
 
 /* the global arrays of one pass */
@@ -241,16 +293,17 @@ __device__ __forceinline__ uint32_t as_release(uint32_t cnt)
 
 /* where a tile touches the box's faces */
 struct as_edges {
-  int xl, xr, ys, yn;     /* i0 == 0, i0 + 128 == nx, j0 == 0, j0 + 8 >= ny */
+  int xl, xr, ys, yn;     /* i0 == 0, i0 + 128 == nx, j0 == 0, j0 + TH >= ny */
 };
 
+template <int TH>
 __device__ __forceinline__ as_edges as_tile_edges(const boxc &B, int i0, int j0)
 {
   as_edges e;
   e.xl = i0 == 0;
   e.xr = i0 + AS_W == B.nx;
   e.ys = j0 == 0;
-  e.yn = j0 + 8 >= B.ny;
+  e.yn = j0 + TH >= B.ny;
   return e;
 }
 
@@ -268,20 +321,20 @@ __device__ __forceinline__ void as_issue(const boxc &B, const as_args<T> &A,
 #pragma unroll
   for(int a = 0; a < L::NA; a++)
     as_box(st + a * L::AREG, &M.h[a], i0 - (L::BOXW - AS_W) / 2,
-      j0 - (L::BOXH - 8) / 2, gk, bar);
-  as_box(st + L::MASK_OFF, &M.m, i0 - (L::MBOXW - AS_W) / 2, j0 - (L::BOXH - 8) / 2,
+      j0 - (L::BOXH - L::TH) / 2, gk, bar);
+  as_box(st + L::MASK_OFF, &M.m, i0 - (L::MBOXW - AS_W) / 2, j0 - (L::BOXH - L::TH) / 2,
     gk, bar);
 #pragma unroll
   for(int b = 0; b < L::NO; b++)
-    as_box(st + L::OWN_OFF + b * 8 * L::OWNB, &M.o[b], i0, j0, gk, bar);
+    as_box(st + L::OWN_OFF + b * L::TH * L::OWNB, &M.o[b], i0, j0, gk, bar);
   for(int side = 0; side < 2; side++) {
     if(side == 0 ? !E.xl : !E.xr) continue;
     int g = side == 0 ? B.wW : B.wE;
-    uint32_t d = st + L::XW_OFF + side * 128;
+    uint32_t d = st + L::XW_OFF + side * L::TH * 16;
 #pragma unroll
     for(int a = 0; a < L::NA; a++)
-      as_box(d + a * 256, &M.hx[a], g / L::CH * L::CH, j0, gk, bar);
-    as_box(d + L::NA * 256, &M.mx, g / 16 * 16, j0, gk, bar);
+      as_box(d + a * L::XWA, &M.hx[a], g / L::CH * L::CH, j0, gk, bar);
+    as_box(d + L::NA * L::XWA, &M.mx, g / 16 * 16, j0, gk, bar);
   }
   for(int side = 0; side < 2; side++) {
     if(side == 0 ? !E.ys : !E.yn) continue;
@@ -430,7 +483,7 @@ __device__ __forceinline__ void as_q4(const uint8_t *h, unsigned mw,
 
 /* The block's own 4 cells of a staged row: q, and the pass's pointwise
  * work -- stores at global index gc, sums into red.  o is the cells' first
- * own-array entry (pass A: x at o, rh at o + 8 rows; pass B: rh at o);
+ * own-array entry (pass A: x at o, rh at o + TH rows; pass B: rh at o);
  * raw0 / raw1 carry what the epilogue needs (pass A: rh; pass B: s, rh). */
 template <typename T, int PASS>
 __device__ __forceinline__ void as_own4(const uint8_t *h, unsigned mw,
@@ -464,7 +517,7 @@ __device__ __forceinline__ void as_own4(const uint8_t *h, unsigned mw,
     }
 #pragma unroll
     for(int a = 0; a < 4; a++) q[a] = dinv[mbyte(mw, a)] * pn[a];
-    as_ld4<T>(o + 8 * L::OWNB, raw0);
+    as_ld4<T>(o + L::TH * L::OWNB, raw0);
     as_dot4<T>(red[1], rr, rr);
     as_dot4<T>(red[2], raw0, rr);
     as_st4<T>(A.w0 + gc, rr);
@@ -534,18 +587,22 @@ __device__ __forceinline__ T as_q1(const uint8_t *h, int stride, unsigned m,
 
 /* One staged pass (PASS 0: BiCGSTAB pass A, 1: pass B, 2: the FP64 outer
  * residual of the defect correction, 3: the Helmholtz CG stencil pass) over
- * this block's units,
- * 256 threads = 8 warps, warp w owning tile row w, lane l cells 4l..4l+3.
- * Per plane: wait for the stage; each warp forms q of its row (with the
- * pointwise work where the plane is the block's) and of its south / north
- * rows and x-halo cells; releases the stage (the last warp to release it
- * refills it with the plane NS ahead); then the stencil and epilogue of
- * the plane below, from registers. */
+ * this block's units, TH / R warps, warp w owning the R adjacent tile rows
+ * R w .. R w + R - 1, lane l cells 4l..4l+3 of each.
+ * Per plane: wait for the stage; each warp forms q of its rows (with the
+ * pointwise work where the plane is the block's), of the rows just south
+ * and north of them and of their x-halo cells; releases the stage (the
+ * last warp to release it refills it with the plane NS ahead); then the
+ * stencil of this plane up to its top term and the epilogue of the plane
+ * below, from registers.  With R > 1 a warp's own rows are each other's
+ * south / north neighbours, so q is formed R + 2 times per R rows instead
+ * of 3 times per row. */
 template <typename T, int PASS>
-__global__ void __launch_bounds__(AS_THREADS, as_layout<T, PASS>::MINB)
+__global__ void __launch_bounds__(as_layout<T, PASS>::THREADS, as_layout<T, PASS>::MINB)
 k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
 {
   typedef as_layout<T, PASS> L;
+  constexpr int R = L::R, NW = L::WARPS;
   bbb_kry *s = A.s;
   if(((volatile bbb_kry *)s)->done) return;
   extern __shared__ __align__(128) uint8_t as_dyn[];
@@ -586,10 +643,13 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
     const int k1 = left_ < (long long)(B.nz - k0) ? k0 + (int)left_ : B.nz;
     const int ti = (int)(gt % gtx) * B.gx + mem % B.gx;
     const int tj = (int)(gt / gtx) * B.gy + mem / B.gx;
-    const int i0 = ti * AS_W, j0 = tj * 8;
-    const int j = j0 + w;
-    const bool valid = j < B.ny;
-    const as_edges E = as_tile_edges(B, i0, j0);
+    const int i0 = ti * AS_W, j0 = tj * L::TH;
+    /* the warp's first row, its rows inside the box (<= 0: none) and the
+     * box row of its first row */
+    const int jw = j0 + R * w;
+    const int nv = B.ny - jw < R ? B.ny - jw : R;
+    const int rb = R * w + 1;
+    const as_edges E = as_tile_edges<L::TH>(B, i0, j0);
     const int cnt = k1 - k0 + 2;
     const long long L0 = nload;
     if(tid == 0)
@@ -598,48 +658,56 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
         as_issue<T, PASS>(B, A, M, sbase + b * L::STAGE, as_saddr(&bars[b]), i0, j0,
           mapz(B, k0 - 1 + a), E);
       }
-    /* this warp's offsets inside a stage: own row (box row w + 1), south
-     * and north rows (box rows w, w + 2, or the wrap rows at the faces),
-     * x-halo cell (lane 0 west, lane 31 east) */
-    const int h_own = (w + 1) * L::ROWP + (L::CH + col) * L::ESZ;
-    const int m_own = L::MASK_OFF + (w + 1) * L::MROWP + 16 + col;
-    const int h_s = j == 0 ? L::EXT_OFF + col * L::ESZ
-                           : w * L::ROWP + (L::CH + col) * L::ESZ;
-    const int m_s = j == 0 ? L::MASK_OFF + L::MEXT_OFF + col
-                           : L::MASK_OFF + w * L::MROWP + 16 + col;
-    const int h_n = j + 1 == B.ny ? L::EXT_OFF + L::OWNB + col * L::ESZ
-                                  : (w + 2) * L::ROWP + (L::CH + col) * L::ESZ;
-    const int m_n = j + 1 == B.ny ? L::MASK_OFF + L::MEXT_OFF + 128 + col
-                                  : L::MASK_OFF + (w + 2) * L::MROWP + 16 + col;
-    int h_x, m_x, x_stride;
+    /* this warp's offsets inside a stage: its first own row (box row rb;
+     * row r at + r ROWP), the row south of its first row (box row rb - 1
+     * or the wrap row at the face), the row north of its last row inside
+     * the box (box row rb + R or the wrap row), the x-halo cell of its
+     * first row (lane 0 west, lane 31 east; row r at + r hx_rs) */
+    const int h_own = rb * L::ROWP + (L::CH + col) * L::ESZ;
+    const int m_own = L::MASK_OFF + rb * L::MROWP + 16 + col;
+    const int h_s = jw == 0 ? L::EXT_OFF + col * L::ESZ
+                            : (rb - 1) * L::ROWP + (L::CH + col) * L::ESZ;
+    const int m_s = jw == 0 ? L::MASK_OFF + L::MEXT_OFF + col
+                            : L::MASK_OFF + (rb - 1) * L::MROWP + 16 + col;
+    const bool nwrap = jw + nv == B.ny;
+    const int h_n = nwrap ? L::EXT_OFF + L::OWNB + col * L::ESZ
+                          : (rb + R) * L::ROWP + (L::CH + col) * L::ESZ;
+    const int m_n = nwrap ? L::MASK_OFF + L::MEXT_OFF + 128 + col
+                          : L::MASK_OFF + (rb + R) * L::MROWP + 16 + col;
+    int h_x, m_x, x_stride, hx_rs, mx_rs;
     if(tx == 0) {
       if(E.xl) {
-        h_x = L::XW_OFF + w * 16 + (B.wW % L::CH) * L::ESZ;
-        m_x = L::XW_OFF + L::NA * 256 + w * 16 + B.wW % 16;
-        x_stride = 256;
+        h_x = L::XW_OFF + (R * w) * 16 + (B.wW % L::CH) * L::ESZ;
+        m_x = L::XW_OFF + L::NA * L::XWA + (R * w) * 16 + B.wW % 16;
+        x_stride = L::XWA; hx_rs = 16; mx_rs = 16;
       } else {
-        h_x = (w + 1) * L::ROWP + (L::CH - 1) * L::ESZ;
-        m_x = L::MASK_OFF + (w + 1) * L::MROWP + 15;
-        x_stride = L::AREG;
+        h_x = rb * L::ROWP + (L::CH - 1) * L::ESZ;
+        m_x = L::MASK_OFF + rb * L::MROWP + 15;
+        x_stride = L::AREG; hx_rs = L::ROWP; mx_rs = L::MROWP;
       }
     } else {
       if(E.xr) {
-        h_x = L::XW_OFF + 128 + w * 16 + (B.wE % L::CH) * L::ESZ;
-        m_x = L::XW_OFF + L::NA * 256 + 128 + w * 16 + B.wE % 16;
-        x_stride = 256;
+        h_x = L::XW_OFF + L::TH * 16 + (R * w) * 16 + (B.wE % L::CH) * L::ESZ;
+        m_x = L::XW_OFF + L::NA * L::XWA + L::TH * 16 + (R * w) * 16 + B.wE % 16;
+        x_stride = L::XWA; hx_rs = 16; mx_rs = 16;
       } else {
-        h_x = (w + 1) * L::ROWP + (L::CH + AS_W) * L::ESZ;
-        m_x = L::MASK_OFF + (w + 1) * L::MROWP + 16 + AS_W;
-        x_stride = L::AREG;
+        h_x = rb * L::ROWP + (L::CH + AS_W) * L::ESZ;
+        m_x = L::MASK_OFF + rb * L::MROWP + 16 + AS_W;
+        x_stride = L::AREG; hx_rs = L::ROWP; mx_rs = L::MROWP;
       }
     }
-    const int o_own = L::OWN_OFF + w * L::OWNB + col * L::ESZ;
-    /* carried from plane to plane: the previous plane's q, its stencil
-     * sum without the top term, its mask word and its epilogue inputs */
-    T qp[4], Pp[4], r0p[4], r1p[4];
-    unsigned mp = 0;
+    const int o_own = L::OWN_OFF + (R * w) * L::OWNB + col * L::ESZ;
+    /* carried from plane to plane, per own row: the previous plane's q,
+     * its stencil sum without the top term, its mask word and its
+     * epilogue inputs */
+    T qp[R][4], Pp[R][4], r0p[R][4], r1p[R][4];
+    unsigned mp[R];
 #pragma unroll
-    for(int v = 0; v < 4; v++) qp[v] = Pp[v] = r0p[v] = r1p[v] = (T)0.;
+    for(int r = 0; r < R; r++) {
+      mp[r] = 0;
+#pragma unroll
+      for(int v = 0; v < 4; v++) qp[r][v] = Pp[r][v] = r0p[r][v] = r1p[r][v] = (T)0.;
+    }
     /* the stage of load L0 + a and its barrier phase, advanced per plane
      * (no 64-bit division in the loop) */
     int buf = (int)(L0 % L::NS);
@@ -649,89 +717,119 @@ k_bicg_async(boxc B, opc O, as_args<T> A, const __grid_constant__ as_maps M)
       const uint8_t *st = sm + buf * L::STAGE;
       if(!as_wait(as_saddr(&bars[buf]), par)) bad = 1;
       const bool full = pl >= k0 && pl < k1;
-      T qk[4], qS[4], qN[4], Pk[4], r0k[4], r1k[4];
-      T xq = (T)0.;
-      unsigned mk = 0;
-      if(valid) {
-        mk = *reinterpret_cast<const unsigned *>(st + m_own);
+      T qk[R][4], qS[4], qN[4], Pk[R][4], r0k[R][4], r1k[R][4];
+      T xq[R];
+      unsigned mk[R];
+#pragma unroll
+      for(int r = 0; r < R; r++) { mk[r] = 0; xq[r] = (T)0.; }
+      if(nv > 0) {
+#pragma unroll
+        for(int r = 0; r < R; r++) {
+          if(r < nv) {
+            mk[r] = *reinterpret_cast<const unsigned *>(st + m_own + r * L::MROWP);
+            if(full)
+              as_own4<T, PASS>(st + h_own + r * L::ROWP, mk[r], st + o_own + r * L::OWNB,
+                tab.dinv, S, lin(B, i0 + col, jw + r, pl), A, qk[r], r0k[r], r1k[r], red);
+            else
+              as_q4<T, PASS>(st + h_own + r * L::ROWP, mk[r], tab.dinv, S, qk[r]);
+          }
+        }
         if(full) {
-          as_own4<T, PASS>(st + h_own, mk, st + o_own, tab.dinv, S,
-            lin(B, i0 + col, j, pl), A, qk, r0k, r1k, red);
           as_q4<T, PASS>(st + h_s, *reinterpret_cast<const unsigned *>(st + m_s),
             tab.dinv, S, qS);
           as_q4<T, PASS>(st + h_n, *reinterpret_cast<const unsigned *>(st + m_n),
             tab.dinv, S, qN);
-          if(tx == 0 || tx == 31)
-            xq = as_q1<T, PASS>(st + h_x, x_stride, st[m_x], tab.dinv, S);
-        } else {
-          as_q4<T, PASS>(st + h_own, mk, tab.dinv, S, qk);
+          if(tx == 0 || tx == 31) {
+#pragma unroll
+            for(int r = 0; r < R; r++)
+              if(r < nv)
+                xq[r] = as_q1<T, PASS>(st + h_x + r * hx_rs, x_stride,
+                  st[m_x + r * mx_rs], tab.dinv, S);
+          }
         }
       }
-      /* release the stage: the last of the 8 warps to finish reading it
+      /* release the stage: the last of the warps to finish reading it
        * refills it with the plane NS ahead (no block-wide barrier, so
        * warps drift apart by up to the stage depth) */
       __syncwarp();
       if(tx == 0) {
         uint32_t old = as_release(as_saddr(&rel[buf]));
-        if(old % 8u == 7u && a + L::NS < cnt)
+        if(old % (uint32_t)NW == (uint32_t)(NW - 1) && a + L::NS < cnt)
           as_issue<T, PASS>(B, A, M, sbase + buf * L::STAGE, as_saddr(&bars[buf]),
             i0, j0, mapz(B, pl + L::NS), E);
       }
-      if(valid) {
+      if(nv > 0) {
         if(full) {
           /* this plane's stencil up to its top term, while its south,
            * north and x-halo q are at hand */
-          T lft = __shfl_up_sync(0xffffffffu, qk[3], 1);
-          T rgt = __shfl_down_sync(0xffffffffu, qk[0], 1);
-          if(tx == 0) lft = xq;
-          if(tx == 31) rgt = xq;
 #pragma unroll
-          for(int v = 0; v < 4; v++) {
-            unsigned mv = mbyte(mk, v);
-            T qW = v > 0 ? qk[v - 1] : lft;
-            T qE = v < 3 ? qk[v + 1] : rgt;
-            Pk[v] = as_apply_lo<T>(mv, tab.diag[mv], wx, wy, qp[v], qS[v], qW,
-              qk[v], qE, qN[v], wz);
+          for(int r = 0; r < R; r++) {
+            if(r < nv) {
+              T lft = __shfl_up_sync(0xffffffffu, qk[r][3], 1);
+              T rgt = __shfl_down_sync(0xffffffffu, qk[r][0], 1);
+              if(tx == 0) lft = xq[r];
+              if(tx == 31) rgt = xq[r];
+              const bool nin = r + 1 < R && r + 1 < nv;
+#pragma unroll
+              for(int v = 0; v < 4; v++) {
+                unsigned mv = mbyte(mk[r], v);
+                T qW = v > 0 ? qk[r][v - 1] : lft;
+                T qE = v < 3 ? qk[r][v + 1] : rgt;
+                T qs = r > 0 ? qk[r > 0 ? r - 1 : 0][v] : qS[v];
+                T qn = nin ? qk[r + 1 < R ? r + 1 : r][v] : qN[v];
+                Pk[r][v] = as_apply_lo<T>(mv, tab.diag[mv], wx, wy, qp[r][v], qs, qW,
+                  qk[r][v], qE, qn, wz);
+              }
+            }
           }
         }
         if(a >= 2) {
           /* the previous plane completed by its top term */
           const int k = pl - 1;
-          T Aq[4];
 #pragma unroll
-          for(int v = 0; v < 4; v++)
-            Aq[v] = as_apply_hi<T>(mbyte(mp, v), wz, Pp[v], qp[v], qk[v]);
-          const long long ge = lin(B, i0 + col, j, k);
-          if constexpr(PASS == 0) {
-            as_st4<T>(A.w2 + ge, Aq);
-            as_dot4<T>(red[0], r0p, Aq);
-          } else if constexpr(PASS == 1) {
-            as_st4<T>(A.w1 + ge, Aq);
-            as_dot4<T>(red[0], Aq, r0p);
-            as_dot4<T>(red[1], Aq, Aq);
-            as_dot4<T>(red[3], r1p, r0p);
-            as_dot4<T>(red[4], r1p, Aq);
-          } else if constexpr(PASS == 3) {
-            /* y = A p and (A p, p), as epi_c1 */
-            as_st4<T>(A.w1 + ge, Aq);
-            as_dot4<T>(red[0], Aq, r0p);
-          } else {
-            /* outer residual r = b - A x in FP64, stored rounded to FP32 */
-            T rr[4];
+          for(int r = 0; r < R; r++) {
+            if(r < nv) {
+              T Aq[4];
 #pragma unroll
-            for(int v = 0; v < 4; v++) rr[v] = r0p[v] - Aq[v];
-            *reinterpret_cast<float4 *>(A.rf + ge) =
-              make_float4((float)rr[0], (float)rr[1], (float)rr[2], (float)rr[3]);
-            as_dot4<T>(red[0], rr, rr);
-            as_sum4<T>(red[2], rr);
+              for(int v = 0; v < 4; v++)
+                Aq[v] = as_apply_hi<T>(mbyte(mp[r], v), wz, Pp[r][v], qp[r][v], qk[r][v]);
+              const long long ge = lin(B, i0 + col, jw + r, k);
+              if constexpr(PASS == 0) {
+                as_st4<T>(A.w2 + ge, Aq);
+                as_dot4<T>(red[0], r0p[r], Aq);
+              } else if constexpr(PASS == 1) {
+                as_st4<T>(A.w1 + ge, Aq);
+                as_dot4<T>(red[0], Aq, r0p[r]);
+                as_dot4<T>(red[1], Aq, Aq);
+                as_dot4<T>(red[3], r1p[r], r0p[r]);
+                as_dot4<T>(red[4], r1p[r], Aq);
+              } else if constexpr(PASS == 3) {
+                /* y = A p and (A p, p), as epi_c1 */
+                as_st4<T>(A.w1 + ge, Aq);
+                as_dot4<T>(red[0], Aq, r0p[r]);
+              } else {
+                /* outer residual r = b - A x in FP64, stored rounded to FP32 */
+                T rr[4];
+#pragma unroll
+                for(int v = 0; v < 4; v++) rr[v] = r0p[r][v] - Aq[v];
+                *reinterpret_cast<float4 *>(A.rf + ge) =
+                  make_float4((float)rr[0], (float)rr[1], (float)rr[2], (float)rr[3]);
+                as_dot4<T>(red[0], rr, rr);
+                as_sum4<T>(red[2], rr);
+              }
+            }
           }
         }
       }
 #pragma unroll
-      for(int v = 0; v < 4; v++) {
-        qp[v] = qk[v]; Pp[v] = Pk[v]; r0p[v] = r0k[v]; r1p[v] = r1k[v];
+      for(int r = 0; r < R; r++) {
+#pragma unroll
+        for(int v = 0; v < 4; v++) {
+          qp[r][v] = qk[r][v]; Pp[r][v] = Pk[r][v];
+          r0p[r][v] = r0k[r][v]; r1p[r][v] = r1k[r][v];
+        }
+        mp[r] = mk[r];
       }
-      mp = mk;
       if(++buf == L::NS) { buf = 0; par ^= 1u; }
     }
     nload = L0 + cnt;
