@@ -10,21 +10,24 @@
  * and v it reads anyway (the same FP32 or FP64 expression, so the same
  * bits), which takes one vector write out of every iteration.  Pass A
  * reads r and writes the new r, so r alternates between two buffers (the
- * second is the one s would have used).  A block owns a 128 x 8 tile and marches along z.  For every plane
- * it needs, one thread issues a handful of 3-D tensor copies -- per input
- * array one box of 10 rows x (128 + two 16-byte x-halo chunks), the mask
- * likewise, the block's own 8 rows of the arrays only it reads -- into a
- * shared-memory stage whose mbarrier completes when all bytes have landed.
+ * second is the one s would have used).  A block owns a tile of 128 cells
+ * x TH rows (TH = 8 or 16, per pass and precision) and marches along z.
+ * For every plane it needs, one thread issues a handful of 3-D tensor
+ * copies -- per input array one box of TH + 2 rows x (128 + two 16-byte
+ * x-halo chunks), the mask likewise, the block's own TH rows of the arrays
+ * only it reads -- into a shared-memory stage whose mbarrier completes when
+ * all bytes have landed.
  * NS stages rotate, so the next plane is in flight while the block
  * computes this one (two stages measured faster than three, four or five
  * on 256x256x512: pass A 2%, pass B 5%, the FP64 pass B 7%); the warps
  * synchronise only through the stages' barriers and release counts, never
  * block-wide inside a run of planes.
  *
- * Every warp owns one tile row and computes the Jacobi-scaled stencil input
- * q for its row and for the rows just south and north of it straight from
- * the stage (no shared ring, so the stages of two blocks fit per SM); the
- * row's x-halo q comes from the stage's halo chunks.  A plane's stencil
+ * Every warp owns R adjacent tile rows (R = 1 or 2) and computes the
+ * Jacobi-scaled stencil input q for its rows and for the rows just south
+ * and north of them straight from the stage (no shared ring, so the stages
+ * of two blocks fit per SM); the rows' x-halo q come from the stage's halo
+ * chunks.  A plane's stencil
  * sum is formed up to its top term as soon as its stage is read, so its
  * south / north q die at once; the plane's q, that partial sum and its
  * epilogue inputs stay in registers until the plane above completes it.
@@ -33,7 +36,7 @@
  * their own, never under a box (two asynchronous writes to one byte would
  * race): the rows y = -1 and y = ny (the box's wS / wN rows) as plain bulk
  * copies of the tile's 128 cells, and the x-halo chunks at x = -1 and
- * x = nx (holding cells wW / wE) as 16-byte-wide boxes of the tile's 8
+ * x = nx (holding cells wW / wE) as 16-byte-wide boxes of the tile's TH
  * rows.  The tiled boxes' out-of-range parts are zero-filled and never read.
  *
  * Waits on the stage barriers are bounded; a wait that runs out marks the
