@@ -132,6 +132,7 @@ bbb_set_record_dir bbb_step bbb_advance_clock bbb_get_stats bbb_last_status
 bbb_status_string bbb_clear_status bbb_set_exit_on_failure bbb_device_count
 bbb_divergence bbb_kernel_launches bbb_reset_kernel_launches
 bbb_profile_enable bbb_profile_reset bbb_profile_get bbb_profile_get_pass
+bbb_stage_layout
 bbb_part_state_push
 bbb_part_state_pull bbb_mark bbb_mark_elapsed bbb_PP_bicgstab_static
 bbb_learn_enable bbb_learn_train bbb_learn_crops bbb_learn_param_count
@@ -197,6 +198,8 @@ def load():
                                     C.POINTER(R)]
     lib.bbb_profile_get_pass.argtypes = [C.c_int, C.POINTER(R),
                                          C.POINTER(C.c_longlong), C.POINTER(R)]
+    lib.bbb_stage_layout.restype = C.c_int
+    lib.bbb_stage_layout.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int]
     lib.bbb_learn_enable.argtypes = [C.c_int]
     lib.bbb_learn_train.argtypes = [C.c_int, R]
     lib.bbb_learn_train.restype = R

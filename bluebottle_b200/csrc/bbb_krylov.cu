@@ -1001,6 +1001,40 @@ extern "C" void bbb_profile_get_pass(int pass, double *ms, long long *launches,
   *ms = g_prof.ms[pass]; *launches = g_prof.launches[pass]; *bytes = g_prof.kbytes[pass];
 }
 
+/* the stage layout constants of one staged pass, in the order the header
+ * lists them; host arithmetic only */
+template <typename T, int PASS>
+static int stage_layout(int *out, int nout)
+{
+  typedef as_layout<T, PASS> L;
+  const int v[BBB_STAGE_LAYOUT_N] = {L::ESZ, L::CH, L::NA, L::NO, L::R, L::TH,
+    L::WARPS, L::THREADS, L::BOXW, L::BOXH, L::ROWP, L::OWNB, L::EXT_OFF, L::AREG,
+    L::MROWP, L::MEXT_OFF, L::MREG, L::MASK_OFF, L::OWN_OFF, L::XW_OFF, L::XWA,
+    L::STAGE, L::NS, L::SMEM, L::TX_BASE, L::TX_XSIDE, L::TX_YSIDE, L::MINB};
+  if(!out || nout < BBB_STAGE_LAYOUT_N) return -1;
+  for(int a = 0; a < BBB_STAGE_LAYOUT_N; a++) out[a] = v[a];
+  return BBB_STAGE_LAYOUT_N;
+}
+
+extern "C" int bbb_stage_layout(int fp64, int pass, int *out, int nout)
+{
+  if(fp64) {
+    switch(pass) {
+    case 0: return stage_layout<double, 0>(out, nout);
+    case 1: return stage_layout<double, 1>(out, nout);
+    case 2: return stage_layout<double, 2>(out, nout);
+    case 3: return stage_layout<double, 3>(out, nout);
+    }
+  } else {
+    switch(pass) {
+    case 0: return stage_layout<float, 0>(out, nout);
+    case 1: return stage_layout<float, 1>(out, nout);
+    case 3: return stage_layout<float, 3>(out, nout);
+    }
+  }
+  return -1;
+}
+
 /* run iterations until the device says done; the host polls the scalars
  * in growing batches so a converged solve costs at most a few no-op
  * launches */

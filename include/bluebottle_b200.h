@@ -308,6 +308,23 @@ void bbb_profile_get(double *ms, long long *iters, double *bytes);
 void bbb_profile_get_pass(int pass, double *ms, long long *launches,
   double *bytes);
 
+/* Shared-memory stage layout of one tensor-map-staged solver pass as
+ * compiled (no counterpart in the reference; a diagnostic for host-side
+ * checks of the copies and reads, no GPU needed).  fp64: 0 or 1; pass: 0
+ * BiCGSTAB pass A, 1 pass B, 2 the FP64 outer residual (fp64 = 1 only), 3
+ * the Helmholtz CG stencil pass.  Writes BBB_STAGE_LAYOUT_N ints, in
+ * bytes unless named otherwise: element size, 16-byte chunk in elements,
+ * halo arrays, own arrays, rows per warp, tile rows, warps, threads, box
+ * width (elements), box rows, box row pitch, own row bytes, wrap-row
+ * offset, halo array region, mask row pitch, mask wrap-row offset, mask
+ * region, mask offset, own-array offset, x-wrap offset, x-wrap bytes per
+ * array, stage, stages, dynamic shared memory per block, armed bytes of
+ * the boxes, of one x side, of one y side, resident blocks the register
+ * budget targets.  Returns BBB_STAGE_LAYOUT_N, or -1 for an unknown pass
+ * or a short buffer. */
+#define BBB_STAGE_LAYOUT_N 28
+int bbb_stage_layout(int fp64, int pass, int *out, int nout);
+
 /* Copy only the particle records (part_struct array) between the host
  * `parts` and the device: the per-step exchange of a caller that moves
  * particle state, without the phase/flag arrays cuda_part_push/pull also
