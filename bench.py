@@ -195,7 +195,7 @@ def profiler_range(on):
 
 def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
              learned=False, prof_range=False, keep=False, lamb_pp_tol=0.0,
-             gate=True):
+             gate=True, barrier=None):
     """One fresh simulation of the workload in precision form `prec`:
     `warmup` untimed steps, PROBE_STEPS untimed steps, `steps` timed steps
     and `e2e_steps` end-to-end steps.  With `learned`, the warm-up steps
@@ -206,7 +206,9 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
     itself is cost-gated (bbb_learn_enable bit 4): the probe step measures
     the guess's cost and its estimated saving, and while the saving stays
     below the cost the guess is evaluated only every 8 .. 256 steps.
-    With `keep` the simulation is returned open in out["sim"]."""
+    With `keep` the simulation is returned open in out["sim"].  Each timed
+    region is bracketed by a drained solver stream and `barrier` (the
+    ranks' barrier under torchrun) on both sides."""
     from bluebottle_b200 import Sim
     import ctypes as C
     wl = workload(wl_name, prec)
@@ -214,6 +216,14 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
                                learned_guess=1 if learned else 0,
                                lamb_pp_tol=lamb_pp_tol))
     lib = sim.lib
+
+    def drain_and_barrier():
+        # event slot 5: record and wait, so the stream is idle here
+        lib.bbb_mark(5)
+        lib.bbb_mark_elapsed(5, 5)
+        if barrier is not None:
+            barrier()
+
     sim.prepare()
     if learned:
         lib.bbb_learn_train.restype = C.c_double
@@ -245,6 +255,7 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
     launches0 = lib.bbb_kernel_launches()
     if prof_range:
         profiler_range(True)
+    drain_and_barrier()
     lib.bbb_mark(0)
     for _ in range(steps):
         sim.step()
@@ -259,6 +270,7 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
         if st.guess_evaluated and st.extrap_r0 > 0 and st.guess_r0 > 0:
             ratios.append(st.guess_r0 / st.extrap_r0)
     lib.bbb_mark(1)
+    drain_and_barrier()
     if prof_range:
         profiler_range(False)
     out["guess_used_steps"] = used
@@ -291,6 +303,7 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
     # untimed: every timed end-to-end step then pushes the records the
     # previous one pulled
     lib.bbb_part_state_pull()
+    drain_and_barrier()
     lib.bbb_mark(2)
     for _ in range(e2e_steps):
         lib.bbb_part_state_push()
@@ -299,6 +312,7 @@ def run_form(prec, steps, warmup, e2e_steps, profile=True, wl_name="c5",
         _ = sim.scalar("dt")
         e2e_iters += sim.stats().pp_iters_total
     lib.bbb_mark(3)
+    drain_and_barrier()
     out["e2e_ms"] = lib.bbb_mark_elapsed(2, 3)
     # the end-to-end steps follow the timed ones, later in the run: their
     # iteration count is reported beside their rate
@@ -459,7 +473,8 @@ def main():
     mixed = run_form(1, steps, warmup, e2e_steps=steps, wl_name=args.workload,
                      prof_range=args.profile_range,
                      learned=not args.no_learned, keep=want_cpu,
-                     lamb_pp_tol=args.lamb_pp_tol, gate=not args.no_gate)
+                     lamb_pp_tol=args.lamb_pp_tol, gate=not args.no_gate,
+                     barrier=dist.barrier)
     clocks = sampler.stop()
     ms = dist.max(mixed["ms"])
     e2e_ms = dist.max(mixed["e2e_ms"])
@@ -475,7 +490,7 @@ def main():
     fp64 = None
     if not args.no_fp64:
         fp64 = run_form(0, steps, warmup, e2e_steps=0, wl_name=args.workload,
-                        lamb_pp_tol=args.lamb_pp_tol)
+                        lamb_pp_tol=args.lamb_pp_tol, barrier=dist.barrier)
         fp64["ms"] = dist.max(fp64["ms"])
     dist.barrier()
     if rank == 0:
